@@ -1,0 +1,238 @@
+"""CPU oracle for the FMM gravity evaluation -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this
+package, and only as the checker / the timed CPU baseline.  The product
+(``taichi_collisional_b200``) never imports it.
+
+Two independent CPU implementations sit behind it:
+
+* ``liboracle.so`` -- ``tc_oracle.c``, a plain-C FP64 restatement of the reference's
+  theta-MAC force evaluation (tree build, Miniball centres, P2M/M2M, dual traversal,
+  rotation M2L, L2L/L2P, P2P with jerks) plus an FP64 direct sum;
+* ``_ref/libtcref_<tree>_p<P>_<isa>.so`` -- the reference's own headers compiled behind
+  ``ref_harness.cpp`` (built here by ``oracle/Makefile``; the reference sources are not
+  part of this repository).  These pin the restatement and give the "reference" CPU
+  baseline.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+VARIANT_TOP, VARIANT_JERKS = 0, 1
+
+_lib = None
+_ref_libs = {}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u8p = C.POINTER(C.c_ubyte)
+
+
+class Params(C.Structure):
+    _fields_ = [("p", C.c_int), ("ncrit", C.c_int), ("variant", C.c_int), ("use_shift", C.c_int),
+                ("theta", C.c_double), ("shift_u", C.c_double * 3), ("direct_below", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n_cells", C.c_longlong), ("n_leaves", C.c_longlong), ("n_m2l", C.c_longlong),
+                ("n_p2p", C.c_longlong), ("n_p2p_inter", C.c_longlong), ("max_level", C.c_int)]
+
+
+def _d(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+
+
+def build():
+    """Compile liboracle.so (and, when the reference tree is present, oracle/_ref)."""
+    subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
+    if os.path.isdir(os.environ.get("TC_REFERENCE", "/root/reference")):
+        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref",
+                               "REF=" + os.environ.get("TC_REFERENCE", "/root/reference")])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
+        L = C.CDLL(path)
+        L.tco_evaluate.argtypes = [C.POINTER(Params), C.c_int] + [_dp] * 7 + [_u8p] + [_dp] * 7 + [C.POINTER(Stats)]
+        L.tco_evaluate.restype = C.c_int
+        L.tco_last_ncell.restype = C.c_int
+        L.tco_last_cells.argtypes = [_ip] * 5 + [_dp, _dp, _ip]
+        L.tco_last_expansions.argtypes = [_dp] * 4
+        L.tco_last_list.argtypes = [C.c_int, _ip, _ip]
+        L.tco_last_list.restype = C.c_longlong
+        L.tco_direct.argtypes = [C.c_int] + [_dp] * 7 + [C.c_int, _ip] + [_dp] * 7
+        L.tco_init.argtypes = [C.c_int]
+        L.tco_make_gnm.argtypes = [_dp, _dp, _dp, C.c_int]
+        L.tco_swap_xz.argtypes = [_dp, C.c_int]
+        L.tco_p2m.argtypes = [C.c_int, C.c_int] + [_dp] * 10
+        L.tco_m2m.argtypes = [C.c_int] + [_dp] * 5
+        L.tco_m2l_rotate.argtypes = [C.c_int] + [_dp] * 5
+        L.tco_m2l_direct.argtypes = [C.c_int] + [_dp] * 3
+        L.tco_l2l.argtypes = [C.c_int] + [_dp] * 5
+        L.tco_l2p.argtypes = [C.c_int] + [_dp] * 5
+        L.tco_miniball.argtypes = [C.c_int, _dp, _dp, _dp]
+        L.tco_miniball.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def evaluate(x, y, z, m, vx=None, vy=None, vz=None, *, p, theta, ncrit, variant=VARIANT_JERKS,
+             shift_u=None, direct_below=0, flags=None):
+    """Oracle force evaluation; returns dict(ax, ay, az, pot, jx, jy, jz, stats)."""
+    L = lib()
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    vx, vy, vz = map(_f64, (vx, vy, vz))
+    prm = Params(p=p, ncrit=ncrit, variant=variant, use_shift=int(shift_u is not None),
+                 theta=theta, direct_below=direct_below)
+    if shift_u is not None:
+        for d in range(3):
+            prm.shift_u[d] = float(shift_u[d])
+    out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
+    st = Stats()
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    rc = L.tco_evaluate(C.byref(prm), n, _d(x), _d(y), _d(z), _d(vx), _d(vy), _d(vz), _d(m),
+                        None if fl is None else fl.ctypes.data_as(_u8p),
+                        *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")], C.byref(st))
+    if rc != 0:
+        raise RuntimeError("oracle evaluate failed (%d)" % rc)
+    out["stats"] = {f: getattr(st, f) for f, _ in Stats._fields_}
+    return out
+
+
+def last_cells():
+    L = lib()
+    nc = L.tco_last_ncell()
+    a = {k: np.zeros(nc, dtype=np.int32) for k in ("begin", "nbody", "nchild", "child", "level")}
+    X = np.zeros((nc, 3))
+    R = np.zeros(nc)
+    L.tco_last_cells(*[a[k].ctypes.data_as(_ip) for k in ("begin", "nbody", "nchild", "child", "level")],
+                     _d(X), _d(R), None)
+    n = int(a["nbody"][0]) if nc else 0
+    perm = np.zeros(n, dtype=np.int32)
+    L.tco_last_cells(*[a[k].ctypes.data_as(_ip) for k in ("begin", "nbody", "nchild", "child", "level")],
+                     _d(X), _d(R), perm.ctypes.data_as(_ip))
+    a["X"], a["R"], a["perm"] = X, R, perm
+    return a
+
+
+def last_lists():
+    L = lib()
+    out = {}
+    for kind, name in ((0, "m2l"), (1, "p2p")):
+        cnt = L.tco_last_list(kind, None, None)
+        t = np.zeros(cnt, dtype=np.int32)
+        s = np.zeros(cnt, dtype=np.int32)
+        L.tco_last_list(kind, t.ctypes.data_as(_ip), s.ctypes.data_as(_ip))
+        out[name] = (t, s)
+    return out
+
+
+def direct(x, y, z, m, vx=None, vy=None, vz=None, targets=None):
+    """FP64 direct summation at the given target indices (default: all)."""
+    L = lib()
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    vx, vy, vz = map(_f64, (vx, vy, vz))
+    tg = None if targets is None else np.ascontiguousarray(targets, dtype=np.int32)
+    nt = n if tg is None else len(tg)
+    out = {k: np.zeros(nt) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
+    L.tco_direct(n, _d(x), _d(y), _d(z), _d(vx), _d(vy), _d(vz), _d(m), nt,
+                 None if tg is None else tg.ctypes.data_as(_ip),
+                 *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")])
+    return out
+
+
+# ----------------------------------------------------------------------------------------
+# The reference's own code (oracle/_ref)
+# ----------------------------------------------------------------------------------------
+def _isa():
+    try:
+        with open("/proc/cpuinfo") as f:
+            flags = f.read()
+        return "avx512" if " avx512f " in flags and " avx512dq " in flags else "avx2"
+    except OSError:
+        return "avx2"
+
+
+def ref_path(variant, p):
+    tree = "jerks" if variant == VARIANT_JERKS else "top"
+    return os.path.join(HERE, "_ref", "libtcref_%s_p%d_%s.so" % (tree, p, _isa()))
+
+
+def ref_available(variant, p):
+    return os.path.exists(ref_path(variant, p))
+
+
+def ref_lib(variant, p):
+    key = (variant, p)
+    if key not in _ref_libs:
+        L = C.CDLL(ref_path(variant, p))
+        L.tcr_evaluate.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_long, C.c_int] + [_dp] * 8
+        L.tcr_evaluate.restype = C.c_int
+        L.tcr_cells.argtypes = [_ip] * 4 + [_dp, _dp, _ip]
+        L.tcr_expansions.argtypes = [_dp, _dp]
+        L.tcr_list.argtypes = [C.c_int, _ip, _ip]
+        L.tcr_list.restype = C.c_longlong
+        L.tcr_shift_uniforms.argtypes = [C.c_long, _dp]
+        _ref_libs[key] = L
+    return _ref_libs[key]
+
+
+def ref_shift_uniforms(variant, p, seed):
+    u = np.zeros(3)
+    ref_lib(variant, p).tcr_shift_uniforms(seed, _d(u))
+    return u
+
+
+def ref_evaluate(x, y, z, m, vx=None, vy=None, vz=None, *, p, theta, ncrit, variant=VARIANT_JERKS,
+                 seed=1, nthreads=1, flags=None):
+    """The reference's own theta-MAC evaluation.  nthreads=1 gives reproducible sums."""
+    L = ref_lib(variant, p)
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    vx, vy, vz = map(_f64, (vx, vy, vz))
+    out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
+    times = np.zeros(4)
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    nc = L.tcr_evaluate(n, _d(x), _d(y), _d(z), _d(vx), _d(vy), _d(vz), _d(m),
+                        None if fl is None else fl.ctypes.data_as(_u8p), theta, ncrit, seed, nthreads,
+                        *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")], _d(times))
+    out["ncell"] = nc
+    out["times"] = times
+    return out
+
+
+def ref_cells(variant, p, ncell, n):
+    L = ref_lib(variant, p)
+    a = {k: np.zeros(ncell, dtype=np.int32) for k in ("begin", "nbody", "nchild", "child")}
+    X = np.zeros((ncell, 3))
+    R = np.zeros(ncell)
+    idx = np.zeros(n, dtype=np.int32)
+    L.tcr_cells(*[a[k].ctypes.data_as(_ip) for k in ("begin", "nbody", "nchild", "child")], _d(X), _d(R),
+                idx.ctypes.data_as(_ip))
+    a["X"], a["R"], a["index"] = X, R, idx
+    return a
+
+
+def ref_lists(variant, p):
+    L = ref_lib(variant, p)
+    out = {}
+    for kind, name in ((0, "m2l"), (1, "p2p")):
+        cnt = L.tcr_list(kind, None, None)
+        t = np.zeros(cnt, dtype=np.int32)
+        s = np.zeros(cnt, dtype=np.int32)
+        L.tcr_list(kind, t.ctypes.data_as(_ip), s.ctypes.data_as(_ip))
+        out[name] = (t, s)
+    return out

@@ -1,0 +1,113 @@
+/* taichi_b200 -- B200-native FMM gravity evaluation behind a C ABI.
+ *
+ * This library replaces the force evaluation of QirongZhu/taichi_collisional:
+ *
+ *   void get_force_and_potential(Bodies& bodies, bool get_steps);
+ *     declared integrator.h:44, defined integrator.h:459-562 (top-level tree) and
+ *     taichi_with_jerks/integrator.h:308-432 (jerks tree); called by kick_naive
+ *     (integrator.h:245), kick_gradient (:353) and kick (:424), and in the jerks tree by
+ *     taichi_with_jerks/integrator.h:163 and :273.
+ *
+ * It computes, for every sink body, the acceleration F (G = 1), the potential p in the
+ * reference's positive convention (p = +sum m/r) and, for the jerks tree, the jerk J,
+ * using the reference's adaptive octree FMM with the theta opening criterion
+ * (traverse_eager.h:151-216; taichi_with_jerks/traverse_eager.h:125-168).
+ *
+ * Differences from the reference boundary (all deliberate):
+ *   - structure-of-arrays pointers instead of the AoS Body vector (exafmm.h:22-45);
+ *   - results are written in the caller's order, so the Body::index round trip
+ *     (integrator.h:190-301) is not needed and the caller's arrays are never reordered;
+ *   - every call returns a status code instead of calling exit() (exafmm.h:8-13).
+ *
+ * All entry points are thread-compatible per context (one context per host thread).
+ */
+#ifndef TAICHI_B200_H
+#define TAICHI_B200_H
+#include <stddef.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TC_PMAX 16
+
+typedef enum {
+  TC_OK = 0,
+  TC_ERR_ARG = 1,        /* bad argument (n <= 0, p out of range, NULL pointer) */
+  TC_ERR_CUDA = 2,       /* a CUDA runtime call failed; see tc_last_error_string */
+  TC_ERR_CAPACITY = 3,   /* an interaction list overflowed; the context grows and retries */
+  TC_ERR_NAN_INPUT = 4,  /* a position or mass is NaN/Inf */
+  TC_ERR_DEPTH = 5,      /* more than ncrit bodies share a level-21 cell (kept as one leaf) */
+  TC_ERR_UNSUPPORTED = 6 /* option not available in this build */
+} tc_status;
+
+typedef enum { TC_VARIANT_TOP = 0, TC_VARIANT_JERKS = 1 } tc_variant;
+typedef enum { TC_PREC_FP64 = 0, TC_PREC_MIXED = 1 } tc_precision;
+typedef enum { TC_MEM_HOST = 0, TC_MEM_DEVICE = 1 } tc_memory;
+
+typedef struct {
+  int p;              /* expansion order, 1..TC_PMAX (reference: EXPANSION, exafmm.h:52)    */
+  int ncrit;          /* max bodies per leaf (reference: ncrit, exafmm.h:113)               */
+  double theta;       /* opening angle: accept if |d|^2 theta^2 > (Ri+Rj)^2                 */
+  int variant;        /* tc_variant: which reference tree the evaluation restates          */
+  int precision;      /* tc_precision                                                       */
+  int use_shift;      /* jerks tree root-centre shift (taichi_with_jerks/build_tree.h:253)  */
+  double shift_u[3];  /* the three uniform draws the shift uses (drand48 in the reference)   */
+  int direct_below;   /* N below this -> direct sum; -1 = reference rule (top: ncrit,
+                         jerks: 8000; integrator.h:462, taichi_with_jerks/integrator.h:311) */
+  int device;         /* CUDA device ordinal                                               */
+} tc_params;
+
+typedef struct {
+  long long n_bodies, n_cells, n_leaves, n_m2l, n_p2p, n_p2p_inter;
+  int max_level;
+  double ms_total, ms_tree, ms_upward, ms_traverse, ms_m2l, ms_p2p, ms_downward;
+} tc_stats;
+
+typedef struct tc_ctx tc_ctx;
+
+/* Fill *prm with the reference defaults (p = 12, ncrit = 64, theta = 0.4, jerks tree). */
+void tc_default_params(tc_params* prm);
+
+/* Create a context on prm->device.  Replaces the globals P/NTERM/ncrit/theta
+ * (exafmm.h:111-114) and initKernel() (kernel_fast_lean.h:122-160). */
+tc_status tc_create(const tc_params* prm, tc_ctx** out);
+tc_status tc_destroy(tc_ctx* ctx);
+
+/* Run work on this CUDA stream (cudaStream_t passed as void*; NULL = legacy default). */
+tc_status tc_set_stream(tc_ctx* ctx, void* stream);
+
+/* One force evaluation: the replacement of get_force_and_potential(bodies, false).
+ *   x,y,z,m          positions and masses (required)
+ *   vx,vy,vz         velocities (jerks tree; may be NULL for the top tree)
+ *   flags            per body bit0 = sink (Body::issink), bit1 = source (Body::issource);
+ *                    NULL = every body is both
+ *   ax,ay,az,pot     outputs, caller order (overwritten, not accumulated)
+ *   jx,jy,jz         jerk outputs (jerks tree; may be NULL)
+ *   mem              TC_MEM_HOST or TC_MEM_DEVICE for ALL the pointers above
+ * Synchronous with respect to the host when mem == TC_MEM_HOST. */
+tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+                      const double* vx, const double* vy, const double* vz, const double* m,
+                      const unsigned char* flags, double* ax, double* ay, double* az,
+                      double* pot, double* jx, double* jy, double* jz, int mem);
+
+/* Statistics of the last evaluation (list sizes, per-phase device times). */
+tc_status tc_get_stats(tc_ctx* ctx, tc_stats* st);
+
+/* Inspection of the last evaluation (parity tests): cells in breadth-first order and the
+ * interaction lists (kind 0 = M2L, 1 = P2P) as (target cell, source cell) pairs sorted by
+ * target then source.  Host pointers; pass NULL to query sizes via tc_get_stats. */
+tc_status tc_get_cells(tc_ctx* ctx, int* begin, int* nbody, int* nchild, int* child, int* level,
+                       double* X /* 3 per cell */, double* R, int* perm /* n */);
+tc_status tc_get_lists(tc_ctx* ctx, int kind, int* tgt, int* src);
+tc_status tc_get_expansions(tc_ctx* ctx, double* M, double* Md, double* L, double* Ld);
+
+const char* tc_status_string(tc_status s);
+const char* tc_last_error_string(tc_ctx* ctx);
+int tc_pmax(void);
+/* 1 if expansion order p has compiled kernels in this build. */
+int tc_order_supported(int p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,232 @@
+"""taichi_collisional_b200 -- B200-native FMM gravity evaluation.
+
+Python view of the C ABI in ``include/taichi_b200.h`` (``libtaichi_b200.so``, built in-tree
+by ``taichi_collisional_b200.build``).  The entry point mirrors the reference's force
+evaluation ``get_force_and_potential(Bodies&, bool)`` (integrator.h:459-562,
+taichi_with_jerks/integrator.h:308-432): it takes positions, masses (and velocities for the
+jerks tree) and returns acceleration, potential (p = +sum m/r) and jerk for every sink body,
+in the caller's order.
+
+There is no CPU fallback: if the CUDA library cannot be loaded the calls raise.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import ics  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libtaichi_b200.so")
+
+VARIANT_TOP, VARIANT_JERKS = 0, 1
+PREC_FP64, PREC_MIXED = 0, 1
+MEM_HOST, MEM_DEVICE = 0, 1
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "capacity exceeded", 4: "non-finite input",
+          5: "tree depth limit reached", 6: "unsupported option"}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_u8p = C.POINTER(C.c_ubyte)
+
+
+class Params(C.Structure):
+    _fields_ = [("p", C.c_int), ("ncrit", C.c_int), ("theta", C.c_double), ("variant", C.c_int),
+                ("precision", C.c_int), ("use_shift", C.c_int), ("shift_u", C.c_double * 3),
+                ("direct_below", C.c_int), ("device", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n_bodies", C.c_longlong), ("n_cells", C.c_longlong), ("n_leaves", C.c_longlong),
+                ("n_m2l", C.c_longlong), ("n_p2p", C.c_longlong), ("n_p2p_inter", C.c_longlong),
+                ("max_level", C.c_int), ("ms_total", C.c_double), ("ms_tree", C.c_double),
+                ("ms_upward", C.c_double), ("ms_traverse", C.c_double), ("ms_m2l", C.c_double),
+                ("ms_p2p", C.c_double), ("ms_downward", C.c_double)]
+
+
+EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_evaluate", "tc_get_stats",
+           "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
+           "tc_pmax", "tc_order_supported"]
+
+_lib = None
+
+
+class TaichiError(RuntimeError):
+    pass
+
+
+def load_library(path=LIB_PATH):
+    """Load the CUDA library (raises if it is missing; there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise TaichiError("libtaichi_b200.so not built: run `python -m taichi_collisional_b200.build`")
+    L = C.CDLL(path)
+    L.tc_default_params.argtypes = [C.POINTER(Params)]
+    L.tc_create.argtypes = [C.POINTER(Params), C.POINTER(C.c_void_p)]
+    L.tc_create.restype = C.c_int
+    L.tc_destroy.argtypes = [C.c_void_p]
+    L.tc_destroy.restype = C.c_int
+    L.tc_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.tc_set_stream.restype = C.c_int
+    L.tc_evaluate.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8 + [C.c_void_p] * 7 + [C.c_int]
+    L.tc_evaluate.restype = C.c_int
+    L.tc_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+    L.tc_get_stats.restype = C.c_int
+    L.tc_get_cells.argtypes = [C.c_void_p] + [_ip] * 5 + [_dp, _dp, _ip]
+    L.tc_get_cells.restype = C.c_int
+    L.tc_get_lists.argtypes = [C.c_void_p, C.c_int, _ip, _ip]
+    L.tc_get_lists.restype = C.c_int
+    L.tc_get_expansions.argtypes = [C.c_void_p] + [_dp] * 4
+    L.tc_get_expansions.restype = C.c_int
+    L.tc_status_string.argtypes = [C.c_int]
+    L.tc_status_string.restype = C.c_char_p
+    L.tc_last_error_string.argtypes = [C.c_void_p]
+    L.tc_last_error_string.restype = C.c_char_p
+    L.tc_pmax.restype = C.c_int
+    L.tc_order_supported.argtypes = [C.c_int]
+    L.tc_order_supported.restype = C.c_int
+    _lib = L
+    return L
+
+
+def default_params(**kw):
+    L = load_library()
+    prm = Params()
+    L.tc_default_params(C.byref(prm))
+    for k, v in kw.items():
+        if k == "shift_u":
+            if v is None:
+                prm.use_shift = 0
+            else:
+                prm.use_shift = 1
+                for d in range(3):
+                    prm.shift_u[d] = float(v[d])
+        else:
+            setattr(prm, k, v)
+    return prm
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):  # torch tensor
+        return C.c_void_p(a.data_ptr())
+    return C.c_void_p(a.ctypes.data)
+
+
+class Gravity:
+    """A force-evaluation context (tc_create ... tc_destroy).
+
+    ``evaluate`` is the replacement of ``get_force_and_potential(bodies, false)``.
+    Inputs are numpy float64 arrays (host) or CUDA float64 torch tensors (device).
+    """
+
+    def __init__(self, p=12, ncrit=64, theta=0.4, variant=VARIANT_JERKS, precision=PREC_FP64, shift_u=None,
+                 direct_below=-1, device=0):
+        self._L = load_library()
+        self.params = default_params(p=p, ncrit=ncrit, theta=theta, variant=variant, precision=precision,
+                                     shift_u=shift_u, direct_below=direct_below, device=device)
+        h = C.c_void_p()
+        rc = self._L.tc_create(C.byref(self.params), C.byref(h))
+        if rc != 0:
+            raise TaichiError("tc_create failed: %s" % STATUS.get(rc, rc))
+        self._h = h
+        self.jerk = variant == VARIANT_JERKS
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.tc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        self._L.tc_set_stream(self._h, C.c_void_p(stream_ptr))
+
+    def _check(self, rc, what):
+        if rc != 0:
+            msg = self._L.tc_last_error_string(self._h).decode()
+            raise TaichiError("%s: %s %s" % (what, STATUS.get(rc, rc), msg))
+
+    def evaluate(self, x, y, z, m, vx=None, vy=None, vz=None, flags=None, out=None):
+        """Returns dict ax, ay, az, pot (and jx, jy, jz with jerks) in the caller's order."""
+        n = len(x)
+        dev = hasattr(x, "data_ptr")
+        if out is None:
+            if dev:
+                import torch
+                out = {k: torch.empty(n, dtype=torch.float64, device=x.device) for k in
+                       (("ax", "ay", "az", "pot", "jx", "jy", "jz") if self.jerk else ("ax", "ay", "az", "pot"))}
+            else:
+                out = {k: np.zeros(n) for k in
+                       (("ax", "ay", "az", "pot", "jx", "jy", "jz") if self.jerk else ("ax", "ay", "az", "pot"))}
+        if not dev:
+            x, y, z, m = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, m))
+            if vx is not None:
+                vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64) for a in (vx, vy, vz))
+            if flags is not None:
+                flags = np.ascontiguousarray(flags, dtype=np.uint8)
+        rc = self._L.tc_evaluate(self._h, n, _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(m),
+                                 _ptr(flags), _ptr(out["ax"]), _ptr(out["ay"]), _ptr(out["az"]), _ptr(out["pot"]),
+                                 _ptr(out.get("jx")), _ptr(out.get("jy")), _ptr(out.get("jz")),
+                                 MEM_DEVICE if dev else MEM_HOST)
+        self._check(rc, "tc_evaluate")
+        return out
+
+    def stats(self):
+        st = Stats()
+        self._L.tc_get_stats(self._h, C.byref(st))
+        return {f: getattr(st, f) for f, _ in Stats._fields_}
+
+    def cells(self):
+        st = self.stats()
+        nc, n = int(st["n_cells"]), int(st["n_bodies"])
+        a = {k: np.zeros(nc, dtype=np.int32) for k in ("begin", "nbody", "nchild", "child", "level")}
+        X = np.zeros((nc, 3))
+        R = np.zeros(nc)
+        perm = np.zeros(n, dtype=np.int32)
+        rc = self._L.tc_get_cells(self._h, *[a[k].ctypes.data_as(_ip) for k in ("begin", "nbody", "nchild", "child",
+                                                                                  "level")],
+                                  X.ctypes.data_as(_dp), R.ctypes.data_as(_dp), perm.ctypes.data_as(_ip))
+        self._check(rc, "tc_get_cells")
+        a["X"], a["R"], a["perm"] = X, R, perm
+        return a
+
+    def lists(self):
+        st = self.stats()
+        out = {}
+        for kind, name, cnt in ((0, "m2l", st["n_m2l"]), (1, "p2p", st["n_p2p"])):
+            t = np.zeros(cnt, dtype=np.int32)
+            s = np.zeros(cnt, dtype=np.int32)
+            rc = self._L.tc_get_lists(self._h, kind, t.ctypes.data_as(_ip), s.ctypes.data_as(_ip))
+            self._check(rc, "tc_get_lists")
+            out[name] = (t, s)
+        return out
+
+    def expansions(self):
+        st = self.stats()
+        nt = (self.params.p + 1) ** 2
+        nc = int(st["n_cells"])
+        M, L = np.zeros((nc, nt)), np.zeros((nc, nt))
+        Md = np.zeros((nc, nt)) if self.jerk else None
+        Ld = np.zeros((nc, nt)) if self.jerk else None
+        rc = self._L.tc_get_expansions(self._h, M.ctypes.data_as(_dp), None if Md is None else Md.ctypes.data_as(_dp),
+                                       L.ctypes.data_as(_dp), None if Ld is None else Ld.ctypes.data_as(_dp))
+        self._check(rc, "tc_get_expansions")
+        return M, Md, L, Ld
+
+
+def get_force_and_potential(x, y, z, m, vx=None, vy=None, vz=None, flags=None, **params):
+    """One-shot helper: create a context, evaluate, destroy."""
+    g = Gravity(**params)
+    try:
+        return g.evaluate(x, y, z, m, vx, vy, vz, flags)
+    finally:
+        g.close()

@@ -1,0 +1,662 @@
+// C ABI and host orchestration of the B200 FMM gravity evaluation (include/taichi_b200.h).
+//
+// One tc_evaluate call replaces get_force_and_potential(bodies, false)
+// (integrator.h:459-562, taichi_with_jerks/integrator.h:308-432) on the theta-MAC path:
+//   bounds -> Morton keys -> radix sort -> octree levels      (build_tree.h)
+//   smallest enclosing balls + P2M / M2M, deepest level first  (traverse_eager.h:9-34)
+//   dual traversal -> sorted M2L and P2P lists                 (traverse_eager.h:151-216)
+//   M2L (rotation, FP64) and P2P                               (kernel_fast_lean.h)
+//   L2L level by level, L2P                                    (traverse_eager.h:326-346)
+// All arithmetic runs on the GPU; there is no CPU fallback.  The only host reads are the
+// tree's level table and the list sizes (to size launches and buffers).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "tc_common.cuh"
+#include "tc_tree.cuh"
+#include "tc_upward.cuh"
+#include "tc_traverse.cuh"
+#include "tc_m2l.cuh"
+#include "tc_down.cuh"
+#include "tc_p2p.cuh"
+#include "tdesign.h"
+
+using namespace tc;
+
+namespace {
+
+template <class T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t ensure(size_t want) {
+    if (want <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    size_t alloc = want + want / 8 + 16;
+    cudaError_t e = cudaMalloc((void**)&p, alloc * sizeof(T));
+    if (e == cudaSuccess) n = alloc;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+
+struct EvalTimes {
+  cudaEvent_t e[8];
+};
+
+}  // namespace
+
+struct tc_ctx {
+  tc_params prm;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  tc_stats stats;
+  // staging (host-memory calls)
+  DBuf<double> in_d;  // 7 * N
+  DBuf<uint8_t> in_f;
+  DBuf<double> out_d;  // 7 * N (caller order)
+  // bodies
+  DBuf<unsigned long long> keys, keys_alt;
+  DBuf<int> vals, vals_alt;
+  DBuf<uint32_t> hist;
+  DBuf<double> bod;  // 7 * N sorted
+  DBuf<uint8_t> bflags;
+  DBuf<int> perm;
+  DBuf<double> outs;  // 7 * N sorted
+  // cells
+  DBuf<int> cint;      // 6 * ccap
+  DBuf<double> cdbl;   // 7 * ccap
+  DBuf<uint8_t> csink;
+  DBuf<int> split_off;
+  DBuf<double> expn;   // (2 or 4) * ncell * NT
+  size_t ccap = 0;
+  // lists
+  DBuf<int2> front[2];
+  DBuf<unsigned long long> m2l, m2l_alt, p2p, p2p_alt;
+  DBuf<int> m2l_start, m2l_src, p2p_start, p2p_src, m2l_tl, p2p_tl, leaves;
+  size_t fcap = 0, mcap = 0, pcap = 0;
+  // small device structs
+  TcRootInfo* d_root = nullptr;
+  TcLevels* d_lv = nullptr;
+  TcTravCounters* d_cnt = nullptr;
+  unsigned int* d_err = nullptr;
+  unsigned int* d_small = nullptr;  // [0] m2l targets, [1] p2p targets, [2] leaves
+  DBuf<double> bpart;
+  // last evaluation
+  TcLevels lv;
+  int n = 0, ncell = 0, nleaf = 0, max_level = 0, direct = 0;
+  unsigned long long n_m2l = 0, n_p2p = 0;
+  int sbits = 1;
+  cudaEvent_t ev[8];
+  bool events = false;
+};
+
+static bool g_const_init[64];
+
+static tc_status cuda_fail(tc_ctx* c, cudaError_t e, const char* what) {
+  if (c) c->err = std::string(what) + ": " + cudaGetErrorString(e);
+  return TC_ERR_CUDA;
+}
+
+#define TC_CK(call)                                   \
+  do {                                                \
+    cudaError_t e_ = (call);                          \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call); \
+  } while (0)
+
+static cudaError_t init_constants(int dev) {
+  if (dev >= 0 && dev < 64 && g_const_init[dev]) return cudaSuccess;
+  double fact[2 * TC_PMAX_DEV + 2];
+  fact[0] = 1.0;
+  for (int i = 1; i < 2 * TC_PMAX_DEV + 2; i++) fact[i] = fact[i - 1] * (double)i;
+  double fc[TC_NTERM(TC_PMAX_DEV)], fci[TC_NTERM(TC_PMAX_DEV)];
+  for (int n = 0; n <= TC_PMAX_DEV; n++)
+    for (int m = -n; m <= n; m++) {
+      int am = m < 0 ? -m : m;
+      double f = fact[n + am] * fact[n - am];
+      fc[n * n + n + m] = f;
+      fci[n * n + n + m] = 1.0 / f;
+    }
+  cudaError_t e;
+  if ((e = cudaMemcpyToSymbol(c_fact, fact, sizeof(fact))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_fc, fc, sizeof(fc))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_fcinv, fci, sizeof(fci))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_tdesign, tc_tdesign, sizeof(tc_tdesign))) != cudaSuccess) return e;
+  if (dev >= 0 && dev < 64) g_const_init[dev] = true;
+  return cudaSuccess;
+}
+
+static inline int nblocks(long long n, int t) { return (int)((n + t - 1) / t); }
+
+static TcCells cells_view(tc_ctx* c, int NT) {
+  TcCells v;
+  size_t cc = c->ccap;
+  int* ci = c->cint.p;
+  v.begin = ci; v.nbody = ci + cc; v.nchild = ci + 2 * cc; v.child = ci + 3 * cc; v.parent = ci + 4 * cc;
+  v.level = ci + 5 * cc;
+  double* cd = c->cdbl.p;
+  v.gx = cd; v.gy = cd + cc; v.gz = cd + 2 * cc; v.X = cd + 3 * cc; v.Y = cd + 4 * cc; v.Z = cd + 5 * cc;
+  v.R = cd + 6 * cc;
+  v.has_sink = c->csink.p;
+  size_t ne = (size_t)c->ncell * NT;
+  bool jerk = c->prm.variant == TC_VARIANT_JERKS;
+  v.M = c->expn.p;
+  v.L = c->expn.p ? c->expn.p + ne : nullptr;
+  v.Md = (jerk && c->expn.p) ? c->expn.p + 2 * ne : nullptr;
+  v.Ld = (jerk && c->expn.p) ? c->expn.p + 3 * ne : nullptr;
+  return v;
+}
+
+static TcBodies bodies_view(tc_ctx* c, int n, bool jerk) {
+  TcBodies b;
+  double* d = c->bod.p;
+  size_t N = (size_t)n;
+  b.x = d; b.y = d + N; b.z = d + 2 * N; b.m = d + 3 * N;
+  b.vx = jerk ? d + 4 * N : nullptr; b.vy = jerk ? d + 5 * N : nullptr; b.vz = jerk ? d + 6 * N : nullptr;
+  b.flags = c->bflags.p;
+  b.perm = c->perm.p;
+  return b;
+}
+
+static TcOut out_view(tc_ctx* c, int n, bool jerk) {
+  TcOut o;
+  double* d = c->outs.p;
+  size_t N = (size_t)n;
+  o.pot = d; o.ax = d + N; o.ay = d + 2 * N; o.az = d + 3 * N;
+  o.jx = jerk ? d + 4 * N : nullptr; o.jy = jerk ? d + 5 * N : nullptr; o.jz = jerk ? d + 6 * N : nullptr;
+  return o;
+}
+
+__global__ void k_identity(int n, int* v) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = i;
+}
+
+__global__ void k_nan_check(int n, const double* x, const double* y, const double* z, const double* m, unsigned* err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !(isfinite(x[i]) && isfinite(y[i]) && isfinite(z[i]) && isfinite(m[i]))) tc_set_err(err, TC_EBIT_NAN);
+}
+
+__global__ void k_leaf_list(int ncell, const int* nchild, int* leaves, unsigned* cnt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool has = i < ncell && nchild[i] == 0;
+  unsigned mask = __ballot_sync(0xffffffffu, has);
+  int lane = threadIdx.x & 31;
+  unsigned base = 0;
+  if (lane == 0 && mask) base = atomicAdd(cnt, (unsigned)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (has) leaves[base + __popc(mask & ((1u << lane) - 1u))] = i;
+}
+
+// ----------------------------------------------------------------------------------------
+// per-order evaluation body
+// ----------------------------------------------------------------------------------------
+template <int P, bool JERK>
+static tc_status run_fmm(tc_ctx* ctx, int n) {
+  constexpr int NT = (P + 1) * (P + 1);
+  cudaStream_t st = ctx->stream;
+  const tc_params& prm = ctx->prm;
+  TcBodies b = bodies_view(ctx, n, JERK);
+  ctx->ncell = 0;
+  // ---- tree levels
+  TcCells cv = cells_view(ctx, NT);
+  k_tree_root<<<1, 1, 0, st>>>(n, cv, ctx->d_root, ctx->d_lv);
+  int tgrid = 148 * 8;
+  for (int l = 0; l < TC_MAX_LEVEL + 1; l++) {
+    k_tree_split<<<tgrid, 128, 0, st>>>(l, prm.ncrit, b, cv, ctx->d_lv, ctx->split_off.p, ctx->d_err);
+    k_tree_scan<<<1, 1024, 0, st>>>(l, cv, ctx->d_lv, (int)ctx->ccap, ctx->d_err);
+    k_tree_emit<<<tgrid, 128, 0, st>>>(l, cv, ctx->d_lv, ctx->split_off.p, ctx->d_root);
+  }
+  TC_CK(cudaMemcpyAsync(&ctx->lv, ctx->d_lv, sizeof(TcLevels), cudaMemcpyDeviceToHost, st));
+  unsigned herr = 0;
+  TC_CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  TC_CK(cudaStreamSynchronize(st));
+  if (herr & TC_EBIT_CELL_CAP) return TC_ERR_CAPACITY;
+  ctx->ncell = ctx->lv.ncell;
+  int maxl = 0;
+  for (int l = 0; l <= TC_MAX_LEVEL; l++)
+    if (ctx->lv.count[l] > 0) maxl = l;
+  ctx->max_level = maxl;
+  if (ctx->events) cudaEventRecord(ctx->ev[1], st);
+  // ---- expansions
+  size_t ne = (size_t)ctx->ncell * NT;
+  TC_CK(ctx->expn.ensure(ne * (JERK ? 4 : 2)));
+  cv = cells_view(ctx, NT);
+  TC_CK(cudaMemsetAsync(cv.L, 0, ne * sizeof(double), st));
+  if (JERK) TC_CK(cudaMemsetAsync(cv.Ld, 0, ne * sizeof(double), st));
+  // ---- upward, deepest level first
+  int* d_start = &((TcLevels*)ctx->d_lv)->start[0];
+  int* d_count = &((TcLevels*)ctx->d_lv)->count[0];
+  for (int l = maxl; l >= 0; l--) {
+    int cnt = ctx->lv.count[l];
+    int g = nblocks(cnt, kUpWarps);
+    if (g > 148 * 16) g = 148 * 16;
+    k_upward_level<P, JERK><<<g, kUpWarps * 32, 0, st>>>(l, b, cv, d_start, d_count, ctx->d_err);
+  }
+  if (ctx->events) cudaEventRecord(ctx->ev[2], st);
+  // ---- traversal
+  int sbits = 1;
+  while ((1 << sbits) < ctx->ncell) sbits++;
+  ctx->sbits = sbits;
+  double theta2 = prm.theta * prm.theta;
+  for (int attempt = 0; attempt < 6; attempt++) {
+    size_t want_m = ctx->mcap ? ctx->mcap : (size_t)ctx->ncell * 640 + 65536;
+    size_t want_p = ctx->pcap ? ctx->pcap : (size_t)ctx->ncell * 240 + 65536;
+    size_t want_f = ctx->fcap ? ctx->fcap : (size_t)ctx->ncell * 256 + 65536;
+    TC_CK(ctx->front[0].ensure(want_f));
+    TC_CK(ctx->front[1].ensure(want_f));
+    TC_CK(ctx->m2l.ensure(want_m));
+    TC_CK(ctx->p2p.ensure(want_p));
+    ctx->mcap = ctx->m2l.n;
+    ctx->pcap = ctx->p2p.n;
+    ctx->fcap = ctx->front[0].n < ctx->front[1].n ? ctx->front[0].n : ctx->front[1].n;
+    TC_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
+    k_trav_init<<<1, 1, 0, st>>>(ctx->front[0].p, ctx->d_cnt);
+    int nsteps = 2 * (maxl + 1) + 2;
+    for (int s = 0; s < nsteps; s++)
+      k_trav_step<<<148 * 8, 256, 0, st>>>(s, ctx->front[s & 1].p, ctx->front[(s + 1) & 1].p, ctx->fcap, ctx->d_cnt,
+                                           cv, theta2, prm.variant == TC_VARIANT_TOP, sbits, ctx->m2l.p, ctx->mcap,
+                                           ctx->p2p.p, ctx->pcap, ctx->d_err);
+    TcTravCounters hc;
+    TC_CK(cudaMemcpyAsync(&hc, ctx->d_cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    TC_CK(cudaStreamSynchronize(st));
+    bool grow = false;
+    if (herr & TC_EBIT_M2L_CAP) { ctx->mcap = (size_t)(hc.n_m2l * 1.25) + 4096; grow = true; }
+    if (herr & TC_EBIT_P2P_CAP) { ctx->pcap = (size_t)(hc.n_p2p * 1.25) + 4096; grow = true; }
+    if (herr & TC_EBIT_FRONTIER_CAP) { ctx->fcap = ctx->fcap * 4; grow = true; }
+    unsigned long long left = hc.frontier[nsteps % 3];
+    if (left != 0) { ctx->err = "traversal did not finish"; return TC_ERR_CAPACITY; }
+    if (!grow) {
+      ctx->n_m2l = hc.n_m2l;
+      ctx->n_p2p = hc.n_p2p;
+      break;
+    }
+    if (attempt == 5) return TC_ERR_CAPACITY;
+  }
+  // ---- sort lists and build per-target offsets
+  int kbits = 2 * sbits;
+  {
+    size_t nm = ctx->n_m2l, np = ctx->n_p2p;
+    size_t hist_need = 256 * ((((nm > np ? nm : np) > (size_t)n ? (nm > np ? nm : np) : (size_t)n) + kRsTile - 1) / kRsTile + 1);
+    TC_CK(ctx->hist.ensure(hist_need));
+    TC_CK(ctx->m2l_alt.ensure(nm + 1));
+    TC_CK(ctx->p2p_alt.ensure(np + 1));
+    radix_sort(ctx->m2l.p, nullptr, ctx->m2l_alt.p, nullptr, (int)nm, kbits, ctx->hist.p, st);
+    radix_sort(ctx->p2p.p, nullptr, ctx->p2p_alt.p, nullptr, (int)np, kbits, ctx->hist.p, st);
+    TC_CK(ctx->m2l_start.ensure(ctx->ncell + 1));
+    TC_CK(ctx->p2p_start.ensure(ctx->ncell + 1));
+    TC_CK(ctx->m2l_src.ensure(nm + 1));
+    TC_CK(ctx->p2p_src.ensure(np + 1));
+    TC_CK(ctx->m2l_tl.ensure(ctx->ncell));
+    TC_CK(ctx->p2p_tl.ensure(ctx->ncell));
+    TC_CK(ctx->leaves.ensure(ctx->ncell));
+    k_list_csr<<<148 * 8, 256, 0, st>>>(ctx->m2l.p, nm, ctx->ncell, sbits, ctx->m2l_start.p, ctx->m2l_src.p);
+    k_list_csr<<<148 * 8, 256, 0, st>>>(ctx->p2p.p, np, ctx->ncell, sbits, ctx->p2p_start.p, ctx->p2p_src.p);
+    TC_CK(cudaMemsetAsync(ctx->d_small, 0, 4 * sizeof(unsigned), st));
+    k_list_targets<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->m2l_start.p, ctx->ncell, ctx->m2l_tl.p, ctx->d_small);
+    k_list_targets<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->p2p_start.p, ctx->ncell, ctx->p2p_tl.p, ctx->d_small + 1);
+    k_leaf_list<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->ncell, cv.nchild, ctx->leaves.p, ctx->d_small + 2);
+  }
+  unsigned hs[4];
+  TC_CK(cudaMemcpyAsync(hs, ctx->d_small, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  TC_CK(cudaStreamSynchronize(st));
+  ctx->nleaf = (int)hs[2];
+  if (ctx->events) cudaEventRecord(ctx->ev[3], st);
+  // ---- far field and near field
+  TcOut o = out_view(ctx, n, JERK);
+  TC_CK(cudaMemsetAsync(ctx->outs.p, 0, sizeof(double) * (size_t)n * (JERK ? 7 : 4), st));
+  if (hs[0] > 0) {
+    size_t smem = (size_t)NT * 32 * sizeof(double);
+    k_m2l<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
+                                                                ctx->m2l_src.p, cv);
+  }
+  if (ctx->events) cudaEventRecord(ctx->ev[4], st);
+  if (hs[1] > 0) {
+    int g = nblocks(hs[1], kP2PWarps);
+    k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o);
+  }
+  if (ctx->events) cudaEventRecord(ctx->ev[5], st);
+  // ---- downward
+  for (int l = 1; l <= maxl; l++) {
+    int cnt = ctx->lv.count[l];
+    int g = nblocks(cnt, kUpWarps);
+    if (g > 148 * 16) g = 148 * 16;
+    k_l2l_level<P, JERK><<<g, kUpWarps * 32, 0, st>>>(l, cv, d_start, d_count);
+  }
+  if (ctx->nleaf > 0) {
+    int g = nblocks(ctx->nleaf, kUpWarps);
+    if (g > 148 * 32) g = 148 * 32;
+    k_l2p<P, JERK><<<g, kUpWarps * 32, 0, st>>>(ctx->leaves.p, ctx->nleaf, b, cv, o);
+  }
+  if (ctx->events) cudaEventRecord(ctx->ev[6], st);
+  return TC_OK;
+}
+
+typedef tc_status (*run_fn)(tc_ctx*, int);
+
+template <int P>
+static void set_m2l_attrs() {
+  size_t smem = (size_t)TC_NTERM(P) * 32 * sizeof(double);
+  cudaFuncSetAttribute(k_m2l<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_m2l<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+#define TC_ORDERS(X) X(4) X(6) X(8) X(10) X(12) X(16)
+
+static run_fn pick(int p, bool jerk) {
+  switch (p) {
+#define TC_CASE(P) \
+  case P:          \
+    return jerk ? run_fmm<P, true> : run_fmm<P, false>;
+    TC_ORDERS(TC_CASE)
+#undef TC_CASE
+    default:
+      return nullptr;
+  }
+}
+
+static void set_attrs(int p) {
+  switch (p) {
+#define TC_CASE(P) \
+  case P:          \
+    set_m2l_attrs<P>(); \
+    break;
+    TC_ORDERS(TC_CASE)
+#undef TC_CASE
+    default:
+      break;
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// C ABI
+// ----------------------------------------------------------------------------------------
+extern "C" {
+
+void tc_default_params(tc_params* prm) {
+  memset(prm, 0, sizeof(*prm));
+  prm->p = 12;
+  prm->ncrit = 64;
+  prm->theta = 0.4;
+  prm->variant = TC_VARIANT_JERKS;
+  prm->precision = TC_PREC_FP64;
+  prm->direct_below = -1;
+  prm->device = 0;
+}
+
+int tc_pmax(void) { return TC_PMAX; }
+
+int tc_order_supported(int p) { return pick(p, false) != nullptr; }
+
+const char* tc_status_string(tc_status s) {
+  switch (s) {
+    case TC_OK: return "ok";
+    case TC_ERR_ARG: return "invalid argument";
+    case TC_ERR_CUDA: return "CUDA error";
+    case TC_ERR_CAPACITY: return "capacity exceeded";
+    case TC_ERR_NAN_INPUT: return "non-finite position or mass";
+    case TC_ERR_DEPTH: return "tree depth limit reached";
+    case TC_ERR_UNSUPPORTED: return "unsupported option";
+  }
+  return "unknown status";
+}
+
+const char* tc_last_error_string(tc_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+tc_status tc_create(const tc_params* prm, tc_ctx** out) {
+  if (!prm || !out) return TC_ERR_ARG;
+  *out = nullptr;
+  if (prm->p < 1 || prm->p > TC_PMAX || !tc_order_supported(prm->p)) return TC_ERR_UNSUPPORTED;
+  if (prm->ncrit < 1 || !(prm->theta > 0.0) || (prm->variant != TC_VARIANT_TOP && prm->variant != TC_VARIANT_JERKS))
+    return TC_ERR_ARG;
+  if (prm->precision != TC_PREC_FP64 && prm->precision != TC_PREC_MIXED) return TC_ERR_ARG;
+  tc_ctx* ctx = new tc_ctx();
+  ctx->prm = *prm;
+  memset(&ctx->stats, 0, sizeof(ctx->stats));
+  cudaError_t e = cudaSetDevice(prm->device);
+  if (e == cudaSuccess) e = init_constants(prm->device);
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_root, sizeof(TcRootInfo));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_lv, sizeof(TcLevels));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_cnt, sizeof(TcTravCounters));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_err, sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_small, 4 * sizeof(unsigned));
+  if (e == cudaSuccess) {
+    for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
+    ctx->events = e == cudaSuccess;
+  }
+  if (e != cudaSuccess) {
+    tc_destroy(ctx);
+    return TC_ERR_CUDA;
+  }
+  set_attrs(prm->p);
+  *out = ctx;
+  return TC_OK;
+}
+
+tc_status tc_destroy(tc_ctx* ctx) {
+  if (!ctx) return TC_ERR_ARG;
+  cudaSetDevice(ctx->prm.device);
+  ctx->in_d.release(); ctx->in_f.release(); ctx->out_d.release();
+  ctx->keys.release(); ctx->keys_alt.release(); ctx->vals.release(); ctx->vals_alt.release(); ctx->hist.release();
+  ctx->bod.release(); ctx->bflags.release(); ctx->perm.release(); ctx->outs.release();
+  ctx->cint.release(); ctx->cdbl.release(); ctx->csink.release(); ctx->split_off.release(); ctx->expn.release();
+  ctx->front[0].release(); ctx->front[1].release();
+  ctx->m2l.release(); ctx->m2l_alt.release(); ctx->p2p.release(); ctx->p2p_alt.release();
+  ctx->m2l_start.release(); ctx->m2l_src.release(); ctx->p2p_start.release(); ctx->p2p_src.release();
+  ctx->m2l_tl.release(); ctx->p2p_tl.release(); ctx->leaves.release(); ctx->bpart.release();
+  if (ctx->d_root) cudaFree(ctx->d_root);
+  if (ctx->d_lv) cudaFree(ctx->d_lv);
+  if (ctx->d_cnt) cudaFree(ctx->d_cnt);
+  if (ctx->d_err) cudaFree(ctx->d_err);
+  if (ctx->d_small) cudaFree(ctx->d_small);
+  if (ctx->events)
+    for (int i = 0; i < 8; i++) cudaEventDestroy(ctx->ev[i]);
+  delete ctx;
+  return TC_OK;
+}
+
+tc_status tc_set_stream(tc_ctx* ctx, void* stream) {
+  if (!ctx) return TC_ERR_ARG;
+  ctx->stream = (cudaStream_t)stream;
+  return TC_OK;
+}
+
+tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
+                      const double* vy, const double* vz, const double* m, const unsigned char* flags, double* ax,
+                      double* ay, double* az, double* pot, double* jx, double* jy, double* jz, int mem) {
+  if (!ctx || n <= 0 || !x || !y || !z || !m || !ax || !ay || !az || !pot) return TC_ERR_ARG;
+  const bool jerk = ctx->prm.variant == TC_VARIANT_JERKS;
+  if (jerk && (!vx || !vy || !vz)) return TC_ERR_ARG;
+  if (mem != TC_MEM_HOST && mem != TC_MEM_DEVICE) return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  cudaStream_t st = ctx->stream;
+  ctx->n = n;
+  size_t N = (size_t)n;
+  if (ctx->events) cudaEventRecord(ctx->ev[0], st);
+  // ---- inputs on the device
+  const double *dx = x, *dy = y, *dz = z, *dm = m, *dvx = vx, *dvy = vy, *dvz = vz;
+  const uint8_t* df = flags;
+  if (mem == TC_MEM_HOST) {
+    TC_CK(ctx->in_d.ensure(7 * N));
+    double* s = ctx->in_d.p;
+    const double* src[7] = {x, y, z, m, vx, vy, vz};
+    for (int a = 0; a < 7; a++) {
+      if (!src[a]) continue;
+      TC_CK(cudaMemcpyAsync(s + a * N, src[a], N * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    dx = s; dy = s + N; dz = s + 2 * N; dm = s + 3 * N;
+    dvx = vx ? s + 4 * N : nullptr; dvy = vy ? s + 5 * N : nullptr; dvz = vz ? s + 6 * N : nullptr;
+    if (flags) {
+      TC_CK(ctx->in_f.ensure(N));
+      TC_CK(cudaMemcpyAsync(ctx->in_f.p, flags, N, cudaMemcpyHostToDevice, st));
+      df = ctx->in_f.p;
+    }
+  }
+  // ---- buffers sized by N
+  TC_CK(ctx->keys.ensure(N)); TC_CK(ctx->keys_alt.ensure(N));
+  TC_CK(ctx->vals.ensure(N)); TC_CK(ctx->vals_alt.ensure(N));
+  TC_CK(ctx->bod.ensure(7 * N)); TC_CK(ctx->bflags.ensure(N)); TC_CK(ctx->perm.ensure(N));
+  TC_CK(ctx->outs.ensure(7 * N));
+  TC_CK(ctx->hist.ensure(256 * ((N + kRsTile - 1) / kRsTile + 1)));
+  TC_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
+  int direct_below = ctx->prm.direct_below;
+  if (direct_below < 0) direct_below = jerk ? 8000 : ctx->prm.ncrit;
+  ctx->direct = n < direct_below;
+  TcBodies b = bodies_view(ctx, n, jerk);
+  TcOut o = out_view(ctx, n, jerk);
+  tc_status rs = TC_OK;
+  if (ctx->direct) {
+    k_nan_check<<<nblocks(n, 256), 256, 0, st>>>(n, dx, dy, dz, dm, ctx->d_err);
+    k_identity<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->vals.p);
+    k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->vals.p, dx, dy, dz, dm, dvx, dvy, dvz, df, b);
+    if (jerk)
+      k_direct<true><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
+    else
+      k_direct<false><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
+    ctx->ncell = 0; ctx->nleaf = 0; ctx->n_m2l = 0; ctx->n_p2p = 0; ctx->max_level = 0;
+    if (ctx->events)
+      for (int i = 1; i <= 6; i++) cudaEventRecord(ctx->ev[i], st);
+  } else {
+    for (int attempt = 0; attempt < 4; attempt++) {
+      size_t want_c = ctx->ccap ? ctx->ccap : (size_t)(2 * N / (size_t)(ctx->prm.ncrit > 8 ? 8 : ctx->prm.ncrit) + 1024);
+      if (want_c > 2 * N + 1024) want_c = 2 * N + 1024;
+      if (ctx->ccap < want_c || !ctx->cint.p) {
+        TC_CK(ctx->cint.ensure(6 * want_c));
+        TC_CK(ctx->cdbl.ensure(7 * want_c));
+        TC_CK(ctx->csink.ensure(want_c));
+        TC_CK(ctx->split_off.ensure(8 * want_c));
+        ctx->ccap = want_c;
+      }
+      int nb = 148 * 4;
+      TC_CK(ctx->bpart.ensure(6 * nb));
+      k_bounds_partial<<<nb, 256, 0, st>>>(n, dx, dy, dz, dm, ctx->bpart.p, ctx->d_err);
+      k_bounds_final<<<1, 1, 0, st>>>(nb, ctx->bpart.p, ctx->d_root, ctx->prm.use_shift, ctx->prm.shift_u[0],
+                                      ctx->prm.shift_u[1], ctx->prm.shift_u[2]);
+      k_morton<<<nblocks(n, 256), 256, 0, st>>>(n, dx, dy, dz, ctx->d_root, ctx->keys.p, ctx->vals.p);
+      radix_sort(ctx->keys.p, ctx->vals.p, ctx->keys_alt.p, ctx->vals_alt.p, n, 63, ctx->hist.p, st);
+      k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->vals.p, dx, dy, dz, dm, dvx, dvy, dvz, df, b);
+      run_fn f = pick(ctx->prm.p, jerk);
+      if (!f) return TC_ERR_UNSUPPORTED;
+      rs = f(ctx, n);
+      if (rs == TC_ERR_CAPACITY && ctx->ncell == 0) {
+        ctx->ccap = 2 * ctx->ccap + 1024;
+        continue;
+      }
+      break;
+    }
+    if (rs != TC_OK) return rs;
+  }
+  // ---- outputs to the caller's order
+  double *opot = pot, *oax = ax, *oay = ay, *oaz = az, *ojx = jx, *ojy = jy, *ojz = jz;
+  if (mem == TC_MEM_HOST) {
+    TC_CK(ctx->out_d.ensure(7 * N));
+    double* s = ctx->out_d.p;
+    opot = s; oax = s + N; oay = s + 2 * N; oaz = s + 3 * N;
+    ojx = jx ? s + 4 * N : nullptr; ojy = jx ? s + 5 * N : nullptr; ojz = jx ? s + 6 * N : nullptr;
+  }
+  k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, o, opot, oax, oay, oaz, ojx, ojy, ojz);
+  if (ctx->events) cudaEventRecord(ctx->ev[7], st);
+  unsigned herr = 0;
+  TC_CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  if (mem == TC_MEM_HOST) {
+    double* s = ctx->out_d.p;
+    double* dst[7] = {pot, ax, ay, az, jx, jy, jz};
+    for (int a = 0; a < 7; a++) {
+      if (!dst[a] || (a >= 4 && !jx)) continue;
+      TC_CK(cudaMemcpyAsync(dst[a], s + a * N, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  TC_CK(cudaStreamSynchronize(st));
+  TC_CK(cudaGetLastError());
+  // ---- statistics
+  tc_stats& S = ctx->stats;
+  S.n_bodies = n;
+  S.n_cells = ctx->ncell;
+  S.n_leaves = ctx->nleaf;
+  S.n_m2l = (long long)ctx->n_m2l;
+  S.n_p2p = (long long)ctx->n_p2p;
+  S.max_level = ctx->max_level;
+  S.n_p2p_inter = -1;
+  if (ctx->events) {
+    float t[8];
+    for (int i = 1; i < 8; i++) cudaEventElapsedTime(&t[i], ctx->ev[i - 1], ctx->ev[i]);
+    cudaEventElapsedTime(&t[0], ctx->ev[0], ctx->ev[7]);
+    S.ms_total = t[0]; S.ms_tree = t[1]; S.ms_upward = t[2]; S.ms_traverse = t[3]; S.ms_m2l = t[4];
+    S.ms_p2p = t[5]; S.ms_downward = t[6];
+  }
+  if (herr & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
+  if (herr & TC_EBIT_DEPTH) return TC_ERR_DEPTH;
+  return TC_OK;
+}
+
+tc_status tc_get_stats(tc_ctx* ctx, tc_stats* st) {
+  if (!ctx || !st) return TC_ERR_ARG;
+  *st = ctx->stats;
+  return TC_OK;
+}
+
+tc_status tc_get_cells(tc_ctx* ctx, int* begin, int* nbody, int* nchild, int* child, int* level, double* X,
+                       double* R, int* perm) {
+  if (!ctx) return TC_ERR_ARG;
+  int nc = ctx->ncell;
+  size_t cc = ctx->ccap;
+  if (nc > 0) {
+    int* ci = ctx->cint.p;
+    int* dsts[5] = {begin, nbody, nchild, child, level};
+    int offs[5] = {0, 1, 2, 3, 5};
+    for (int a = 0; a < 5; a++)
+      if (dsts[a]) TC_CK(cudaMemcpy(dsts[a], ci + offs[a] * cc, nc * sizeof(int), cudaMemcpyDeviceToHost));
+    if (X) {
+      std::vector<double> t(nc);
+      for (int d = 0; d < 3; d++) {
+        TC_CK(cudaMemcpy(t.data(), ctx->cdbl.p + (3 + d) * cc, nc * sizeof(double), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < nc; i++) X[3 * i + d] = t[i];
+      }
+    }
+    if (R) TC_CK(cudaMemcpy(R, ctx->cdbl.p + 6 * cc, nc * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  if (perm) TC_CK(cudaMemcpy(perm, ctx->perm.p, ctx->n * sizeof(int), cudaMemcpyDeviceToHost));
+  return TC_OK;
+}
+
+tc_status tc_get_lists(tc_ctx* ctx, int kind, int* tgt, int* src) {
+  if (!ctx || (kind != 0 && kind != 1)) return TC_ERR_ARG;
+  unsigned long long cnt = kind ? ctx->n_p2p : ctx->n_m2l;
+  if (!cnt) return TC_OK;
+  std::vector<unsigned long long> k(cnt);
+  TC_CK(cudaMemcpy(k.data(), kind ? ctx->p2p.p : ctx->m2l.p, cnt * sizeof(unsigned long long),
+                   cudaMemcpyDeviceToHost));
+  unsigned long long mask = (1ull << ctx->sbits) - 1ull;
+  for (unsigned long long i = 0; i < cnt; i++) {
+    if (tgt) tgt[i] = (int)(k[i] >> ctx->sbits);
+    if (src) src[i] = (int)(k[i] & mask);
+  }
+  return TC_OK;
+}
+
+tc_status tc_get_expansions(tc_ctx* ctx, double* M, double* Md, double* L, double* Ld) {
+  if (!ctx) return TC_ERR_ARG;
+  int NT = TC_NTERM(ctx->prm.p);
+  size_t ne = (size_t)ctx->ncell * NT;
+  if (!ne) return TC_OK;
+  TcCells cv = cells_view(ctx, NT);
+  if (M) TC_CK(cudaMemcpy(M, cv.M, ne * sizeof(double), cudaMemcpyDeviceToHost));
+  if (L) TC_CK(cudaMemcpy(L, cv.L, ne * sizeof(double), cudaMemcpyDeviceToHost));
+  if (Md && cv.Md) TC_CK(cudaMemcpy(Md, cv.Md, ne * sizeof(double), cudaMemcpyDeviceToHost));
+  if (Ld && cv.Ld) TC_CK(cudaMemcpy(Ld, cv.Ld, ne * sizeof(double), cudaMemcpyDeviceToHost));
+  return TC_OK;
+}
+
+}  // extern "C"

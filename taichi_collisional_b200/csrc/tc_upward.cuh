@@ -1,0 +1,368 @@
+// Upward pass on the device, one warp per cell, one launch per tree level (deepest first).
+// Restates upwardPass (traverse_eager.h:9-34) with MINIBALL: each cell's expansion centre
+// and radius are the smallest ball enclosing its bodies (leaf, kernel_fast_lean.h:707-737)
+// or, for an inner cell, the bodies of its leaf children plus 64 t-design points around
+// every grandchild (:833-892); R = r_ball + 1e-6.  Then P2M (:745-781) for leaves and M2M
+// (:900-938) for inner cells; with jerks also Mdot (taichi_with_jerks/kernel_fast_lean.h:
+// 769-817, :950-998).
+#pragma once
+#include "tc_harmonics.cuh"
+
+namespace tc {
+
+// ---------------------------------------------------------------------------------------
+// smallest enclosing ball: pivoting (farthest point, warp-parallel) + exact small solver
+// ---------------------------------------------------------------------------------------
+struct TcPointSet {
+  // children of an inner cell: leaf children give bodies, inner children give 64 points
+  // per grandchild.  For a leaf cell: its own bodies.
+  int leaf, nseg;
+  int seg_start[9];   // prefix of point counts
+  int seg_kind[8];    // 0 = bodies [seg_a, seg_a + count), 1 = t-design around cells [seg_a ..)
+  int seg_a[8];
+  int total;
+};
+
+__device__ __forceinline__ void tc_point(const TcPointSet& ps, int idx, const TcBodies& b, const TcCells& c,
+                                         double* p) {
+  if (ps.leaf) {
+    int i = ps.seg_a[0] + idx;
+    p[0] = b.x[i]; p[1] = b.y[i]; p[2] = b.z[i];
+    return;
+  }
+  int s = 0;
+  while (idx >= ps.seg_start[s + 1]) s++;
+  int loc = idx - ps.seg_start[s];
+  if (ps.seg_kind[s] == 0) {
+    int i = ps.seg_a[s] + loc;
+    p[0] = b.x[i]; p[1] = b.y[i]; p[2] = b.z[i];
+  } else {
+    int g = ps.seg_a[s] + (loc >> 6), k = loc & 63;
+    double R = c.R[g];
+    p[0] = c.X[g] + R * c_tdesign[3 * k];
+    p[1] = c.Y[g] + R * c_tdesign[3 * k + 1];
+    p[2] = c.Z[g] + R * c_tdesign[3 * k + 2];
+  }
+}
+
+__device__ __forceinline__ double tc_d2(const double* a, const double* b) {
+  double x = a[0] - b[0], y = a[1] - b[1], z = a[2] - b[2];
+  return x * x + y * y + z * z;
+}
+
+// ball through q[0..k-1] with centre in their affine hull; false if degenerate
+__device__ bool tc_circumsphere(int k, const double (*q)[3], double* c, double* r2) {
+  if (k == 1) {
+    c[0] = q[0][0]; c[1] = q[0][1]; c[2] = q[0][2];
+    *r2 = 0;
+    return true;
+  }
+  double v[3][3], A[3][3], bb[3], lam[3];
+  int d = k - 1;
+  for (int i = 0; i < d; i++)
+    for (int j = 0; j < 3; j++) v[i][j] = q[i + 1][j] - q[0][j];
+  for (int i = 0; i < d; i++) {
+    for (int j = 0; j < d; j++) A[i][j] = 2 * (v[i][0] * v[j][0] + v[i][1] * v[j][1] + v[i][2] * v[j][2]);
+    bb[i] = v[i][0] * v[i][0] + v[i][1] * v[i][1] + v[i][2] * v[i][2];
+  }
+  double scale = 0;
+  for (int i = 0; i < d; i++) scale = fmax(scale, fabs(A[i][i]));
+  for (int col = 0; col < d; col++) {
+    int piv = col;
+    for (int r = col + 1; r < d; r++)
+      if (fabs(A[r][col]) > fabs(A[piv][col])) piv = r;
+    if (fabs(A[piv][col]) <= 1e-13 * scale) return false;
+    if (piv != col) {
+      for (int j = 0; j < d; j++) { double t = A[col][j]; A[col][j] = A[piv][j]; A[piv][j] = t; }
+      double t = bb[col]; bb[col] = bb[piv]; bb[piv] = t;
+    }
+    for (int r = col + 1; r < d; r++) {
+      double f = A[r][col] / A[col][col];
+      for (int j = col; j < d; j++) A[r][j] -= f * A[col][j];
+      bb[r] -= f * bb[col];
+    }
+  }
+  for (int i = d - 1; i >= 0; i--) {
+    double s = bb[i];
+    for (int j = i + 1; j < d; j++) s -= A[i][j] * lam[j];
+    lam[i] = s / A[i][i];
+  }
+  double off[3] = {0, 0, 0};
+  for (int i = 0; i < d; i++)
+    for (int j = 0; j < 3; j++) off[j] += lam[i] * v[i][j];
+  for (int j = 0; j < 3; j++) c[j] = q[0][j] + off[j];
+  *r2 = off[0] * off[0] + off[1] * off[1] + off[2] * off[2];
+  return true;
+}
+
+// smallest ball with q on its boundary enclosing the support set s; updates s
+__device__ bool tc_mb_small(double (*s)[3], int& ns, const double* q, double* c, double* r2) {
+  int best = -1;
+  double bc[3] = {0, 0, 0}, br2 = INFINITY;
+  for (int mask = 0; mask < (1 << ns); mask++) {
+    if (__popc(mask) > 3) continue;
+    double pts[4][3];
+    int k = 0;
+    pts[k][0] = q[0]; pts[k][1] = q[1]; pts[k][2] = q[2]; k++;
+    for (int i = 0; i < ns; i++)
+      if (mask & (1 << i)) { pts[k][0] = s[i][0]; pts[k][1] = s[i][1]; pts[k][2] = s[i][2]; k++; }
+    double cc[3], rr;
+    if (!tc_circumsphere(k, pts, cc, &rr)) continue;
+    if (rr >= br2) continue;
+    bool ok = true;
+    for (int i = 0; i < ns && ok; i++)
+      if (!(mask & (1 << i)) && tc_d2(s[i], cc) > rr * (1 + 1e-13) + 1e-300) ok = false;
+    if (ok) { br2 = rr; bc[0] = cc[0]; bc[1] = cc[1]; bc[2] = cc[2]; best = mask; }
+  }
+  if (best < 0) return false;
+  double nsv[4][3];
+  int k = 0;
+  nsv[k][0] = q[0]; nsv[k][1] = q[1]; nsv[k][2] = q[2]; k++;
+  for (int i = 0; i < ns; i++)
+    if (best & (1 << i)) { nsv[k][0] = s[i][0]; nsv[k][1] = s[i][1]; nsv[k][2] = s[i][2]; k++; }
+  for (int i = 0; i < k; i++) { s[i][0] = nsv[i][0]; s[i][1] = nsv[i][1]; s[i][2] = nsv[i][2]; }
+  ns = k;
+  c[0] = bc[0]; c[1] = bc[1]; c[2] = bc[2];
+  *r2 = br2;
+  return true;
+}
+
+// every lane of the warp ends with the same (c, r2)
+__device__ void tc_warp_miniball(const TcPointSet& ps, const TcBodies& b, const TcCells& cl, double* c, double* r2,
+                                 unsigned int* err) {
+  int lane = threadIdx.x & 31;
+  double s[4][3];
+  int ns = 1;
+  tc_point(ps, 0, b, cl, s[0]);
+  c[0] = s[0][0]; c[1] = s[0][1]; c[2] = s[0][2];
+  *r2 = 0;
+  for (int it = 0; it < 256; it++) {
+    double best_e = 0;
+    int best_i = 0x7fffffff;
+    for (int i = lane; i < ps.total; i += 32) {
+      double p[3];
+      tc_point(ps, i, b, cl, p);
+      double e = tc_d2(p, c) - *r2;
+      if (e > best_e) { best_e = e; best_i = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      double oe = __shfl_xor_sync(0xffffffffu, best_e, o);
+      int oi = __shfl_xor_sync(0xffffffffu, best_i, o);
+      if (oe > best_e || (oe == best_e && oi < best_i)) { best_e = oe; best_i = oi; }
+    }
+    if (best_i == 0x7fffffff || best_e <= *r2 * 1e-15) return;
+    double q[3];
+    tc_point(ps, best_i, b, cl, q);
+    if (!tc_mb_small(s, ns, q, c, r2)) break;
+  }
+  // not converged: grow the ball to enclose every point and flag it
+  double mx = 0;
+  for (int i = lane; i < ps.total; i += 32) {
+    double p[3];
+    tc_point(ps, i, b, cl, p);
+    mx = fmax(mx, tc_d2(p, c));
+  }
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  *r2 = fmax(*r2, mx);
+  if (lane == 0) tc_set_err(err, TC_EBIT_MINIBALL);
+}
+
+// ---------------------------------------------------------------------------------------
+// P2M: lane m accumulates column m of sum_b q_b G(x_b - X) (and of Gdot(v_b) with jerks)
+// ---------------------------------------------------------------------------------------
+template <int P, bool JERK>
+__device__ void tc_p2m_warp(int ci, const TcBodies& b, const TcCells& c) {
+  constexpr int NT = (P + 1) * (P + 1);
+  int lane = threadIdx.x & 31;
+  int beg = c.begin[ci], nb = c.nbody[ci];
+  double X = c.X[ci], Y = c.Y[ci], Z = c.Z[ci];
+  double* M = c.M + (size_t)ci * NT;
+  double* Md = JERK ? c.Md + (size_t)ci * NT : nullptr;
+  if (lane > P) return;
+  const int m = lane;
+  cd acc[P + 1], accd[P + 1];
+#pragma unroll
+  for (int n = 0; n <= P; n++) { acc[n] = mk(0, 0); accd[n] = mk(0, 0); }
+  for (int i = beg; i < beg + nb; i++) {
+    double q = (b.flags[i] & 2) ? b.m[i] : 0.0;
+    double dx = b.x[i] - X, dy = b.y[i] - Y, dz = b.z[i] - Z;
+    double r2 = dx * dx + dy * dy + dz * dz;
+    if (!JERK) {
+      cd d0 = mk(1, 0);
+      for (int j = 1; j <= m; j++) d0 = d0 * mk(dx / (2 * j), dy / (2 * j));
+      TcCol col;
+      col.init(m, d0);
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        cd g = col.step(n, dz, r2);
+        acc[n] += q * g;
+      }
+    } else {
+      double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
+      cd etad = mk(-vx * 0.5, vy * 0.5), zd = mk(vz, 0), ksid = mk(vx * 0.5, vy * 0.5);
+      TcCols3 cols;
+      cols.init(m, dx, dy);
+      cd pa = mk(0, 0), pb = mk(0, 0), pc = mk(0, 0);
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        cd ga, gb, gc;
+        cols.step(n, dz, r2, ga, gb, gc);
+        acc[n] += q * gb;
+        if (n >= 1) {
+          cd gd = mk(0, 0);
+          if (m <= n - 2) gd += pc * etad;
+          if (m <= n - 1) gd += pb * zd;
+          if (n - 1 >= 1 || m >= 1) gd += pa * ksid;  // G[0][-1] reads as zero
+          accd[n] += q * gd;
+        }
+        pa = ga; pb = gb; pc = gc;
+      }
+    }
+  }
+#pragma unroll
+  for (int n = 0; n <= P; n++) {
+    if (n < m) continue;
+    int is = n * n + n;
+    M[is + m] = acc[n].x;
+    if (m > 0) M[is - m] = acc[n].y;
+    if (JERK) {
+      Md[is + m] = accd[n].x;
+      if (m > 0) Md[is - m] = accd[n].y;
+    }
+  }
+}
+
+// G(dX) into shared memory, complex full storage (negative m by symmetry)
+template <int P>
+__device__ __forceinline__ void tc_warp_gnm_smem(double dx, double dy, double dz, cd* G) {
+  int lane = threadIdx.x & 31;
+  double r2 = dx * dx + dy * dy + dz * dz;
+  for (int m = lane; m <= P; m += 32) {
+    cd d0 = mk(1, 0);
+    for (int j = 1; j <= m; j++) d0 = d0 * mk(dx / (2 * j), dy / (2 * j));
+    TcCol col;
+    col.init(m, d0);
+    double s = (m & 1) ? -1.0 : 1.0;
+    for (int n = 0; n <= P; n++) {
+      cd g = col.step(n, dz, r2);
+      if (n < m) continue;
+      G[n * n + n + m] = g;
+      if (m > 0) G[n * n + n - m] = mk(s * g.x, -s * g.y);
+    }
+  }
+  __syncwarp();
+}
+
+// M2M into cell ci from its children (O(p^4) complex translation, kernel_fast_lean.h:921-931)
+template <int P, bool JERK>
+__device__ void tc_m2m_warp(int ci, const TcCells& c, cd* G) {
+  constexpr int NT = (P + 1) * (P + 1);
+  constexpr int NOUT = (P + 1) * (P + 2) / 2;
+  constexpr int PER = (NOUT + 31) / 32;
+  int lane = threadIdx.x & 31;
+  cd acc[PER], accd[PER];
+#pragma unroll
+  for (int k = 0; k < PER; k++) { acc[k] = mk(0, 0); accd[k] = mk(0, 0); }
+  int ch0 = c.child[ci], nch = c.nchild[ci];
+  for (int ch = ch0; ch < ch0 + nch; ch++) {
+    tc_warp_gnm_smem<P>(c.X[ch] - c.X[ci], c.Y[ch] - c.Y[ci], c.Z[ch] - c.Z[ci], G);
+    const double* Mc = c.M + (size_t)ch * NT;
+    const double* Mdc = JERK ? c.Md + (size_t)ch * NT : nullptr;
+#pragma unroll
+    for (int k = 0; k < PER; k++) {
+      int o = lane + 32 * k;
+      if (o >= NOUT) break;
+      int n = 0;
+      while ((n + 1) * (n + 2) / 2 <= o) n++;
+      int m = o - n * (n + 1) / 2;
+      cd s = mk(0, 0), sd = mk(0, 0);
+      for (int kk = 0; kk <= n; kk++) {
+        int lo = max(-kk, m - n + kk), hi = min(kk, m + n - kk);
+        for (int l = lo; l <= hi; l++) {
+          cd g = G[kk * kk + kk + l];
+          s += tc_r2c(Mc, n - kk, m - l) * g;
+          if (JERK) sd += tc_r2c(Mdc, n - kk, m - l) * g;
+        }
+      }
+      acc[k] += s;
+      if (JERK) accd[k] += sd;
+    }
+    __syncwarp();
+  }
+  double* M = c.M + (size_t)ci * NT;
+  double* Md = JERK ? c.Md + (size_t)ci * NT : nullptr;
+#pragma unroll
+  for (int k = 0; k < PER; k++) {
+    int o = lane + 32 * k;
+    if (o >= NOUT) break;
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= o) n++;
+    int m = o - n * (n + 1) / 2;
+    int is = n * n + n;
+    M[is + m] = acc[k].x;
+    if (m > 0) M[is - m] = acc[k].y;
+    if (JERK) {
+      Md[is + m] = accd[k].x;
+      if (m > 0) Md[is - m] = accd[k].y;
+    }
+  }
+}
+
+constexpr int kUpWarps = 4;
+
+template <int P, bool JERK>
+__global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcBodies b, TcCells c,
+                                                                const int* __restrict__ lv_start,
+                                                                const int* __restrict__ lv_count, unsigned int* err) {
+  __shared__ cd sG[kUpWarps][(P + 1) * (P + 1)];
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int cnt = lv_count[l], st = lv_start[l];
+  for (int k = blockIdx.x * kUpWarps + w; k < cnt; k += gridDim.x * kUpWarps) {
+    int ci = st + k;
+    TcPointSet ps;
+    int nch = c.nchild[ci];
+    bool sink = false;
+    if (nch == 0) {
+      ps.leaf = 1;
+      ps.seg_a[0] = c.begin[ci];
+      ps.total = c.nbody[ci];
+      for (int i = c.begin[ci] + lane; i < c.begin[ci] + c.nbody[ci]; i += 32) sink |= (b.flags[i] & 1) != 0;
+    } else {
+      ps.leaf = 0;
+      ps.nseg = nch;
+      int tot = 0;
+      for (int s = 0; s < nch; s++) {
+        int ch = c.child[ci] + s;
+        ps.seg_start[s] = tot;
+        sink |= c.has_sink[ch] != 0;
+        if (c.nchild[ch] == 0) {
+          ps.seg_kind[s] = 0;
+          ps.seg_a[s] = c.begin[ch];
+          tot += c.nbody[ch];
+        } else {
+          ps.seg_kind[s] = 1;
+          ps.seg_a[s] = c.child[ch];
+          tot += 64 * c.nchild[ch];
+        }
+      }
+      ps.seg_start[nch] = tot;
+      ps.total = tot;
+    }
+    sink = __any_sync(0xffffffffu, sink);
+    double cc[3], r2;
+    tc_warp_miniball(ps, b, c, cc, &r2, err);
+    if (lane == 0) {
+      c.X[ci] = cc[0]; c.Y[ci] = cc[1]; c.Z[ci] = cc[2];
+      c.R[ci] = sqrt(r2) + 1e-6;
+      c.has_sink[ci] = sink;
+    }
+    __syncwarp();
+    if (nch == 0)
+      tc_p2m_warp<P, JERK>(ci, b, c);
+    else
+      tc_m2m_warp<P, JERK>(ci, c, sG[w]);
+    __syncwarp();
+  }
+}
+
+}  // namespace tc

@@ -1,0 +1,54 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures from the reference's own code (oracle/_ref).
+
+Run from the repository root, where the reference tree is available and
+``make -C oracle ref`` has built the harness libraries:
+
+    python tests/golden/make_golden.py
+
+Each case stores its inputs, the reference's per-body outputs (single-threaded, so the
+sums are reproducible), the reference's cells (begin, nbody, nchild, child, centre,
+radius) and its M2L / P2P lists as visited by the reference recursion.
+"""
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+from taichi_collisional_b200 import ics  # noqa: E402
+
+CASES = [
+    # name, variant, generator, n, seed, p, theta, ncrit, shift seed
+    ("top_plummer1k_p8", oracle.VARIANT_TOP, "plummer", 1024, 11, 8, 0.5, 32, 0),
+    ("jerks_plummer1k_p8", oracle.VARIANT_JERKS, "plummer", 1024, 12, 8, 0.5, 32, 5),
+    ("jerks_kroupa1500_p10", oracle.VARIANT_JERKS, "plummer_kroupa", 1500, 13, 10, 0.4, 32, 7),
+    ("top_kroupa1500_p12", oracle.VARIANT_TOP, "plummer_kroupa", 1500, 14, 12, 0.4, 24, 0),
+]
+
+
+def main():
+    out_dir = os.path.dirname(os.path.abspath(__file__))
+    for name, variant, gen, n, seed, p, theta, ncrit, sseed in CASES:
+        x, y, z, vx, vy, vz, m = getattr(ics, gen)(n, seed)
+        r = oracle.ref_evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, variant=variant,
+                                seed=sseed, nthreads=1)
+        cells = oracle.ref_cells(variant, p, r["ncell"], n)
+        lists = oracle.ref_lists(variant, p)
+        shift = oracle.ref_shift_uniforms(variant, p, sseed) if variant == oracle.VARIANT_JERKS else np.full(3, np.nan)
+        np.savez_compressed(
+            os.path.join(out_dir, name + ".npz"),
+            variant=variant, p=p, theta=theta, ncrit=ncrit, shift_u=shift,
+            x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m,
+            ax=r["ax"], ay=r["ay"], az=r["az"], pot=r["pot"], jx=r["jx"], jy=r["jy"], jz=r["jz"],
+            cell_begin=cells["begin"], cell_nbody=cells["nbody"], cell_nchild=cells["nchild"],
+            cell_child=cells["child"], cell_X=cells["X"], cell_R=cells["R"], body_index=cells["index"],
+            m2l_t=lists["m2l"][0], m2l_s=lists["m2l"][1], p2p_t=lists["p2p"][0], p2p_s=lists["p2p"][1])
+        print(name, "cells", r["ncell"], "m2l", len(lists["m2l"][0]), "p2p", len(lists["p2p"][0]))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,317 @@
+#!/usr/bin/env python3
+"""Benchmark: particle-steps/s of the FMM gravity step on one B200 (replicas on N GPUs).
+
+Workload (one "step"): FP64 leapfrog kick+drift, one full force evaluation (acceleration,
+potential and jerk; jerks tree, theta-MAC), closing kick -- on a Plummer sphere of
+N = 4,194,304 bodies with Kroupa (2001) masses, p = 12, theta = 0.4, ncrit = 64.  Inputs are
+seeded synthetic data (no dataset is involved) and stay resident in HBM; the state
+(7 x 32 MiB) is larger than L2, so every step streams from HBM.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+N > 1 (torchrun, one process per GPU): independent replicas, no data-path collective; the
+timed region is bracketed by barriers and the slowest rank's device time is reported.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at N=4M, mixed+learned vs FP64 GPU FMM at equal force error"
+UNIT = "particle-steps/s"
+WORKLOAD = {"workload": "plummer_kroupa_N4194304_p12_theta0.4_ncrit64_jerks", "n": 4194304, "p": 12,
+            "theta": 0.4, "ncrit": 64, "tree": "taichi_with_jerks", "step": "kick-drift + force/jerk eval + kick",
+            "l2": "inputs larger than L2 (7 x 32 MiB state)"}
+CPU_SAMPLE_N = 131072
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=WORKLOAD["n"])
+    ap.add_argument("--p", type=int, default=WORKLOAD["p"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_ics(n, seed):
+    from taichi_collisional_b200 import ics
+    return ics.plummer_kroupa(n, seed)
+
+
+# ---------------------------------------------------------------------------------------
+# algorithmic work per unit
+# ---------------------------------------------------------------------------------------
+def m2l_flops_per_pair(p, jerk):
+    """FP64 operations of one rotation M2L (per source array): scaling 2 x NT, 4 phase
+    rotations (12 flops per (n, m>0): complex multiply + next power), 4 swaps (2 per
+    non-zero), z-translation (2 per term) and the accumulation (NT)."""
+    sys.path.insert(0, os.path.join(ROOT, "taichi_collisional_b200", "csrc"))
+    import gen_swap_tables as g
+    mats = g.derive(p)
+    nnz = sum(1 for n in range(p + 1) for row in mats[n] for v in row if v != 0)
+    nt = (p + 1) ** 2
+    rot = 4 * 12 * p * (p + 1) // 2
+    trans = 0
+    for n in range(p + 1):
+        trans += (p - n + 1)
+        for m in range(1, min(n, p - n) + 1):
+            trans += 2 * (p - n - m + 1)
+    per_array = 2 * nt + rot + 4 * 2 * nnz + 2 * trans + nt
+    return per_array * (2 if jerk else 1)
+
+
+P2P_FLOPS = {False: 23, True: 60}
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.f = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+        self.proc = None
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(gpu_index)], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.strip().split(",") for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+# CPU baseline: the reference's own code (oracle/_ref) or the oracle port
+# ---------------------------------------------------------------------------------------
+def cpu_baseline(n_sample, p, theta, ncrit, steps=1, warmup=0):
+    import oracle
+    cores = os.cpu_count() or 1
+    x, y, z, vx, vy, vz, m = make_ics(n_sample, 2026)
+    if oracle.ref_available(oracle.VARIANT_JERKS, p):
+        kind = "reference"
+        os.environ.setdefault("OMP_PROC_BIND", "close")
+
+        def run():
+            oracle.ref_evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, variant=oracle.VARIANT_JERKS,
+                                seed=1, nthreads=cores)
+    else:
+        kind = "port"
+        cores = 1
+
+        def run():
+            oracle.evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, variant=oracle.VARIANT_JERKS,
+                            direct_below=0)
+    for _ in range(warmup):
+        run()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        run()
+    dt = time.perf_counter() - t0
+    sample = ("%d force evaluation(s) (acc+pot+jerk, theta-MAC) of a N=%d Plummer/Kroupa sample, p=%d, theta=%g, "
+              "ncrit=%d; the per-particle cost grows ~log N, so the N=4M rate is lower" %
+              (steps, n_sample, p, theta, ncrit))
+    return {"value": n_sample * steps / dt, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+            "seconds": dt}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    try:
+        cb = cpu_baseline(CPU_SAMPLE_N, args.p, WORKLOAD["theta"], WORKLOAD["ncrit"], steps=args.steps,
+                          warmup=args.warmup)
+    except Exception as e:  # pragma: no cover - reported, not hidden
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build failed: %s" % e}))
+        return
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds"] / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Plummer/Kroupa sample)",
+            "config": dict(WORKLOAD, n_sample=CPU_SAMPLE_N),
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import datetime
+
+    import torch
+    import taichi_collisional_b200 as tcb
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    n, p = args.n, args.p
+    x, y, z, vx, vy, vz, m = make_ics(n, 2026 + rank)
+    T = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)  # noqa: E731
+    st = {k: T(a) for k, a in zip(("x", "y", "z", "vx", "vy", "vz", "m"), (x, y, z, vx, vy, vz, m))}
+    out = {k: torch.empty(n, dtype=torch.float64, device=dev) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
+    g = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
+                    precision=tcb.PREC_FP64 if args.precision == "fp64" else tcb.PREC_MIXED, device=local)
+    dt = 1.0 / 4096
+
+    def evaluate():
+        g.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"], out=out)
+
+    def step():
+        g.kick_drift(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], out["ax"], out["ay"], out["az"],
+                     0.5 * dt, dt)
+        evaluate()
+        g.kick_drift(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], out["ax"], out["ay"], out["az"],
+                     0.5 * dt, 0.0)
+
+    evaluate()
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    phase = {k: 0.0 for k in ("ms_tree", "ms_upward", "ms_traverse", "ms_m2l", "ms_p2p", "ms_downward")}
+    launches = 0
+    e0.record()
+    for _ in range(args.steps):
+        step()
+        s = g.stats()
+        for k in phase:
+            phase[k] += s[k]
+        launches += s["n_launches"] + 2
+    e1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n * args.steps / (ms * 1e-3)
+    stats = g.stats()
+
+    # ---- end to end through the public API: pinned host state in, results out, every step
+    e2e = None
+    if not args.no_e2e:
+        hin = {k: st[k].to("cpu").pin_memory() for k in st}
+        hout = {k: torch.empty(n, dtype=torch.float64).pin_memory() for k in out}
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(args.steps):
+            for k in st:
+                st[k].copy_(hin[k], non_blocking=True)
+            step()
+            for k in out:
+                hout[k].copy_(out[k], non_blocking=True)
+        f1.record()
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1)
+        if dist:
+            t = torch.tensor([ems], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": world * n * args.steps / (ems * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 7 * 8 * n,
+               "d2h_bytes_per_step": 7 * 8 * n, "ms_per_step": ems / args.steps}
+
+    # ---- roofline of the dominant kernel
+    per = {k: v / args.steps for k, v in phase.items()}
+    fp64_peak = g.probe_peak(0) / 1e3  # TFLOP/s, measured FMA throughput of this GPU
+    m2l_flops = stats["n_m2l"] * m2l_flops_per_pair(p, True)
+    p2p_flops = stats["n_p2p_inter"] * P2P_FLOPS[True]
+    kern = {"k_m2l": (per["ms_m2l"], m2l_flops), "k_p2p": (per["ms_p2p"], p2p_flops)}
+    dom = max(kern, key=lambda k: kern[k][0])
+    ach = kern[dom][1] / (kern[dom][0] * 1e-3) / 1e12
+    roof = {"kernel": dom, "bound": "fp64", "achieved": ach, "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": ach / fp64_peak if fp64_peak > 0 else None, "traffic": None,
+            "peak_source": "FP64 FMA throughput measured on this GPU by tc_probe_peak (MEASURED_PEAKS.json has "
+                           "no FP64 figure)",
+            "work": "%s: %.3e flop per launch" % (dom, kern[dom][1]),
+            "phase_ms": {k: round(v, 3) for k, v in per.items()},
+            "other": {k: {"ms": round(v[0], 3), "tflops": round(v[1] / (v[0] * 1e-3) / 1e12, 3) if v[0] else None}
+                      for k, v in kern.items()}}
+
+    cb = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            cb = cpu_baseline(CPU_SAMPLE_N, p, WORKLOAD["theta"], WORKLOAD["ncrit"])
+            cb.pop("seconds", None)
+        except Exception as e:
+            cb = {"value": None, "error": str(e)}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+                "data": "synthetic (seeded Plummer sphere, Kroupa IMF masses)",
+                "config": dict(WORKLOAD, n=n, p=p, precision=args.precision,
+                               parallelism="replicas" if world > 1 else "single"),
+                "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb, "clocks": clocks,
+                "lists": {"cells": stats["n_cells"], "m2l_pairs": stats["n_m2l"], "p2p_pairs": stats["n_p2p"],
+                          "p2p_interactions": stats["n_p2p_inter"], "max_level": stats["max_level"]}}
+        print(json.dumps(line))
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -61,6 +61,7 @@ typedef struct {
   long long n_bodies, n_cells, n_leaves, n_m2l, n_p2p, n_p2p_inter;
   int max_level;
   double ms_total, ms_tree, ms_upward, ms_traverse, ms_m2l, ms_p2p, ms_downward;
+  long long n_launches; /* kernels launched by the last tc_evaluate */
 } tc_stats;
 
 typedef struct tc_ctx tc_ctx;
@@ -100,6 +101,18 @@ tc_status tc_get_cells(tc_ctx* ctx, int* begin, int* nbody, int* nchild, int* ch
                        double* X /* 3 per cell */, double* R, int* perm /* n */);
 tc_status tc_get_lists(tc_ctx* ctx, int kind, int* tgt, int* src);
 tc_status tc_get_expansions(tc_ctx* ctx, double* M, double* Md, double* L, double* Ld);
+
+/* FP64 leapfrog update on device arrays (the integrator step around each evaluation):
+ *   v += a * dt_kick;  x += v * dt_drift
+ * Restates kick (integrator.h:378-457, v += a dt) and drift (integrator.h:642-670,
+ * x += v dt) for a single shared time step; device pointers only, on the context's stream. */
+tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy,
+                        double* vz, const double* ax, const double* ay, const double* az,
+                        double dt_kick, double dt_drift);
+
+/* Measured arithmetic throughput of this GPU in GFLOP/s (kind 0: FP64 FMA, 1: FP32 FMA),
+ * used as the roofline denominator of the FP64 / FP32 kernels.  Returns < 0 on error. */
+double tc_probe_peak(tc_ctx* ctx, int kind);
 
 const char* tc_status_string(tc_status s);
 const char* tc_last_error_string(tc_ctx* ctx);

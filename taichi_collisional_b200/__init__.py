@@ -42,12 +42,12 @@ class Stats(C.Structure):
                 ("n_m2l", C.c_longlong), ("n_p2p", C.c_longlong), ("n_p2p_inter", C.c_longlong),
                 ("max_level", C.c_int), ("ms_total", C.c_double), ("ms_tree", C.c_double),
                 ("ms_upward", C.c_double), ("ms_traverse", C.c_double), ("ms_m2l", C.c_double),
-                ("ms_p2p", C.c_double), ("ms_downward", C.c_double)]
+                ("ms_p2p", C.c_double), ("ms_downward", C.c_double), ("n_launches", C.c_longlong)]
 
 
 EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_evaluate", "tc_get_stats",
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
-           "tc_pmax", "tc_order_supported"]
+           "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak"]
 
 _lib = None
 
@@ -88,6 +88,10 @@ def load_library(path=LIB_PATH):
     L.tc_pmax.restype = C.c_int
     L.tc_order_supported.argtypes = [C.c_int]
     L.tc_order_supported.restype = C.c_int
+    L.tc_kick_drift.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 9 + [C.c_double, C.c_double]
+    L.tc_kick_drift.restype = C.c_int
+    L.tc_probe_peak.argtypes = [C.c_void_p, C.c_int]
+    L.tc_probe_peak.restype = C.c_double
     _lib = L
     return L
 
@@ -179,6 +183,16 @@ class Gravity:
                                  MEM_DEVICE if dev else MEM_HOST)
         self._check(rc, "tc_evaluate")
         return out
+
+    def kick_drift(self, x, y, z, vx, vy, vz, ax, ay, az, dt_kick, dt_drift):
+        """FP64 leapfrog update on CUDA tensors: v += a dt_kick; x += v dt_drift."""
+        rc = self._L.tc_kick_drift(self._h, len(x), *[_ptr(a) for a in (x, y, z, vx, vy, vz, ax, ay, az)],
+                                   float(dt_kick), float(dt_drift))
+        self._check(rc, "tc_kick_drift")
+
+    def probe_peak(self, kind):
+        """Measured FMA throughput of this GPU in GFLOP/s (0: FP64, 1: FP32)."""
+        return self._L.tc_probe_peak(self._h, kind)
 
     def stats(self):
         st = Stats()

@@ -98,6 +98,8 @@ struct tc_ctx {
   int n = 0, ncell = 0, nleaf = 0, max_level = 0, direct = 0;
   unsigned long long n_m2l = 0, n_p2p = 0;
   int sbits = 1;
+  long long launches = 0;
+  unsigned long long n_inter = 0;
   cudaEvent_t ev[8];
   bool events = false;
 };
@@ -199,6 +201,20 @@ __global__ void k_leaf_list(int ncell, const int* nchild, int* leaves, unsigned*
   if (has) leaves[base + __popc(mask & ((1u << lane) - 1u))] = i;
 }
 
+// sum over the P2P list of (sink-cell bodies) x (source-cell bodies)
+__global__ void k_p2p_count(const unsigned long long* __restrict__ keys, unsigned long long n, int sbits,
+                            const int* __restrict__ nbody, const uint8_t* __restrict__ has_sink,
+                            unsigned long long* total) {
+  unsigned long long loc = 0, mask = (1ull << sbits) - 1ull;
+  for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    int t = (int)(keys[k] >> sbits), s = (int)(keys[k] & mask);
+    if (has_sink[t]) loc += (unsigned long long)nbody[t] * (unsigned long long)nbody[s];
+  }
+  for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
+  if ((threadIdx.x & 31) == 0 && loc) atomicAdd(total, loc);
+}
+
 // ----------------------------------------------------------------------------------------
 // per-order evaluation body
 // ----------------------------------------------------------------------------------------
@@ -212,6 +228,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   // ---- tree levels
   TcCells cv = cells_view(ctx, NT);
   k_tree_root<<<1, 1, 0, st>>>(n, cv, ctx->d_root, ctx->d_lv);
+  ctx->launches += 1 + 3 * (TC_MAX_LEVEL + 1);
   int tgrid = 148 * 8;
   for (int l = 0; l < TC_MAX_LEVEL + 1; l++) {
     k_tree_split<<<tgrid, 128, 0, st>>>(l, prm.ncrit, b, cv, ctx->d_lv, ctx->split_off.p, ctx->d_err);
@@ -238,6 +255,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   // ---- upward, deepest level first
   int* d_start = &((TcLevels*)ctx->d_lv)->start[0];
   int* d_count = &((TcLevels*)ctx->d_lv)->count[0];
+  ctx->launches += maxl + 1;
   for (int l = maxl; l >= 0; l--) {
     int cnt = ctx->lv.count[l];
     int g = nblocks(cnt, kUpWarps);
@@ -264,6 +282,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     TC_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
     k_trav_init<<<1, 1, 0, st>>>(ctx->front[0].p, ctx->d_cnt);
     int nsteps = 2 * (maxl + 1) + 2;
+    ctx->launches += 1 + nsteps;
     for (int s = 0; s < nsteps; s++)
       k_trav_step<<<148 * 8, 256, 0, st>>>(s, ctx->front[s & 1].p, ctx->front[(s + 1) & 1].p, ctx->fcap, ctx->d_cnt,
                                            cv, theta2, prm.variant == TC_VARIANT_TOP, sbits, ctx->m2l.p, ctx->mcap,
@@ -295,6 +314,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     TC_CK(ctx->p2p_alt.ensure(np + 1));
     radix_sort(ctx->m2l.p, nullptr, ctx->m2l_alt.p, nullptr, (int)nm, kbits, ctx->hist.p, st);
     radix_sort(ctx->p2p.p, nullptr, ctx->p2p_alt.p, nullptr, (int)np, kbits, ctx->hist.p, st);
+    ctx->launches += (nm > 1 ? 3 * ((kbits + 7) / 8) : 0) + (np > 1 ? 3 * ((kbits + 7) / 8) : 0) + 5;
     TC_CK(ctx->m2l_start.ensure(ctx->ncell + 1));
     TC_CK(ctx->p2p_start.ensure(ctx->ncell + 1));
     TC_CK(ctx->m2l_src.ensure(nm + 1));
@@ -305,12 +325,16 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     k_list_csr<<<148 * 8, 256, 0, st>>>(ctx->m2l.p, nm, ctx->ncell, sbits, ctx->m2l_start.p, ctx->m2l_src.p);
     k_list_csr<<<148 * 8, 256, 0, st>>>(ctx->p2p.p, np, ctx->ncell, sbits, ctx->p2p_start.p, ctx->p2p_src.p);
     TC_CK(cudaMemsetAsync(ctx->d_small, 0, 4 * sizeof(unsigned), st));
+    TC_CK(cudaMemsetAsync(&ctx->d_cnt->frontier[0], 0, sizeof(unsigned long long), st));
+    k_p2p_count<<<148 * 4, 256, 0, st>>>(ctx->p2p.p, np, sbits, cv.nbody, cv.has_sink, &ctx->d_cnt->frontier[0]);
+    ctx->launches++;
     k_list_targets<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->m2l_start.p, ctx->ncell, ctx->m2l_tl.p, ctx->d_small);
     k_list_targets<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->p2p_start.p, ctx->ncell, ctx->p2p_tl.p, ctx->d_small + 1);
     k_leaf_list<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->ncell, cv.nchild, ctx->leaves.p, ctx->d_small + 2);
   }
   unsigned hs[4];
   TC_CK(cudaMemcpyAsync(hs, ctx->d_small, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  TC_CK(cudaMemcpyAsync(&ctx->n_inter, &ctx->d_cnt->frontier[0], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   TC_CK(cudaStreamSynchronize(st));
   ctx->nleaf = (int)hs[2];
   if (ctx->events) cudaEventRecord(ctx->ev[3], st);
@@ -321,14 +345,17 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     size_t smem = (size_t)NT * 32 * sizeof(double);
     k_m2l<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
                                                                 ctx->m2l_src.p, cv);
+    ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[4], st);
   if (hs[1] > 0) {
     int g = nblocks(hs[1], kP2PWarps);
     k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o);
+    ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[5], st);
   // ---- downward
+  ctx->launches += maxl + (ctx->nleaf > 0);
   for (int l = 1; l <= maxl; l++) {
     int cnt = ctx->lv.count[l];
     int g = nblocks(cnt, kUpWarps);
@@ -378,6 +405,32 @@ static void set_attrs(int p) {
     default:
       break;
   }
+}
+
+__global__ void k_kick_drift(int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                             const double* ax, const double* ay, const double* az, double dk, double dd) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double u = vx[i] + ax[i] * dk, v = vy[i] + ay[i] * dk, w = vz[i] + az[i] * dk;
+  vx[i] = u; vy[i] = v; vz[i] = w;
+  if (dd != 0.0) {
+    x[i] += u * dd; y[i] += v * dd; z[i] += w * dd;
+  }
+}
+
+template <typename T>
+__global__ void k_fma_probe(T* out, int iters) {
+  T a0 = (T)threadIdx.x * (T)1e-3, a1 = a0 + (T)1, a2 = a0 + (T)2, a3 = a0 + (T)3;
+  T a4 = a0 + (T)4, a5 = a0 + (T)5, a6 = a0 + (T)6, a7 = a0 + (T)7;
+  const T b = (T)0.999999, c = (T)1e-7;
+  for (int i = 0; i < iters; i++) {
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      a0 = a0 * b + c; a1 = a1 * b + c; a2 = a2 * b + c; a3 = a3 * b + c;
+      a4 = a4 * b + c; a5 = a5 * b + c; a6 = a6 * b + c; a7 = a7 * b + c;
+    }
+  }
+  if (a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7 == (T)-1) out[0] = a0;
 }
 
 // ----------------------------------------------------------------------------------------
@@ -483,6 +536,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   TC_CK(cudaSetDevice(ctx->prm.device));
   cudaStream_t st = ctx->stream;
   ctx->n = n;
+  ctx->launches = 0;
   size_t N = (size_t)n;
   if (ctx->events) cudaEventRecord(ctx->ev[0], st);
   // ---- inputs on the device
@@ -525,6 +579,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
       k_direct<true><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
     else
       k_direct<false><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
+    ctx->launches += 4;
     ctx->ncell = 0; ctx->nleaf = 0; ctx->n_m2l = 0; ctx->n_p2p = 0; ctx->max_level = 0;
     if (ctx->events)
       for (int i = 1; i <= 6; i++) cudaEventRecord(ctx->ev[i], st);
@@ -546,6 +601,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
                                       ctx->prm.shift_u[1], ctx->prm.shift_u[2]);
       k_morton<<<nblocks(n, 256), 256, 0, st>>>(n, dx, dy, dz, ctx->d_root, ctx->keys.p, ctx->vals.p);
       radix_sort(ctx->keys.p, ctx->vals.p, ctx->keys_alt.p, ctx->vals_alt.p, n, 63, ctx->hist.p, st);
+      ctx->launches += 4 + 3 * 8;
       k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->vals.p, dx, dy, dz, dm, dvx, dvy, dvz, df, b);
       run_fn f = pick(ctx->prm.p, jerk);
       if (!f) return TC_ERR_UNSUPPORTED;
@@ -567,6 +623,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
     ojx = jx ? s + 4 * N : nullptr; ojy = jx ? s + 5 * N : nullptr; ojz = jx ? s + 6 * N : nullptr;
   }
   k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, o, opot, oax, oay, oaz, ojx, ojy, ojz);
+  ctx->launches++;
   if (ctx->events) cudaEventRecord(ctx->ev[7], st);
   unsigned herr = 0;
   TC_CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -588,7 +645,8 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   S.n_m2l = (long long)ctx->n_m2l;
   S.n_p2p = (long long)ctx->n_p2p;
   S.max_level = ctx->max_level;
-  S.n_p2p_inter = -1;
+  S.n_p2p_inter = ctx->direct ? (long long)n * n : (long long)ctx->n_inter;
+  S.n_launches = ctx->launches;
   if (ctx->events) {
     float t[8];
     for (int i = 1; i < 8; i++) cudaEventElapsedTime(&t[i], ctx->ev[i - 1], ctx->ev[i]);
@@ -599,6 +657,47 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   if (herr & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
   if (herr & TC_EBIT_DEPTH) return TC_ERR_DEPTH;
   return TC_OK;
+}
+
+tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                        const double* ax, const double* ay, const double* az, double dt_kick, double dt_drift) {
+  if (!ctx || n <= 0 || !x || !y || !z || !vx || !vy || !vz || !ax || !ay || !az) return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, vx, vy, vz, ax, ay, az, dt_kick, dt_drift);
+  TC_CK(cudaGetLastError());
+  return TC_OK;
+}
+
+double tc_probe_peak(tc_ctx* ctx, int kind) {
+  if (!ctx || (kind != 0 && kind != 1)) return -1.0;
+  if (cudaSetDevice(ctx->prm.device) != cudaSuccess) return -1.0;
+  int nsm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->prm.device);
+  void* out = nullptr;
+  if (cudaMalloc(&out, 64) != cudaSuccess) return -1.0;
+  int blocks = nsm * 8, threads = 256, iters = 4096;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  for (int r = 0; r < 4; r++) {
+    cudaEventRecord(e0, ctx->stream);
+    if (kind == 0)
+      k_fma_probe<double><<<blocks, threads, 0, ctx->stream>>>((double*)out, iters);
+    else
+      k_fma_probe<float><<<blocks, threads, 0, ctx->stream>>>((float*)out, iters);
+    cudaEventRecord(e1, ctx->stream);
+    cudaEventSynchronize(e1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (r > 0 && ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (cudaGetLastError() != cudaSuccess) return -1.0;
+  double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+  return flops / (best * 1e-3) / 1e9;
 }
 
 tc_status tc_get_stats(tc_ctx* ctx, tc_stats* st) {

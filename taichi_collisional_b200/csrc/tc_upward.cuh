@@ -23,28 +23,6 @@ struct TcPointSet {
   int total;
 };
 
-__device__ __forceinline__ void tc_point(const TcPointSet& ps, int idx, const TcBodies& b, const TcCells& c,
-                                         double* p) {
-  if (ps.leaf) {
-    int i = ps.seg_a[0] + idx;
-    p[0] = b.x[i]; p[1] = b.y[i]; p[2] = b.z[i];
-    return;
-  }
-  int s = 0;
-  while (idx >= ps.seg_start[s + 1]) s++;
-  int loc = idx - ps.seg_start[s];
-  if (ps.seg_kind[s] == 0) {
-    int i = ps.seg_a[s] + loc;
-    p[0] = b.x[i]; p[1] = b.y[i]; p[2] = b.z[i];
-  } else {
-    int g = ps.seg_a[s] + (loc >> 6), k = loc & 63;
-    double R = c.R[g];
-    p[0] = c.X[g] + R * c_tdesign[3 * k];
-    p[1] = c.Y[g] + R * c_tdesign[3 * k + 1];
-    p[2] = c.Z[g] + R * c_tdesign[3 * k + 2];
-  }
-}
-
 __device__ __forceinline__ double tc_d2(const double* a, const double* b) {
   double x = a[0] - b[0], y = a[1] - b[1], z = a[2] - b[2];
   return x * x + y * y + z * z;
@@ -127,39 +105,99 @@ __device__ bool tc_mb_small(double (*s)[3], int& ns, const double* q, double* c,
   return true;
 }
 
+// Farthest point from c (largest excess e = |p - c|^2 - r2; ties -> lowest point index).
+// Items are bodies or t-design groups (64 points around one grandchild); a group whose
+// bounding sphere cannot beat the best excess found so far is skipped.
+__device__ __forceinline__ void tc_mb_farthest(const TcPointSet& ps, const TcBodies& b, const TcCells& cl,
+                                               const double* td, const double* c, double r2, double& best_e,
+                                               int& best_i) {
+  int lane = threadIdx.x & 31;
+  best_e = 0;
+  best_i = 0x7fffffff;
+  if (ps.leaf) {
+    for (int i = lane; i < ps.total; i += 32) {
+      int bi = ps.seg_a[0] + i;
+      double p[3] = {b.x[bi], b.y[bi], b.z[bi]};
+      double e = tc_d2(p, c) - r2;
+      if (e > best_e) { best_e = e; best_i = i; }
+    }
+  } else {
+    for (int s = 0; s < ps.nseg; s++) {
+      int cnt = ps.seg_kind[s] == 0 ? ps.seg_start[s + 1] - ps.seg_start[s] : (ps.seg_start[s + 1] - ps.seg_start[s]) >> 6;
+      for (int it = lane; it < cnt; it += 32) {
+        if (ps.seg_kind[s] == 0) {
+          int bi = ps.seg_a[s] + it;
+          double p[3] = {b.x[bi], b.y[bi], b.z[bi]};
+          double e = tc_d2(p, c) - r2;
+          if (e > best_e) { best_e = e; best_i = ps.seg_start[s] + it; }
+        } else {
+          int g = ps.seg_a[s] + it;
+          double X = cl.X[g], Y = cl.Y[g], Z = cl.Z[g], R = cl.R[g];
+          double q[3] = {X, Y, Z};
+          double dc = sqrt(tc_d2(q, c)) + R;
+          if (dc * dc * (1.0 + 1e-12) - r2 < best_e) continue;
+          int base = ps.seg_start[s] + (it << 6);
+          for (int k = 0; k < 64; k++) {
+            double p[3] = {X + R * td[3 * k], Y + R * td[3 * k + 1], Z + R * td[3 * k + 2]};
+            double e = tc_d2(p, c) - r2;
+            if (e > best_e) { best_e = e; best_i = base + k; }
+          }
+        }
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    double oe = __shfl_xor_sync(0xffffffffu, best_e, o);
+    int oi = __shfl_xor_sync(0xffffffffu, best_i, o);
+    if (oe > best_e || (oe == best_e && oi < best_i)) { best_e = oe; best_i = oi; }
+  }
+}
+
+__device__ __forceinline__ void tc_point_td(const TcPointSet& ps, int idx, const TcBodies& b, const TcCells& c,
+                                            const double* td, double* p) {
+  if (ps.leaf) {
+    int i = ps.seg_a[0] + idx;
+    p[0] = b.x[i]; p[1] = b.y[i]; p[2] = b.z[i];
+    return;
+  }
+  int s = 0;
+  while (idx >= ps.seg_start[s + 1]) s++;
+  int loc = idx - ps.seg_start[s];
+  if (ps.seg_kind[s] == 0) {
+    int i = ps.seg_a[s] + loc;
+    p[0] = b.x[i]; p[1] = b.y[i]; p[2] = b.z[i];
+  } else {
+    int g = ps.seg_a[s] + (loc >> 6), k = loc & 63;
+    double R = c.R[g];
+    p[0] = c.X[g] + R * td[3 * k];
+    p[1] = c.Y[g] + R * td[3 * k + 1];
+    p[2] = c.Z[g] + R * td[3 * k + 2];
+  }
+}
+
 // every lane of the warp ends with the same (c, r2)
-__device__ void tc_warp_miniball(const TcPointSet& ps, const TcBodies& b, const TcCells& cl, double* c, double* r2,
-                                 unsigned int* err) {
+__device__ void tc_warp_miniball(const TcPointSet& ps, const TcBodies& b, const TcCells& cl, const double* td,
+                                 double* c, double* r2, unsigned int* err) {
   int lane = threadIdx.x & 31;
   double s[4][3];
   int ns = 1;
-  tc_point(ps, 0, b, cl, s[0]);
+  tc_point_td(ps, 0, b, cl, td, s[0]);
   c[0] = s[0][0]; c[1] = s[0][1]; c[2] = s[0][2];
   *r2 = 0;
-  for (int it = 0; it < 256; it++) {
-    double best_e = 0;
-    int best_i = 0x7fffffff;
-    for (int i = lane; i < ps.total; i += 32) {
-      double p[3];
-      tc_point(ps, i, b, cl, p);
-      double e = tc_d2(p, c) - *r2;
-      if (e > best_e) { best_e = e; best_i = i; }
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      double oe = __shfl_xor_sync(0xffffffffu, best_e, o);
-      int oi = __shfl_xor_sync(0xffffffffu, best_i, o);
-      if (oe > best_e || (oe == best_e && oi < best_i)) { best_e = oe; best_i = oi; }
-    }
+  for (int it = 0; it < 512; it++) {
+    double best_e;
+    int best_i;
+    tc_mb_farthest(ps, b, cl, td, c, *r2, best_e, best_i);
     if (best_i == 0x7fffffff || best_e <= *r2 * 1e-15) return;
     double q[3];
-    tc_point(ps, best_i, b, cl, q);
+    tc_point_td(ps, best_i, b, cl, td, q);
     if (!tc_mb_small(s, ns, q, c, r2)) break;
   }
   // not converged: grow the ball to enclose every point and flag it
   double mx = 0;
   for (int i = lane; i < ps.total; i += 32) {
     double p[3];
-    tc_point(ps, i, b, cl, p);
+    tc_point_td(ps, i, b, cl, td, p);
     mx = fmax(mx, tc_d2(p, c));
   }
   for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -315,6 +353,9 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcB
                                                                 const int* __restrict__ lv_start,
                                                                 const int* __restrict__ lv_count, unsigned int* err) {
   __shared__ cd sG[kUpWarps][(P + 1) * (P + 1)];
+  __shared__ double s_td[192];
+  for (int i = threadIdx.x; i < 192; i += blockDim.x) s_td[i] = c_tdesign[i];
+  __syncthreads();
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int cnt = lv_count[l], st = lv_start[l];
   for (int k = blockIdx.x * kUpWarps + w; k < cnt; k += gridDim.x * kUpWarps) {
@@ -350,7 +391,7 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcB
     }
     sink = __any_sync(0xffffffffu, sink);
     double cc[3], r2;
-    tc_warp_miniball(ps, b, c, cc, &r2, err);
+    tc_warp_miniball(ps, b, c, s_td, cc, &r2, err);
     if (lane == 0) {
       c.X[ci] = cc[0]; c.Y[ci] = cc[1]; c.Z[ci] = cc[2];
       c.R[ci] = sqrt(r2) + 1e-6;

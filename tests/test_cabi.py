@@ -1,0 +1,95 @@
+"""The C-ABI library loads and exports every entry point declared in include/taichi_b200.h;
+argument checks that need no GPU; the Python mirror's structures match the header."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import taichi_collisional_b200 as tcb
+from taichi_collisional_b200 import ics
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "taichi_b200.h")
+
+
+def declared_functions():
+    txt = open(HEADER).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_]+\*?\s+\**(tc_[a-z_]+)\s*\(", txt, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = tcb.load_library()
+    names = declared_functions()
+    assert len(names) >= 12
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) == set(tcb.EXPORTS)
+
+
+def test_struct_layouts_match_header():
+    # tc_params: int p, int ncrit, double theta, int variant, int precision, int use_shift,
+    # double shift_u[3], int direct_below, int device
+    assert C.sizeof(tcb.Params) == 4 + 4 + 8 + 4 + 4 + 4 + 4 + 24 + 4 + 4
+    assert tcb.Params.theta.offset == 8
+    assert tcb.Params.shift_u.offset == 32
+
+
+def test_defaults_and_orders():
+    L = tcb.load_library()
+    prm = tcb.default_params()
+    assert (prm.p, prm.ncrit, prm.theta, prm.variant, prm.direct_below) == (12, 64, 0.4, 1, -1)
+    assert L.tc_pmax() == 16
+    for p in (4, 6, 8, 10, 12, 16):
+        assert L.tc_order_supported(p)
+    assert not L.tc_order_supported(0) and not L.tc_order_supported(17)
+    assert L.tc_status_string(3) == b"capacity exceeded"
+
+
+def test_create_rejects_bad_params_without_touching_the_gpu():
+    L = tcb.load_library()
+    h = C.c_void_p()
+    for bad in (dict(p=0), dict(p=17), dict(ncrit=0), dict(theta=0.0), dict(variant=5), dict(precision=9)):
+        prm = tcb.default_params(**bad)
+        rc = L.tc_create(C.byref(prm), C.byref(h))
+        assert rc in (1, 6), (bad, rc)
+        assert not h.value
+
+
+def test_evaluate_rejects_null_context():
+    L = tcb.load_library()
+    rc = L.tc_evaluate(None, 10, *([None] * 15), 0)
+    assert rc == 1
+
+
+def test_plummer_generator_statistics():
+    x, y, z, vx, vy, vz, m = ics.plummer(20000, seed=3)
+    assert abs(m.sum() - 1) < 1e-12
+    assert np.sqrt(x ** 2 + y ** 2 + z ** 2).max() < 10
+    ke = 0.5 * (m * (vx ** 2 + vy ** 2 + vz ** 2)).sum()
+    assert abs(ke - 0.25) < 0.02  # virial equilibrium in Henon units: T = -E = 1/4
+    x2, *_ = ics.plummer(20000, seed=3)
+    assert np.array_equal(x, x2)
+
+
+def test_kroupa_masses():
+    m = ics.kroupa_masses(200000, seed=1)
+    assert abs(m.sum() - 1) < 1e-12
+    r = m / m.min()
+    assert r.max() < 100 / 0.08 * 1.0001
+    # fraction above the 0.5 Msun break for alpha 1.3 / 2.3 on [0.08, 100]: ~ 0.17
+    mm = m / m.sum() * 200000  # relative masses; compare shape via quantile ratio
+    assert 0.1 < (mm > np.quantile(mm, 0.5) * 4).mean() < 0.3
+
+
+@pytest.mark.skipif(tcb.load_library() is None, reason="library")
+def test_missing_library_raises(tmp_path):
+    with pytest.raises(tcb.TaichiError):
+        tcb._lib_save = tcb._lib
+        try:
+            tcb._lib = None
+            tcb.load_library(str(tmp_path / "nope.so"))
+        finally:
+            tcb._lib = tcb._lib_save

@@ -306,7 +306,8 @@ def main():
                                parallelism="replicas" if world > 1 else "single"),
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb, "clocks": clocks,
                 "lists": {"cells": stats["n_cells"], "m2l_pairs": stats["n_m2l"], "p2p_pairs": stats["n_p2p"],
-                          "p2p_interactions": stats["n_p2p_inter"], "max_level": stats["max_level"]}}
+                          "p2p_interactions": stats["n_p2p_inter"], "max_level": stats["max_level"],
+                          "flags": stats["flags"]}}
         print(json.dumps(line))
     g.close()
     if dist:

@@ -62,6 +62,8 @@ typedef struct {
   int max_level;
   double ms_total, ms_tree, ms_upward, ms_traverse, ms_m2l, ms_p2p, ms_downward;
   long long n_launches; /* kernels launched by the last tc_evaluate */
+  long long flags;      /* diagnostic bits of the last evaluation (1 M2L, 2 P2P, 4 frontier capacity
+                           retries; 8 depth limit; 16 an enclosing ball hit its iteration cap) */
 } tc_stats;
 
 typedef struct tc_ctx tc_ctx;

@@ -462,7 +462,9 @@ int tco_miniball(int np, const double* pts, double* c, double* r2) {
       if (e > maxe) { maxe = e; piv = i; }
     }
     if (piv < 0 || maxe <= *r2 * 1e-15) return 0;
+    double old = *r2;
     if (!mb_small(s, &ns, pts + 3 * piv, c, r2)) return 2;
+    if (!(*r2 > old)) return 0; /* no growth: final (pivot loop of miniball.hpp stops the same way) */
   }
   return 1;
 }

@@ -42,7 +42,8 @@ class Stats(C.Structure):
                 ("n_m2l", C.c_longlong), ("n_p2p", C.c_longlong), ("n_p2p_inter", C.c_longlong),
                 ("max_level", C.c_int), ("ms_total", C.c_double), ("ms_tree", C.c_double),
                 ("ms_upward", C.c_double), ("ms_traverse", C.c_double), ("ms_m2l", C.c_double),
-                ("ms_p2p", C.c_double), ("ms_downward", C.c_double), ("n_launches", C.c_longlong)]
+                ("ms_p2p", C.c_double), ("ms_downward", C.c_double), ("n_launches", C.c_longlong),
+                ("flags", C.c_longlong)]
 
 
 EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_evaluate", "tc_get_stats",

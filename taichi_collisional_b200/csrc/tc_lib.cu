@@ -99,6 +99,7 @@ struct tc_ctx {
   unsigned long long n_m2l = 0, n_p2p = 0;
   int sbits = 1;
   long long launches = 0;
+  unsigned tree_flags = 0;
   unsigned long long n_inter = 0;
   cudaEvent_t ev[8];
   bool events = false;
@@ -239,7 +240,9 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   unsigned herr = 0;
   TC_CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   TC_CK(cudaStreamSynchronize(st));
+  if (herr & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
   if (herr & TC_EBIT_CELL_CAP) return TC_ERR_CAPACITY;
+  ctx->tree_flags = herr;
   ctx->ncell = ctx->lv.ncell;
   int maxl = 0;
   for (int l = 0; l <= TC_MAX_LEVEL; l++)
@@ -537,6 +540,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   cudaStream_t st = ctx->stream;
   ctx->n = n;
   ctx->launches = 0;
+  ctx->tree_flags = 0;
   size_t N = (size_t)n;
   if (ctx->events) cudaEventRecord(ctx->ev[0], st);
   // ---- inputs on the device
@@ -647,6 +651,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   S.max_level = ctx->max_level;
   S.n_p2p_inter = ctx->direct ? (long long)n * n : (long long)ctx->n_inter;
   S.n_launches = ctx->launches;
+  S.flags = herr | ctx->tree_flags;
   if (ctx->events) {
     float t[8];
     for (int i = 1; i < 8; i++) cudaEventElapsedTime(&t[i], ctx->ev[i - 1], ctx->ev[i]);
@@ -654,8 +659,8 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
     S.ms_total = t[0]; S.ms_tree = t[1]; S.ms_upward = t[2]; S.ms_traverse = t[3]; S.ms_m2l = t[4];
     S.ms_p2p = t[5]; S.ms_downward = t[6];
   }
-  if (herr & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
-  if (herr & TC_EBIT_DEPTH) return TC_ERR_DEPTH;
+  if ((herr | ctx->tree_flags) & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
+  if ((herr | ctx->tree_flags) & TC_EBIT_DEPTH) return TC_ERR_DEPTH;
   return TC_OK;
 }
 

@@ -134,7 +134,7 @@ __device__ __forceinline__ void tc_mb_farthest(const TcPointSet& ps, const TcBod
           int g = ps.seg_a[s] + it;
           double X = cl.X[g], Y = cl.Y[g], Z = cl.Z[g], R = cl.R[g];
           double q[3] = {X, Y, Z};
-          double dc = sqrt(tc_d2(q, c)) + R;
+          double dc = sqrt(tc_d2(q, c)) + R * td[192];  // td[192] = largest |t_k| of the table
           if (dc * dc * (1.0 + 1e-12) - r2 < best_e) continue;
           int base = ps.seg_start[s] + (it << 6);
           for (int k = 0; k < 64; k++) {
@@ -191,7 +191,9 @@ __device__ void tc_warp_miniball(const TcPointSet& ps, const TcBodies& b, const 
     if (best_i == 0x7fffffff || best_e <= *r2 * 1e-15) return;
     double q[3];
     tc_point_td(ps, best_i, b, cl, td, q);
+    double old = *r2;
     if (!tc_mb_small(s, ns, q, c, r2)) break;
+    if (!(*r2 > old)) return;  // no growth: the ball is final (the reference's stop rule)
   }
   // not converged: grow the ball to enclose every point and flag it
   double mx = 0;
@@ -353,8 +355,17 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcB
                                                                 const int* __restrict__ lv_start,
                                                                 const int* __restrict__ lv_count, unsigned int* err) {
   __shared__ cd sG[kUpWarps][(P + 1) * (P + 1)];
-  __shared__ double s_td[192];
+  __shared__ double s_td[193];
   for (int i = threadIdx.x; i < 192; i += blockDim.x) s_td[i] = c_tdesign[i];
+  if (threadIdx.x == 0) {
+    // rows 36-47 of the reference's table are not unit vectors (|t| = 1.1968), so the
+    // pruning bound uses the largest norm
+    double mx = 0;
+    for (int k = 0; k < 64; k++)
+      mx = fmax(mx, sqrt(c_tdesign[3 * k] * c_tdesign[3 * k] + c_tdesign[3 * k + 1] * c_tdesign[3 * k + 1] +
+                         c_tdesign[3 * k + 2] * c_tdesign[3 * k + 2]));
+    s_td[192] = mx * (1.0 + 1e-12);
+  }
   __syncthreads();
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int cnt = lv_count[l], st = lv_start[l];

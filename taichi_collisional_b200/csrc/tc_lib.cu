@@ -311,13 +311,15 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   int kbits = 2 * sbits;
   {
     size_t nm = ctx->n_m2l, np = ctx->n_p2p;
-    size_t hist_need = 256 * ((((nm > np ? nm : np) > (size_t)n ? (nm > np ? nm : np) : (size_t)n) + kRsTile - 1) / kRsTile + 1);
+    size_t mx = nm > np ? nm : np;
+    if (mx < (size_t)n) mx = (size_t)n;
+    size_t hist_need = 257 * ((mx + kRsTile - 1) / kRsTile + 1) + 1024;
     TC_CK(ctx->hist.ensure(hist_need));
     TC_CK(ctx->m2l_alt.ensure(nm + 1));
     TC_CK(ctx->p2p_alt.ensure(np + 1));
-    radix_sort(ctx->m2l.p, nullptr, ctx->m2l_alt.p, nullptr, (int)nm, kbits, ctx->hist.p, st);
-    radix_sort(ctx->p2p.p, nullptr, ctx->p2p_alt.p, nullptr, (int)np, kbits, ctx->hist.p, st);
-    ctx->launches += (nm > 1 ? 3 * ((kbits + 7) / 8) : 0) + (np > 1 ? 3 * ((kbits + 7) / 8) : 0) + 5;
+    ctx->launches += radix_sort(ctx->m2l.p, nullptr, ctx->m2l_alt.p, nullptr, (int)nm, kbits, ctx->hist.p, st);
+    ctx->launches += radix_sort(ctx->p2p.p, nullptr, ctx->p2p_alt.p, nullptr, (int)np, kbits, ctx->hist.p, st);
+    ctx->launches += 5;
     TC_CK(ctx->m2l_start.ensure(ctx->ncell + 1));
     TC_CK(ctx->p2p_start.ensure(ctx->ncell + 1));
     TC_CK(ctx->m2l_src.ensure(nm + 1));
@@ -345,7 +347,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   TcOut o = out_view(ctx, n, JERK);
   TC_CK(cudaMemsetAsync(ctx->outs.p, 0, sizeof(double) * (size_t)n * (JERK ? 7 : 4), st));
   if (hs[0] > 0) {
-    size_t smem = (size_t)NT * 32 * sizeof(double);
+    size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
     k_m2l<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
                                                                 ctx->m2l_src.p, cv);
     ctx->launches++;
@@ -378,7 +380,7 @@ typedef tc_status (*run_fn)(tc_ctx*, int);
 
 template <int P>
 static void set_m2l_attrs() {
-  size_t smem = (size_t)TC_NTERM(P) * 32 * sizeof(double);
+  size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
   cudaFuncSetAttribute(k_m2l<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_m2l<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
@@ -567,7 +569,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   TC_CK(ctx->vals.ensure(N)); TC_CK(ctx->vals_alt.ensure(N));
   TC_CK(ctx->bod.ensure(7 * N)); TC_CK(ctx->bflags.ensure(N)); TC_CK(ctx->perm.ensure(N));
   TC_CK(ctx->outs.ensure(7 * N));
-  TC_CK(ctx->hist.ensure(256 * ((N + kRsTile - 1) / kRsTile + 1)));
+  TC_CK(ctx->hist.ensure(257 * ((N + kRsTile - 1) / kRsTile + 1) + 1024));
   TC_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
   int direct_below = ctx->prm.direct_below;
   if (direct_below < 0) direct_below = jerk ? 8000 : ctx->prm.ncrit;
@@ -604,8 +606,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
       k_bounds_final<<<1, 1, 0, st>>>(nb, ctx->bpart.p, ctx->d_root, ctx->prm.use_shift, ctx->prm.shift_u[0],
                                       ctx->prm.shift_u[1], ctx->prm.shift_u[2]);
       k_morton<<<nblocks(n, 256), 256, 0, st>>>(n, dx, dy, dz, ctx->d_root, ctx->keys.p, ctx->vals.p);
-      radix_sort(ctx->keys.p, ctx->vals.p, ctx->keys_alt.p, ctx->vals_alt.p, n, 63, ctx->hist.p, st);
-      ctx->launches += 4 + 3 * 8;
+      ctx->launches += 4 + radix_sort(ctx->keys.p, ctx->vals.p, ctx->keys_alt.p, ctx->vals_alt.p, n, 63, ctx->hist.p, st);
       k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->vals.p, dx, dy, dz, dm, dvx, dvy, dvz, df, b);
       run_fn f = pick(ctx->prm.p, jerk);
       if (!f) return TC_ERR_UNSUPPORTED;

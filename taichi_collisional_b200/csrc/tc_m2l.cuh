@@ -12,8 +12,10 @@
 // source) pairs at a time, one pair per lane, so every per-degree step -- including the
 // constant swap matrices, emitted as straight-line code with immediate coefficients --
 // runs in registers.  The only exchange is the z-translation, which mixes degrees and goes
-// through shared memory (NT x 32 doubles).  Each lane accumulates its pairs' locals in
-// registers; one warp reduction per target gives deterministic sums.
+// through shared memory (NT x 32 doubles).  Each lane accumulates its pairs' locals in its
+// own column of a shared NT x 32 accumulator; one fixed-order sum over the 32 columns per
+// coefficient gives deterministic results.  Per pair, warp 0 also stores the rotation
+// angles and the translation factors j!/r^(j+1) for the other warps.
 #pragma once
 #include "swap_tables.h"
 #include "tc_harmonics.cuh"
@@ -70,7 +72,7 @@ __device__ __forceinline__ TcPairGeo tc_pair_geo(double dx, double dy, double dz
 
 // forward half for degree D: scaled, rotated into the pair frame, unscaled -> smem
 template <int P, int D>
-__device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, const TcPairGeo& g, double* buf, int lane) {
+__device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1, cd ex1, double* buf, int lane) {
   double v[2 * D + 1], o[2 * D + 1];
 #pragma unroll
   for (int k = 0; k < 2 * D + 1; k++) v[k] = __ldg(Ms + D * D + k) * c_fc[D * D + k];
@@ -78,136 +80,152 @@ __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, const 
     v[0] = 0.0;
     v[2 * D] = 0.0;
   }
-  tc_rot_fwd<D>(v, g.ez1);
+  tc_rot_fwd<D>(v, ez1);
   TcSwapDeg<D>::apply(v, o);
-  tc_rot_fwd<D>(o, g.ex1);
+  tc_rot_fwd<D>(o, ex1);
   TcSwapDeg<D>::apply(o, v);
 #pragma unroll
   for (int k = 0; k < 2 * D + 1; k++) buf[(D * D + k) * 32 + lane] = v[k] * c_fcinv[D * D + k];
 }
 
-// translation along z to output degree N, then rotation back; accumulate into acc
+// translation along z to output degree N, then rotation back; accumulate into the lane's
+// column of the shared accumulator.  gz[j*32+lane] = j! / r^(j+1).
 template <int P, int N>
-__device__ __forceinline__ void tc_m2l_back(const double* buf, int lane, const TcPairGeo& g, double* acc, bool valid) {
+__device__ __forceinline__ void tc_m2l_back(const double* buf, const double* gz, int lane, cd ez1, cd ex1,
+                                            double* acc, bool valid) {
   double l[2 * N + 1], o[2 * N + 1];
 #pragma unroll
   for (int k = 0; k < 2 * N + 1; k++) l[k] = 0.0;
-  const double rinv = g.rinv;
-  double pn = rinv;
-#pragma unroll
-  for (int j = 0; j < N; j++) pn *= rinv;  // rinv^(N+1)
   {
-    double s = 0.0, pr = pn;
+    double s = 0.0;
 #pragma unroll
-    for (int k = 0; k <= P - N; k++) {
-      s += buf[(k * k + k) * 32 + lane] * (c_fact[N + k] * pr);
-      pr *= rinv;
-    }
+    for (int k = 0; k <= P - N; k++) s += buf[(k * k + k) * 32 + lane] * gz[(N + k) * 32 + lane];
     l[N] = s;
   }
-  double pm = rinv, sg = -1.0;
   constexpr int MMAX = N < P - N ? N : P - N;
 #pragma unroll
   for (int m = 1; m <= MMAX; m++) {
-    double pr = pn * pm, sn = 0.0, sp = 0.0;
+    double sn = 0.0, sp = 0.0;
 #pragma unroll
     for (int k = m; k <= P - N; k++) {
-      double f = c_fact[N + k] * pr * sg;
+      double f = gz[(N + k) * 32 + lane];
       sn += buf[(k * k + k - m) * 32 + lane] * f;
       sp += buf[(k * k + k + m) * 32 + lane] * f;
-      pr *= rinv;
     }
-    l[N - m] = sn;
-    l[N + m] = sp;
-    sg = -sg;
-    pm *= rinv;
+    const double sg = (m & 1) ? -1.0 : 1.0;
+    l[N - m] = sg * sn;
+    l[N + m] = sg * sp;
   }
   TcSwapDeg<N>::apply(l, o);
-  tc_rot_inv<N>(o, g.ex1);
+  tc_rot_inv<N>(o, ex1);
   TcSwapDeg<N>::apply(o, l);
-  tc_rot_inv<N>(l, g.ez1);
+  tc_rot_inv<N>(l, ez1);
   if (valid) {
 #pragma unroll
-    for (int k = 0; k < 2 * N + 1; k++) acc[k] += l[k];
+    for (int k = 0; k < 2 * N + 1; k++) acc[(N * N + k) * 32 + lane] += l[k];
   }
 }
 
-template <int N>
-__device__ __forceinline__ void tc_warp_sum_store(double* acc, double* dst) {
-#pragma unroll
-  for (int k = 0; k < 2 * N + 1; k++) {
-    double v = acc[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    acc[k] = v;
-  }
-  if ((threadIdx.x & 31) == 0) {
-#pragma unroll
-    for (int k = 0; k < 2 * N + 1; k++) dst[N * N + k] = acc[k];
-  }
+// shared-memory layout of one M2L CTA (doubles): buf | acc | gz | geo
+template <int P>
+struct TcM2LSmem {
+  static constexpr int NT = (P + 1) * (P + 1);
+  static constexpr int BUF = 0, ACC = NT * 32, GZ = 2 * NT * 32, GEO = 2 * NT * 32 + (P + 1) * 32;
+  static constexpr int TOTAL = GEO + 4 * 32;
+};
+
+// warp g owns the degree pair (g, P - g)
+template <int P, int G>
+__device__ __forceinline__ void tc_m2l_fwd_group(const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
+  tc_m2l_fwd<P, G>(Ms, ez1, ex1, buf, lane);
+  if (G != P - G) tc_m2l_fwd<P, P - G>(Ms, ez1, ex1, buf, lane);
+}
+template <int P, int G>
+__device__ __forceinline__ void tc_m2l_back_group(const double* buf, const double* gz, int lane, cd ez1, cd ex1,
+                                                  double* acc, bool valid) {
+  tc_m2l_back<P, G>(buf, gz, lane, ez1, ex1, acc, valid);
+  if (G != P - G) tc_m2l_back<P, P - G>(buf, gz, lane, ez1, ex1, acc, valid);
 }
 
-template <int P, int G, bool JERK>
-__device__ void tc_m2l_group(int t, int s_beg, int s_end, const int* __restrict__ src, const TcCells& c, double* buf) {
-  constexpr int NT = (P + 1) * (P + 1);
-  constexpr int D1 = G, D2 = P - G;
-  constexpr bool TWO = D1 != D2;
-  int lane = threadIdx.x & 31;
-  double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
-  for (int arr = 0; arr < (JERK ? 2 : 1); arr++) {
-    const double* Mbase = arr ? c.Md : c.M;
-    double a1[2 * D1 + 1], a2[2 * D2 + 1];
-#pragma unroll
-    for (int k = 0; k < 2 * D1 + 1; k++) a1[k] = 0.0;
-#pragma unroll
-    for (int k = 0; k < 2 * D2 + 1; k++) a2[k] = 0.0;
-    for (int b0 = s_beg; b0 < s_end; b0 += 32) {
-      int idx = b0 + lane;
-      bool valid = idx < s_end;
-      int s = src[valid ? idx : s_beg];
-      TcPairGeo g = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
-      const double* Ms = Mbase + (size_t)s * NT;
-      tc_m2l_fwd<P, D1>(Ms, g, buf, lane);
-      if (TWO) tc_m2l_fwd<P, D2>(Ms, g, buf, lane);
-      tc_bar_cta();
-      tc_m2l_back<P, D1>(buf, lane, g, a1, valid);
-      if (TWO) tc_m2l_back<P, D2>(buf, lane, g, a2, valid);
-      tc_bar_cta();
-    }
-    double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NT;
-    tc_warp_sum_store<D1>(a1, Lt);
-    if (TWO) tc_warp_sum_store<D2>(a2, Lt);
-  }
-}
-
-template <int P, int G, bool JERK>
+template <int P, int G>
 struct TcM2LDispatch {
-  static __device__ __forceinline__ void run(int g, int t, int sb, int se, const int* src, const TcCells& c, double* buf) {
-    if (g == G)
-      tc_m2l_group<P, G, JERK>(t, sb, se, src, c, buf);
-    else
-      TcM2LDispatch<P, G + 1, JERK>::run(g, t, sb, se, src, c, buf);
+  static __device__ __forceinline__ void fwd(int g, const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
+    if (g == G) tc_m2l_fwd_group<P, G>(Ms, ez1, ex1, buf, lane);
+    else TcM2LDispatch<P, G + 1>::fwd(g, Ms, ez1, ex1, buf, lane);
+  }
+  static __device__ __forceinline__ void back(int g, const double* buf, const double* gz, int lane, cd ez1, cd ex1,
+                                              double* acc, bool valid) {
+    if (g == G) tc_m2l_back_group<P, G>(buf, gz, lane, ez1, ex1, acc, valid);
+    else TcM2LDispatch<P, G + 1>::back(g, buf, gz, lane, ez1, ex1, acc, valid);
   }
 };
-template <int P, bool JERK>
-struct TcM2LDispatch<P, P / 2 + 1, JERK> {
-  static __device__ __forceinline__ void run(int, int, int, int, const int*, const TcCells&, double*) {}
+template <int P>
+struct TcM2LDispatch<P, P / 2 + 1> {
+  static __device__ __forceinline__ void fwd(int, const double*, cd, cd, double*, int) {}
+  static __device__ __forceinline__ void back(int, const double*, const double*, int, cd, cd, double*, bool) {}
 };
 
 template <int P>
 constexpr int tc_m2l_threads() { return 32 * (P / 2 + 1); }
 
 template <int P, bool JERK>
-__global__ void __launch_bounds__(tc_m2l_threads<P>()) k_m2l(const int* __restrict__ tlist, int ntl,
-                                                               const int* __restrict__ tstart,
-                                                               const int* __restrict__ src, TcCells c) {
-  extern __shared__ double tc_m2l_buf[];
+__global__ void __launch_bounds__(tc_m2l_threads<P>(), (P >= 14 ? 1 : 2)) k_m2l(const int* __restrict__ tlist, int ntl,
+                                                                  const int* __restrict__ tstart,
+                                                                  const int* __restrict__ src, TcCells c) {
+  using SM = TcM2LSmem<P>;
+  constexpr int NT = SM::NT;
+  extern __shared__ double tc_m2l_smem[];
+  double* buf = tc_m2l_smem + SM::BUF;
+  double* acc = tc_m2l_smem + SM::ACC;
+  double* gz = tc_m2l_smem + SM::GZ;
+  double* geo = tc_m2l_smem + SM::GEO;
   int ti = blockIdx.x;
   if (ti >= ntl) return;
   int t = tlist[ti];
   if (!c.has_sink[t]) return;
-  int g = threadIdx.x >> 5;
-  TcM2LDispatch<P, 0, JERK>::run(g, t, tstart[t], tstart[t + 1], src, c, tc_m2l_buf);
+  const int g = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int s_beg = tstart[t], s_end = tstart[t + 1];
+  const double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
+  for (int arr = 0; arr < (JERK ? 2 : 1); arr++) {
+    const double* Mbase = arr ? c.Md : c.M;
+    for (int i = threadIdx.x; i < NT * 32; i += blockDim.x) acc[i] = 0.0;
+    for (int b0 = s_beg; b0 < s_end; b0 += 32) {
+      int idx = b0 + lane;
+      bool valid = idx < s_end;
+      int s = src[valid ? idx : s_beg];
+      cd ez1, ex1;
+      if (g == 0) {
+        TcPairGeo pg = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
+        ez1 = pg.ez1;
+        ex1 = pg.ex1;
+        geo[0 * 32 + lane] = ez1.x; geo[1 * 32 + lane] = ez1.y;
+        geo[2 * 32 + lane] = ex1.x; geo[3 * 32 + lane] = ex1.y;
+        double pr = pg.rinv;
+#pragma unroll
+        for (int j = 0; j <= P; j++) {
+          gz[j * 32 + lane] = c_fact[j] * pr;
+          pr *= pg.rinv;
+        }
+      }
+      tc_bar_cta();
+      if (g != 0) {
+        ez1 = mk(geo[0 * 32 + lane], geo[1 * 32 + lane]);
+        ex1 = mk(geo[2 * 32 + lane], geo[3 * 32 + lane]);
+      }
+      TcM2LDispatch<P, 0>::fwd(g, Mbase + (size_t)s * NT, ez1, ex1, buf, lane);
+      tc_bar_cta();
+      TcM2LDispatch<P, 0>::back(g, buf, gz, lane, ez1, ex1, acc, valid);
+      tc_bar_cta();
+    }
+    double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NT;
+    for (int r = threadIdx.x; r < NT; r += blockDim.x) {
+      double v = 0.0;
+#pragma unroll 8
+      for (int q = 0; q < 32; q++) v += acc[r * 32 + q];
+      Lt[r] = v;
+    }
+    tc_bar_cta();
+  }
 }
 
 }  // namespace tc

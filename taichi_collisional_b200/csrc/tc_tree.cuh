@@ -147,6 +147,54 @@ __global__ void k_excl_scan_u32(uint32_t* __restrict__ a, int total, uint32_t* _
   if (t == T - 1 && sum_out) *sum_out = s[t];
 }
 
+// multi-block exclusive scan: 4096 counters per block, then the block sums, then the fix-up
+constexpr int kScanThreads = 1024, kScanItems = 4;
+__global__ void __launch_bounds__(kScanThreads) k_scan_blocks(uint32_t* __restrict__ a, int total,
+                                                              uint32_t* __restrict__ sums) {
+  __shared__ uint32_t s[kScanThreads];
+  int t = threadIdx.x;
+  int base = blockIdx.x * kScanThreads * kScanItems + t * kScanItems;
+  uint32_t v[kScanItems], loc = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) {
+    v[i] = base + i < total ? a[base + i] : 0u;
+    loc += v[i];
+  }
+  s[t] = loc;
+  __syncthreads();
+  for (int o = 1; o < kScanThreads; o <<= 1) {
+    uint32_t w = t >= o ? s[t - o] : 0u;
+    __syncthreads();
+    s[t] += w;
+    __syncthreads();
+  }
+  uint32_t run = s[t] - loc;
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) {
+    if (base + i < total) a[base + i] = run;
+    run += v[i];
+  }
+  if (t == kScanThreads - 1) sums[blockIdx.x] = s[t];
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ a, int total, const uint32_t* __restrict__ sums) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) a[i] += sums[i / (kScanThreads * kScanItems)];
+}
+
+// exclusive scan of a[total] in place; sums needs total / 4096 + 1 entries
+inline int excl_scan(uint32_t* a, int total, uint32_t* sums, cudaStream_t st) {
+  int nb = (total + kScanThreads * kScanItems - 1) / (kScanThreads * kScanItems);
+  if (nb <= 1) {
+    k_excl_scan_u32<<<1, 1024, 0, st>>>(a, total, nullptr);
+    return 1;
+  }
+  k_scan_blocks<<<nb, kScanThreads, 0, st>>>(a, total, sums);
+  k_excl_scan_u32<<<1, 1024, 0, st>>>(sums, nb, nullptr);
+  k_scan_add<<<(total + 255) / 256, 256, 0, st>>>(a, total, sums);
+  return 3;
+}
+
 template <bool kVals>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long long* __restrict__ kin, const int* __restrict__ vin,
                                                            unsigned long long* __restrict__ kout, int* __restrict__ vout, int n,
@@ -183,9 +231,10 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long l
 }
 
 // Sorts (keys, vals) by key bits [0, bits).  Uses alt buffers; the result ends in keys/vals.
-inline void radix_sort(unsigned long long* keys, int* vals, unsigned long long* keys_alt, int* vals_alt, int n, int bits, uint32_t* hist,
-                       cudaStream_t st) {
-  if (n <= 1) return;
+inline int radix_sort(unsigned long long* keys, int* vals, unsigned long long* keys_alt, int* vals_alt, int n, int bits, uint32_t* hist,
+                      cudaStream_t st) {
+  if (n <= 1) return 0;
+  int launches = 0;
   int nblk = (n + kRsTile - 1) / kRsTile;
   int passes = (bits + 7) / 8;
   unsigned long long *ka = keys, *kb = keys_alt;
@@ -193,7 +242,7 @@ inline void radix_sort(unsigned long long* keys, int* vals, unsigned long long* 
   for (int p = 0; p < passes; p++) {
     int shift = 8 * p;
     k_rs_hist<<<nblk, kRsThreads, 0, st>>>(ka, n, shift, hist);
-    k_excl_scan_u32<<<1, 1024, 0, st>>>(hist, 256 * nblk, nullptr);
+    launches += 2 + excl_scan(hist, 256 * nblk, hist + 256 * (size_t)nblk, st);
     if (vals)
       k_rs_scatter<true><<<nblk, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, hist);
     else
@@ -205,6 +254,7 @@ inline void radix_sort(unsigned long long* keys, int* vals, unsigned long long* 
     cudaMemcpyAsync(keys, ka, sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, st);
     if (vals) cudaMemcpyAsync(vals, va, sizeof(int) * n, cudaMemcpyDeviceToDevice, st);
   }
+  return launches;
 }
 
 // gather the caller's arrays into Morton order

@@ -127,6 +127,20 @@ def swap_matrix(G, n):
     return [[A[k][j] * D[k] / D[j] for j in range(2 * n + 1)] for k in range(2 * n + 1)]
 
 
+def orthogonal_form(S, n):
+    """T = E S E^-1 (float64 entries), orthogonal; E_k = c_k / sqrt(D_k)."""
+    D = [math.factorial(n + abs(m)) * math.factorial(n - abs(m)) for m in range(-n, n + 1)]
+    E = [(1.0 if m == 0 else math.sqrt(2.0)) / math.sqrt(D[m + n]) for m in range(-n, n + 1)]
+    out = []
+    for k in range(2 * n + 1):
+        row = []
+        for j in range(2 * n + 1):
+            v = S[k][j]
+            row.append(0.0 if v == 0 else float(v) * E[k] / E[j])
+        out.append(row)
+    return out
+
+
 def derive(pmax):
     G = regular_harmonics(pmax)
     return [swap_matrix(G, n) for n in range(pmax + 1)]
@@ -187,6 +201,18 @@ def write_header(mats, path):
             for j in range(2 * n + 1):
                 if S[k][j] != 0:
                     terms.append("T(%s) * v[%d]" % (_fmt(S[k][j]), j))
+            L.append("    o[%d] = %s;" % (k, " + ".join(terms) if terms else "T(0)"))
+        L.append("  }")
+        L.append("};")
+    L.append("// Orthogonal form used by the mixed-precision M2L: T_n = E S_n E^-1 with")
+    L.append("// E = diag(sqrt((n+|m|)!(n-|m|)!) c_m / ((n+|m|)!(n-|m|)!)), c_0 = 1, c_m = sqrt(2).")
+    L.append("template <int N> struct TcSwapOrthDeg;")
+    for n, S in enumerate(mats):
+        T = orthogonal_form(S, n)
+        L.append("template <> struct TcSwapOrthDeg<%d> {" % n)
+        L.append("  template <typename T> static __device__ __forceinline__ void apply(const T* v, T* o) {")
+        for k in range(2 * n + 1):
+            terms = ["T(%r) * v[%d]" % (T[k][j], j) for j in range(2 * n + 1) if T[k][j] != 0.0]
             L.append("    o[%d] = %s;" % (k, " + ".join(terms) if terms else "T(0)"))
         L.append("  }")
         L.append("};")

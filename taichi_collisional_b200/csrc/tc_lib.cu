@@ -22,6 +22,7 @@
 #include "tc_upward.cuh"
 #include "tc_traverse.cuh"
 #include "tc_m2l.cuh"
+#include "tc_m2l_mixed.cuh"
 #include "tc_down.cuh"
 #include "tc_p2p.cuh"
 #include "tdesign.h"
@@ -136,6 +137,29 @@ static cudaError_t init_constants(int dev) {
   if ((e = cudaMemcpyToSymbol(c_fc, fc, sizeof(fc))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_fcinv, fci, sizeof(fci))) != cudaSuccess) return e;
   if ((e = cudaMemcpyToSymbol(c_tdesign, tc_tdesign, sizeof(tc_tdesign))) != cudaSuccess) return e;
+  // mixed-precision M2L scalings (tc_m2l_mixed.cuh)
+  double mF[TC_NTERM(TC_PMAX_DEV)], mDoF[TC_NTERM(TC_PMAX_DEV)];
+  static float mC[(TC_PMAX_DEV + 1) * (TC_PMAX_DEV + 1) * (TC_PMAX_DEV + 1)];
+  for (int n = 0; n <= TC_PMAX_DEV; n++)
+    for (int m = -n; m <= n; m++) {
+      int am = m < 0 ? -m : m;
+      double D = fact[n + am] * fact[n - am];
+      double F = sqrt(D) * (am ? sqrt(2.0) : 1.0);
+      mF[n * n + n + m] = F;
+      mDoF[n * n + n + m] = D / F;
+    }
+  for (int n = 0; n <= TC_PMAX_DEV; n++)
+    for (int k = 0; k <= TC_PMAX_DEV; k++)
+      for (int m = 0; m <= TC_PMAX_DEV; m++) {
+        double v = 0.0;
+        if (m <= n && m <= k && n + k <= 2 * TC_PMAX_DEV)
+          v = ((m & 1) ? -1.0 : 1.0) * fact[n + k] /
+              sqrt(fact[n + m] * fact[n - m] * fact[k + m] * fact[k - m]);
+        mC[(n * (TC_PMAX_DEV + 1) + k) * (TC_PMAX_DEV + 1) + m] = (float)v;
+      }
+  if ((e = cudaMemcpyToSymbol(c_mF, mF, sizeof(mF))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_mDoF, mDoF, sizeof(mDoF))) != cudaSuccess) return e;
+  if ((e = cudaMemcpyToSymbol(c_mC, mC, sizeof(mC))) != cudaSuccess) return e;
   if (dev >= 0 && dev < 64) g_const_init[dev] = true;
   return cudaSuccess;
 }
@@ -346,16 +370,27 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   // ---- far field and near field
   TcOut o = out_view(ctx, n, JERK);
   TC_CK(cudaMemsetAsync(ctx->outs.p, 0, sizeof(double) * (size_t)n * (JERK ? 7 : 4), st));
+  const bool mixed = prm.precision == TC_PREC_MIXED;
   if (hs[0] > 0) {
-    size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
-    k_m2l<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
-                                                                ctx->m2l_src.p, cv);
+    if (mixed) {
+      size_t smem = (size_t)TcM2LMixSmem<P>::BYTES;
+      k_m2l_mixed<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
+                                                                        ctx->m2l_src.p, cv);
+    } else {
+      size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
+      k_m2l<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
+                                                                  ctx->m2l_src.p, cv);
+    }
     ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[4], st);
   if (hs[1] > 0) {
     int g = nblocks(hs[1], kP2PWarps);
-    k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o);
+    if (mixed)
+      k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b,
+                                                       cv, o);
+    else
+      k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o);
     ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[5], st);
@@ -383,6 +418,9 @@ static void set_m2l_attrs() {
   size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
   cudaFuncSetAttribute(k_m2l<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_m2l<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  size_t smx = (size_t)TcM2LMixSmem<P>::BYTES;
+  cudaFuncSetAttribute(k_m2l_mixed<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
+  cudaFuncSetAttribute(k_m2l_mixed<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
 }
 
 #define TC_ORDERS(X) X(4) X(6) X(8) X(10) X(12) X(16)

@@ -116,6 +116,29 @@ tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, dou
  * used as the roofline denominator of the FP64 / FP32 kernels.  Returns < 0 on error. */
 double tc_probe_peak(tc_ctx* ctx, int kind);
 
+/* Direct-summation evaluation that allocates no device memory.  It has no counterpart in the
+ * reference; it serves callers that cannot call cudaMalloc -- for example a host program
+ * whose own allocator already owns the GPU memory it may use, or a time-stepping loop that
+ * must not stall on the implicit device synchronisation cudaMalloc/cudaFree bring.
+ *
+ * Same arithmetic as tc_evaluate's direct branch (every sink against every source, FP64,
+ * r = 0 skipped; the jerk when `jerk` is non-zero).  All pointers are device pointers;
+ * vx/vy/vz are required when jerk != 0, flags may be NULL.  Work is queued on `stream`
+ * (cudaStream_t as void*; NULL = legacy default) and the call returns without waiting.
+ * Its working storage is one fixed static device array per GPU that loads the library
+ * (held until the process exits), sized for TC_NOALLOC_MAX_N bodies; larger n returns
+ * TC_ERR_CAPACITY without doing any work.  The first call on a device looks that array
+ * up (cudaGetSymbolAddress) with the caller's current device; make that first call before
+ * any stream capture.  Every call reuses the same array, and every entry a call reads is
+ * written earlier in that same call, so nothing has to be cleared between calls; calls that
+ * overlap on the GPU (different streams, or another host thread) race on the array. */
+#define TC_NOALLOC_MAX_N 16384
+tc_status tc_evaluate_direct_noalloc(int n, const double* x, const double* y, const double* z,
+                                     const double* vx, const double* vy, const double* vz,
+                                     const double* m, const unsigned char* flags, double* ax,
+                                     double* ay, double* az, double* pot, double* jx, double* jy,
+                                     double* jz, int jerk, void* stream);
+
 const char* tc_status_string(tc_status s);
 const char* tc_last_error_string(tc_ctx* ctx);
 int tc_pmax(void);

@@ -48,7 +48,8 @@ class Stats(C.Structure):
 
 EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_evaluate", "tc_get_stats",
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
-           "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak"]
+           "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc"]
+NOALLOC_MAX_N = 16384
 
 _lib = None
 
@@ -93,6 +94,8 @@ def load_library(path=LIB_PATH):
     L.tc_kick_drift.restype = C.c_int
     L.tc_probe_peak.argtypes = [C.c_void_p, C.c_int]
     L.tc_probe_peak.restype = C.c_double
+    L.tc_evaluate_direct_noalloc.argtypes = [C.c_int] + [C.c_void_p] * 8 + [C.c_void_p] * 7 + [C.c_int, C.c_void_p]
+    L.tc_evaluate_direct_noalloc.restype = C.c_int
     _lib = L
     return L
 
@@ -236,6 +239,28 @@ class Gravity:
                                        L.ctypes.data_as(_dp), None if Ld is None else Ld.ctypes.data_as(_dp))
         self._check(rc, "tc_get_expansions")
         return M, Md, L, Ld
+
+
+def evaluate_direct_noalloc(x, y, z, m, vx=None, vy=None, vz=None, flags=None, out=None, stream=0):
+    """Direct sum without any device allocation by the library (tc_evaluate_direct_noalloc).
+
+    For callers that cannot allocate device memory; CUDA float64 tensors in and out, at most
+    NOALLOC_MAX_N bodies.  The library's working storage is a fixed static device array, so
+    calls that overlap on the GPU race.  Returns the output dict (queued on ``stream``)."""
+    import torch
+    L = load_library()
+    n = len(x)
+    jerk = vx is not None
+    if out is None:
+        keys = ("ax", "ay", "az", "pot", "jx", "jy", "jz") if jerk else ("ax", "ay", "az", "pot")
+        out = {k: torch.empty(n, dtype=torch.float64, device=x.device) for k in keys}
+    rc = L.tc_evaluate_direct_noalloc(n, _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(m),
+                                      _ptr(flags), _ptr(out["ax"]), _ptr(out["ay"]), _ptr(out["az"]),
+                                      _ptr(out["pot"]), _ptr(out.get("jx")), _ptr(out.get("jy")),
+                                      _ptr(out.get("jz")), int(jerk), C.c_void_p(stream))
+    if rc != 0:
+        raise TaichiError("tc_evaluate_direct_noalloc: %s" % STATUS.get(rc, rc))
+    return out
 
 
 def get_force_and_potential(x, y, z, m, vx=None, vy=None, vz=None, flags=None, **params):

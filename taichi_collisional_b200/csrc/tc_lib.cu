@@ -477,6 +477,21 @@ __global__ void k_fma_probe(T* out, int iters) {
 }
 
 // ----------------------------------------------------------------------------------------
+// Scratch of tc_evaluate_direct_noalloc: a fixed static device array instead of cudaMalloc.
+// Layout: 7 body arrays (x y z m vx vy vz) | 7 output arrays, each TC_NOALLOC_MAX_N doubles.
+// ----------------------------------------------------------------------------------------
+static __device__ __align__(256) double g_noalloc_scratch[14 * TC_NOALLOC_MAX_N];
+static __device__ __align__(256) int g_noalloc_index[TC_NOALLOC_MAX_N];
+static __device__ __align__(256) uint8_t g_noalloc_flags[TC_NOALLOC_MAX_N];
+
+struct TcNoallocDev {
+  double* scratch = nullptr;
+  int* index = nullptr;
+  uint8_t* flags = nullptr;
+};
+static TcNoallocDev g_noalloc_dev[64];
+
+// ----------------------------------------------------------------------------------------
 // C ABI
 // ----------------------------------------------------------------------------------------
 extern "C" {
@@ -742,6 +757,49 @@ double tc_probe_peak(tc_ctx* ctx, int kind) {
   if (cudaGetLastError() != cudaSuccess) return -1.0;
   double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
   return flops / (best * 1e-3) / 1e9;
+}
+
+tc_status tc_evaluate_direct_noalloc(int n, const double* x, const double* y, const double* z, const double* vx,
+                                     const double* vy, const double* vz, const double* m, const unsigned char* flags,
+                                     double* ax, double* ay, double* az, double* pot, double* jx, double* jy,
+                                     double* jz, int jerk, void* stream) {
+  if (n <= 0 || !x || !y || !z || !m || !ax || !ay || !az || !pot) return TC_ERR_ARG;
+  if (jerk && (!vx || !vy || !vz || !jx || !jy || !jz)) return TC_ERR_ARG;
+  if (n > TC_NOALLOC_MAX_N) return TC_ERR_CAPACITY;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return TC_ERR_CUDA;
+  TcNoallocDev& D = g_noalloc_dev[dev];
+  if (!D.scratch) {  // once per device: device addresses of the static arrays
+    double* ps = nullptr;
+    int* pi = nullptr;
+    uint8_t* pf = nullptr;
+    if (cudaGetSymbolAddress((void**)&ps, g_noalloc_scratch) != cudaSuccess) return TC_ERR_CUDA;
+    if (cudaGetSymbolAddress((void**)&pi, g_noalloc_index) != cudaSuccess) return TC_ERR_CUDA;
+    if (cudaGetSymbolAddress((void**)&pf, g_noalloc_flags) != cudaSuccess) return TC_ERR_CUDA;
+    D.index = pi;
+    D.flags = pf;
+    D.scratch = ps;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t S = TC_NOALLOC_MAX_N;
+  TcBodies b;
+  b.x = D.scratch; b.y = D.scratch + S; b.z = D.scratch + 2 * S; b.m = D.scratch + 3 * S;
+  b.vx = jerk ? D.scratch + 4 * S : nullptr; b.vy = jerk ? D.scratch + 5 * S : nullptr;
+  b.vz = jerk ? D.scratch + 6 * S : nullptr;
+  b.flags = D.flags;
+  b.perm = D.index;
+  TcOut o;
+  o.pot = D.scratch + 7 * S; o.ax = D.scratch + 8 * S; o.ay = D.scratch + 9 * S; o.az = D.scratch + 10 * S;
+  o.jx = jerk ? D.scratch + 11 * S : nullptr; o.jy = jerk ? D.scratch + 12 * S : nullptr;
+  o.jz = jerk ? D.scratch + 13 * S : nullptr;
+  k_identity<<<nblocks(n, 256), 256, 0, st>>>(n, D.index);
+  k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, D.index, x, y, z, m, vx, vy, vz, flags, b);
+  if (jerk)
+    k_direct<true><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
+  else
+    k_direct<false><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
+  k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, D.index, o, pot, ax, ay, az, jerk ? jx : nullptr, jy, jz);
+  return cudaGetLastError() == cudaSuccess ? TC_OK : TC_ERR_CUDA;
 }
 
 tc_status tc_get_stats(tc_ctx* ctx, tc_stats* st) {

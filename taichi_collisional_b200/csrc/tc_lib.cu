@@ -374,7 +374,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   if (hs[0] > 0) {
     if (mixed) {
       size_t smem = (size_t)TcM2LMixSmem<P>::BYTES;
-      k_m2l_mixed<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
+      k_m2l_mixed<P, JERK><<<hs[0], tc_m2lx_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
                                                                         ctx->m2l_src.p, cv);
     } else {
       size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);

@@ -19,6 +19,7 @@
 #pragma once
 #include "swap_tables.h"
 #include "tc_harmonics.cuh"
+#include "m2l_schedule.h"
 
 namespace tc {
 
@@ -89,17 +90,29 @@ __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1
 }
 
 // translation along z to output degree N, then rotation back; accumulate into the lane's
-// column of the shared accumulator.  gz[j*32+lane] = j! / r^(j+1).
+// column of the shared accumulator.  Factors (n+k)! / r^(n+k+1) are formed on the fly.
 template <int P, int N>
-__device__ __forceinline__ void tc_m2l_back(const double* buf, const double* gz, int lane, cd ez1, cd ex1,
+__device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int lane, cd ez1, cd ex1,
                                             double* acc, bool valid) {
   double l[2 * N + 1], o[2 * N + 1];
 #pragma unroll
   for (int k = 0; k < 2 * N + 1; k++) l[k] = 0.0;
+  double pn = rinv;
+#pragma unroll
+  for (int j = 0; j < N; j++) pn *= rinv;  // rinv^(N+1)
+  double fk[P - N + 1];                    // (N+k)! rinv^(N+k+1)
+  {
+    double pr = pn;
+#pragma unroll
+    for (int k = 0; k <= P - N; k++) {
+      fk[k] = c_fact[N + k] * pr;
+      pr *= rinv;
+    }
+  }
   {
     double s = 0.0;
 #pragma unroll
-    for (int k = 0; k <= P - N; k++) s += buf[(k * k + k) * 32 + lane] * gz[(N + k) * 32 + lane];
+    for (int k = 0; k <= P - N; k++) s += buf[(k * k + k) * 32 + lane] * fk[k];
     l[N] = s;
   }
   constexpr int MMAX = N < P - N ? N : P - N;
@@ -108,9 +121,8 @@ __device__ __forceinline__ void tc_m2l_back(const double* buf, const double* gz,
     double sn = 0.0, sp = 0.0;
 #pragma unroll
     for (int k = m; k <= P - N; k++) {
-      double f = gz[(N + k) * 32 + lane];
-      sn += buf[(k * k + k - m) * 32 + lane] * f;
-      sp += buf[(k * k + k + m) * 32 + lane] * f;
+      sn += buf[(k * k + k - m) * 32 + lane] * fk[k];
+      sp += buf[(k * k + k + m) * 32 + lane] * fk[k];
     }
     const double sg = (m & 1) ? -1.0 : 1.0;
     l[N - m] = sg * sn;
@@ -126,64 +138,67 @@ __device__ __forceinline__ void tc_m2l_back(const double* buf, const double* gz,
   }
 }
 
-// shared-memory layout of one M2L CTA (doubles): buf | acc | gz | geo
+// shared-memory layout of one M2L CTA (doubles): buf | acc
 template <int P>
 struct TcM2LSmem {
   static constexpr int NT = (P + 1) * (P + 1);
-  static constexpr int BUF = 0, ACC = NT * 32, GZ = 2 * NT * 32, GEO = 2 * NT * 32 + (P + 1) * 32;
-  static constexpr int TOTAL = GEO + 4 * 32;
+  static constexpr int BUF = 0, ACC = NT * 32;
+  static constexpr int TOTAL = 2 * NT * 32;
 };
 
-// warp g owns the degree pair (g, P - g)
-template <int P, int G>
-__device__ __forceinline__ void tc_m2l_fwd_group(const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
-  tc_m2l_fwd<P, G>(Ms, ez1, ex1, buf, lane);
-  if (G != P - G) tc_m2l_fwd<P, P - G>(Ms, ez1, ex1, buf, lane);
-}
-template <int P, int G>
-__device__ __forceinline__ void tc_m2l_back_group(const double* buf, const double* gz, int lane, cd ez1, cd ex1,
-                                                  double* acc, bool valid) {
-  tc_m2l_back<P, G>(buf, gz, lane, ez1, ex1, acc, valid);
-  if (G != P - G) tc_m2l_back<P, P - G>(buf, gz, lane, ez1, ex1, acc, valid);
-}
-
-template <int P, int G>
-struct TcM2LDispatch {
-  static __device__ __forceinline__ void fwd(int g, const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
-    if (g == G) tc_m2l_fwd_group<P, G>(Ms, ez1, ex1, buf, lane);
-    else TcM2LDispatch<P, G + 1>::fwd(g, Ms, ez1, ex1, buf, lane);
+// Warp w owns the degrees TcDegSets<P>::d[w][*] (balanced by a per-degree cost model), for
+// the same 32 pairs in every warp; each warp forms the pair geometry itself.
+template <int P, int W, int I>
+struct TcDegSeq {
+  static constexpr int D = TcDegSets<P>::d[W][I];
+  static __device__ __forceinline__ void fwd(const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
+    if constexpr (D >= 0) {
+      tc_m2l_fwd<P, D>(Ms, ez1, ex1, buf, lane);
+      TcDegSeq<P, W, I + 1>::fwd(Ms, ez1, ex1, buf, lane);
+    }
   }
-  static __device__ __forceinline__ void back(int g, const double* buf, const double* gz, int lane, cd ez1, cd ex1,
-                                              double* acc, bool valid) {
-    if (g == G) tc_m2l_back_group<P, G>(buf, gz, lane, ez1, ex1, acc, valid);
-    else TcM2LDispatch<P, G + 1>::back(g, buf, gz, lane, ez1, ex1, acc, valid);
+  static __device__ __forceinline__ void back(const double* buf, double rinv, int lane, cd ez1, cd ex1, double* acc,
+                                              bool valid) {
+    if constexpr (D >= 0) {
+      tc_m2l_back<P, D>(buf, rinv, lane, ez1, ex1, acc, valid);
+      TcDegSeq<P, W, I + 1>::back(buf, rinv, lane, ez1, ex1, acc, valid);
+    }
   }
-};
-template <int P>
-struct TcM2LDispatch<P, P / 2 + 1> {
-  static __device__ __forceinline__ void fwd(int, const double*, cd, cd, double*, int) {}
-  static __device__ __forceinline__ void back(int, const double*, const double*, int, cd, cd, double*, bool) {}
 };
 
 template <int P>
-constexpr int tc_m2l_threads() { return 32 * (P / 2 + 1); }
+__device__ __forceinline__ void tc_m2l_fwd_warp(int w, const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
+  if (w == 0) TcDegSeq<P, 0, 0>::fwd(Ms, ez1, ex1, buf, lane);
+  else if (w == 1) TcDegSeq<P, 1, 0>::fwd(Ms, ez1, ex1, buf, lane);
+  else if (w == 2) TcDegSeq<P, 2, 0>::fwd(Ms, ez1, ex1, buf, lane);
+  else TcDegSeq<P, 3, 0>::fwd(Ms, ez1, ex1, buf, lane);
+}
+template <int P>
+__device__ __forceinline__ void tc_m2l_back_warp(int w, const double* buf, double rinv, int lane, cd ez1, cd ex1,
+                                                 double* acc, bool valid) {
+  if (w == 0) TcDegSeq<P, 0, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
+  else if (w == 1) TcDegSeq<P, 1, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
+  else if (w == 2) TcDegSeq<P, 2, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
+  else TcDegSeq<P, 3, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
+}
+
+template <int P>
+constexpr int tc_m2l_threads() { return 128; }
 
 template <int P, bool JERK>
-__global__ void __launch_bounds__(tc_m2l_threads<P>(), (P >= 14 ? 1 : 2)) k_m2l(const int* __restrict__ tlist, int ntl,
-                                                                  const int* __restrict__ tstart,
-                                                                  const int* __restrict__ src, TcCells c) {
+__global__ void __launch_bounds__(128, 2) k_m2l(const int* __restrict__ tlist, int ntl,
+                                               const int* __restrict__ tstart,
+                                               const int* __restrict__ src, TcCells c) {
   using SM = TcM2LSmem<P>;
   constexpr int NT = SM::NT;
   extern __shared__ double tc_m2l_smem[];
   double* buf = tc_m2l_smem + SM::BUF;
   double* acc = tc_m2l_smem + SM::ACC;
-  double* gz = tc_m2l_smem + SM::GZ;
-  double* geo = tc_m2l_smem + SM::GEO;
   int ti = blockIdx.x;
   if (ti >= ntl) return;
   int t = tlist[ti];
   if (!c.has_sink[t]) return;
-  const int g = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int s_beg = tstart[t], s_end = tstart[t + 1];
   const double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
   for (int arr = 0; arr < (JERK ? 2 : 1); arr++) {
@@ -193,28 +208,10 @@ __global__ void __launch_bounds__(tc_m2l_threads<P>(), (P >= 14 ? 1 : 2)) k_m2l(
       int idx = b0 + lane;
       bool valid = idx < s_end;
       int s = src[valid ? idx : s_beg];
-      cd ez1, ex1;
-      if (g == 0) {
-        TcPairGeo pg = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
-        ez1 = pg.ez1;
-        ex1 = pg.ex1;
-        geo[0 * 32 + lane] = ez1.x; geo[1 * 32 + lane] = ez1.y;
-        geo[2 * 32 + lane] = ex1.x; geo[3 * 32 + lane] = ex1.y;
-        double pr = pg.rinv;
-#pragma unroll
-        for (int j = 0; j <= P; j++) {
-          gz[j * 32 + lane] = c_fact[j] * pr;
-          pr *= pg.rinv;
-        }
-      }
+      TcPairGeo pg = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
+      tc_m2l_fwd_warp<P>(w, Mbase + (size_t)s * NT, pg.ez1, pg.ex1, buf, lane);
       tc_bar_cta();
-      if (g != 0) {
-        ez1 = mk(geo[0 * 32 + lane], geo[1 * 32 + lane]);
-        ex1 = mk(geo[2 * 32 + lane], geo[3 * 32 + lane]);
-      }
-      TcM2LDispatch<P, 0>::fwd(g, Mbase + (size_t)s * NT, ez1, ex1, buf, lane);
-      tc_bar_cta();
-      TcM2LDispatch<P, 0>::back(g, buf, gz, lane, ez1, ex1, acc, valid);
+      tc_m2l_back_warp<P>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, acc, valid);
       tc_bar_cta();
     }
     double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NT;

@@ -144,8 +144,11 @@ struct TcM2LXDispatch<P, P / 2 + 1> {
                                               bool) {}
 };
 
+template <int P>
+constexpr int tc_m2lx_threads() { return 32 * (P / 2 + 1); }
+
 template <int P, bool JERK>
-__global__ void __launch_bounds__(tc_m2l_threads<P>(), 2) k_m2l_mixed(const int* __restrict__ tlist, int ntl,
+__global__ void __launch_bounds__(tc_m2lx_threads<P>(), 2) k_m2l_mixed(const int* __restrict__ tlist, int ntl,
                                                                         const int* __restrict__ tstart,
                                                                         const int* __restrict__ src, TcCells c) {
   using SM = TcM2LMixSmem<P>;

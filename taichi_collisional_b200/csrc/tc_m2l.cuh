@@ -91,42 +91,48 @@ __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1
 
 // translation along z to output degree N, then rotation back; accumulate into the lane's
 // column of the shared accumulator.  Factors (n+k)! / r^(n+k+1) are formed on the fly.
+// Pair batches processed at once by one CTA (each batch by 4 warps); limited by shared memory.
+template <int P>
+struct TcM2LGroups {
+  static constexpr int G = (P >= 14) ? 1 : 2;
+};
+
 template <int P, int N>
 __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int lane, cd ez1, cd ex1,
-                                            double* acc, bool valid) {
+                                            double* acc, int acol, bool valid) {
   double l[2 * N + 1], o[2 * N + 1];
 #pragma unroll
   for (int k = 0; k < 2 * N + 1; k++) l[k] = 0.0;
   double pn = rinv;
 #pragma unroll
   for (int j = 0; j < N; j++) pn *= rinv;  // rinv^(N+1)
-  double fk[P - N + 1];                    // (N+k)! rinv^(N+k+1)
+  // the k loops stay rolled: the translation is a quarter of the unrolled code otherwise
   {
-    double pr = pn;
-#pragma unroll
+    double s = 0.0, pr = pn;
+#pragma unroll 1
     for (int k = 0; k <= P - N; k++) {
-      fk[k] = c_fact[N + k] * pr;
+      s += buf[(k * k + k) * 32 + lane] * (c_fact[N + k] * pr);
       pr *= rinv;
     }
-  }
-  {
-    double s = 0.0;
-#pragma unroll
-    for (int k = 0; k <= P - N; k++) s += buf[(k * k + k) * 32 + lane] * fk[k];
     l[N] = s;
   }
   constexpr int MMAX = N < P - N ? N : P - N;
+  double pm = rinv;
 #pragma unroll
   for (int m = 1; m <= MMAX; m++) {
-    double sn = 0.0, sp = 0.0;
-#pragma unroll
+    double sn = 0.0, sp = 0.0, pr = pn * pm;
+#pragma unroll 1
     for (int k = m; k <= P - N; k++) {
-      sn += buf[(k * k + k - m) * 32 + lane] * fk[k];
-      sp += buf[(k * k + k + m) * 32 + lane] * fk[k];
+      const double f = c_fact[N + k] * pr;
+      const int b = (k * k + k) * 32 + lane;
+      sn += buf[b - m * 32] * f;
+      sp += buf[b + m * 32] * f;
+      pr *= rinv;
     }
     const double sg = (m & 1) ? -1.0 : 1.0;
     l[N - m] = sg * sn;
     l[N + m] = sg * sp;
+    pm *= rinv;
   }
   TcSwapDeg<N>::apply(l, o);
   tc_rot_inv<N>(o, ex1);
@@ -134,20 +140,22 @@ __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int 
   tc_rot_inv<N>(l, ez1);
   if (valid) {
 #pragma unroll
-    for (int k = 0; k < 2 * N + 1; k++) acc[(N * N + k) * 32 + lane] += l[k];
+    for (int k = 0; k < 2 * N + 1; k++) acc[(N * N + k) * (32 * TcM2LGroups<P>::G) + acol] += l[k];
   }
 }
 
-// shared-memory layout of one M2L CTA (doubles): buf | acc
+// shared-memory layout of one M2L CTA (doubles): buf[G groups] | acc (32 G columns)
 template <int P>
 struct TcM2LSmem {
   static constexpr int NT = (P + 1) * (P + 1);
-  static constexpr int BUF = 0, ACC = NT * 32;
-  static constexpr int TOTAL = 2 * NT * 32;
+  static constexpr int G = TcM2LGroups<P>::G;
+  static constexpr int BUF = 0, ACC = G * NT * 32;
+  static constexpr int TOTAL = G * NT * 32 + NT * 32 * G;
 };
 
-// Warp w owns the degrees TcDegSets<P>::d[w][*] (balanced by a per-degree cost model), for
-// the same 32 pairs in every warp; each warp forms the pair geometry itself.
+// Warp w of each 4-warp group owns the degrees TcDegSets<P>::d[w][*] (balanced by a
+// per-degree cost model) for the group's 32 pairs; warps w and w + 4 run the same degree code,
+// which keeps each SM sub-partition's instruction working set to one degree set.
 template <int P, int W, int I>
 struct TcDegSeq {
   static constexpr int D = TcDegSets<P>::d[W][I];
@@ -158,10 +166,10 @@ struct TcDegSeq {
     }
   }
   static __device__ __forceinline__ void back(const double* buf, double rinv, int lane, cd ez1, cd ex1, double* acc,
-                                              bool valid) {
+                                              int acol, bool valid) {
     if constexpr (D >= 0) {
-      tc_m2l_back<P, D>(buf, rinv, lane, ez1, ex1, acc, valid);
-      TcDegSeq<P, W, I + 1>::back(buf, rinv, lane, ez1, ex1, acc, valid);
+      tc_m2l_back<P, D>(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+      TcDegSeq<P, W, I + 1>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
     }
   }
 };
@@ -175,50 +183,58 @@ __device__ __forceinline__ void tc_m2l_fwd_warp(int w, const double* Ms, cd ez1,
 }
 template <int P>
 __device__ __forceinline__ void tc_m2l_back_warp(int w, const double* buf, double rinv, int lane, cd ez1, cd ex1,
-                                                 double* acc, bool valid) {
-  if (w == 0) TcDegSeq<P, 0, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
-  else if (w == 1) TcDegSeq<P, 1, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
-  else if (w == 2) TcDegSeq<P, 2, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
-  else TcDegSeq<P, 3, 0>::back(buf, rinv, lane, ez1, ex1, acc, valid);
+                                                 double* acc, int acol, bool valid) {
+  if (w == 0) TcDegSeq<P, 0, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+  else if (w == 1) TcDegSeq<P, 1, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+  else if (w == 2) TcDegSeq<P, 2, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+  else TcDegSeq<P, 3, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+}
+
+__device__ __forceinline__ void tc_bar_group(int grp) {
+  asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
 }
 
 template <int P>
-constexpr int tc_m2l_threads() { return 128; }
+constexpr int tc_m2l_threads() { return 128 * TcM2LGroups<P>::G; }
 
 template <int P, bool JERK>
-__global__ void __launch_bounds__(128, 2) k_m2l(const int* __restrict__ tlist, int ntl,
+__global__ void __launch_bounds__(tc_m2l_threads<P>(), 1) k_m2l(const int* __restrict__ tlist, int ntl,
                                                const int* __restrict__ tstart,
                                                const int* __restrict__ src, TcCells c) {
   using SM = TcM2LSmem<P>;
   constexpr int NT = SM::NT;
+  constexpr int G = SM::G;
   extern __shared__ double tc_m2l_smem[];
-  double* buf = tc_m2l_smem + SM::BUF;
   double* acc = tc_m2l_smem + SM::ACC;
   int ti = blockIdx.x;
   if (ti >= ntl) return;
   int t = tlist[ti];
   if (!c.has_sink[t]) return;
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int grp = warp >> 2, w = warp & 3, acol = grp * 32 + lane;
+  double* buf = tc_m2l_smem + SM::BUF + grp * NT * 32;
   const int s_beg = tstart[t], s_end = tstart[t + 1];
   const double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
   for (int arr = 0; arr < (JERK ? 2 : 1); arr++) {
     const double* Mbase = arr ? c.Md : c.M;
-    for (int i = threadIdx.x; i < NT * 32; i += blockDim.x) acc[i] = 0.0;
-    for (int b0 = s_beg; b0 < s_end; b0 += 32) {
+    for (int i = threadIdx.x; i < NT * 32 * G; i += blockDim.x) acc[i] = 0.0;
+    tc_bar_cta();
+    for (int b0 = s_beg + grp * 32; b0 < s_end; b0 += 32 * G) {
       int idx = b0 + lane;
       bool valid = idx < s_end;
       int s = src[valid ? idx : s_beg];
       TcPairGeo pg = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
       tc_m2l_fwd_warp<P>(w, Mbase + (size_t)s * NT, pg.ez1, pg.ex1, buf, lane);
-      tc_bar_cta();
-      tc_m2l_back_warp<P>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, acc, valid);
-      tc_bar_cta();
+      tc_bar_group(grp);
+      tc_m2l_back_warp<P>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, acc, acol, valid);
+      tc_bar_group(grp);
     }
+    tc_bar_cta();
     double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NT;
     for (int r = threadIdx.x; r < NT; r += blockDim.x) {
       double v = 0.0;
 #pragma unroll 8
-      for (int q = 0; q < 32; q++) v += acc[r * 32 + q];
+      for (int q = 0; q < 32 * G; q++) v += acc[r * (32 * G) + q];
       Lt[r] = v;
     }
     tc_bar_cta();

@@ -42,7 +42,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
     ap.add_argument("--p", type=int, default=WORKLOAD["p"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_m2l"])
+    ap.add_argument("--judge", type=int, default=256, help="bodies checked against FP64 direct sums each step")
+    ap.add_argument("--no-fp64-arm", action="store_true", help="skip timing the plain FP64 form alongside")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -202,8 +204,9 @@ def main():
     T = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)  # noqa: E731
     st = {k: T(a) for k, a in zip(("x", "y", "z", "vx", "vy", "vz", "m"), (x, y, z, vx, vy, vz, m))}
     out = {k: torch.empty(n, dtype=torch.float64, device=dev) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
+    prec = {"fp64": tcb.PREC_FP64, "mixed": tcb.PREC_MIXED, "mixed_m2l": tcb.PREC_MIXED_M2L}[args.precision]
     g = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
-                    precision=tcb.PREC_FP64 if args.precision == "fp64" else tcb.PREC_MIXED, device=local)
+                    precision=prec, device=local, judge_n=args.judge)
     dt = 1.0 / 4096
 
     def evaluate():
@@ -246,6 +249,32 @@ def main():
         ms = float(t.item())
     value = world * n * args.steps / (ms * 1e-3)
     stats = g.stats()
+
+    # ---- the plain FP64 form on the same state, same timing rules (the comparison arm)
+    fp64 = None
+    if not args.no_fp64_arm and args.precision != "fp64":
+        g64 = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
+                          precision=tcb.PREC_FP64, device=local, judge_n=args.judge)
+        out64 = {k: torch.empty_like(v) for k, v in out.items()}
+        g64.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"], out=out64)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        h0.record()
+        for _ in range(args.steps):
+            g64.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"], out=out64)
+        h1.record()
+        torch.cuda.synchronize()
+        ms64 = h0.elapsed_time(h1)
+        if dist:
+            t = torch.tensor([ms64], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms64 = float(t.item())
+        s64 = g64.stats()
+        fp64 = {"value": world * n * args.steps / (ms64 * 1e-3), "ms_per_eval": ms64 / args.steps,
+                "judge_rms_acc_err": s64["judge_rms"], "note": "force evaluations only (no kick/drift)"}
+        g64.close()
 
     # ---- end to end through the public API: pinned host state in, results out, every step
     e2e = None
@@ -305,6 +334,8 @@ def main():
                 "config": dict(WORKLOAD, n=n, p=p, precision=args.precision,
                                parallelism="replicas" if world > 1 else "single"),
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb, "clocks": clocks,
+                "accuracy": {"judge_bodies": args.judge, "rms_rel_acc_err_vs_fp64_direct": stats["judge_rms"]},
+                "fp64_form": fp64,
                 "lists": {"cells": stats["n_cells"], "m2l_pairs": stats["n_m2l"], "p2p_pairs": stats["n_p2p"],
                           "p2p_interactions": stats["n_p2p_inter"], "max_level": stats["max_level"],
                           "flags": stats["flags"]}}

@@ -41,7 +41,10 @@ typedef enum {
 } tc_status;
 
 typedef enum { TC_VARIANT_TOP = 0, TC_VARIANT_JERKS = 1 } tc_variant;
-typedef enum { TC_PREC_FP64 = 0, TC_PREC_MIXED = 1 } tc_precision;
+/* TC_PREC_FP64: every stage FP64 (parity with the reference at 1e-12).
+ * TC_PREC_MIXED: near field (P2P) in FP32 with compensated sums, far field FP64.
+ * TC_PREC_MIXED_M2L: near field as MIXED, and the M2L rotations in FP32 as well. */
+typedef enum { TC_PREC_FP64 = 0, TC_PREC_MIXED = 1, TC_PREC_MIXED_M2L = 2 } tc_precision;
 typedef enum { TC_MEM_HOST = 0, TC_MEM_DEVICE = 1 } tc_memory;
 
 typedef struct {
@@ -55,6 +58,15 @@ typedef struct {
   int direct_below;   /* N below this -> direct sum; -1 = reference rule (top: ncrit,
                          jerks: 8000; integrator.h:462, taichi_with_jerks/integrator.h:311) */
   int device;         /* CUDA device ordinal                                               */
+  int selector;       /* far-field order per pair: 0 fixed p (the reference), 1 analytic error
+                         estimate (the reference's MAC estimate, traverse_eager.h:82-96),
+                         2 learned (MLP, after tc_train_selector)                         */
+  double selector_tol;/* per-pair tolerance: |acc error| <= tol * M_source / r^2            */
+  int judge_n;        /* >0: after each evaluation, FP64 direct sums at judge_n seeded bodies;
+                         with a selector, an RMS relative acceleration error above judge_tol
+                         makes the call redo the far field at the fixed order p             */
+  double judge_tol;
+  unsigned long long judge_seed;
 } tc_params;
 
 typedef struct {
@@ -64,6 +76,12 @@ typedef struct {
   long long n_launches; /* kernels launched by the last tc_evaluate */
   long long flags;      /* diagnostic bits of the last evaluation (1 M2L, 2 P2P, 4 frontier capacity
                            retries; 8 depth limit; 16 an enclosing ball hit its iteration cap) */
+  int n_classes;                /* far-field order classes used by the last evaluation     */
+  int class_order[6];           /* their orders                                            */
+  long long class_pairs[6];     /* M2L pairs evaluated at each order                       */
+  double m2l_flop_fraction;     /* sum over pairs of (q+1)^3 / (p+1)^3, divided by pairs   */
+  double judge_rms;             /* RMS relative acceleration error at the judge's bodies   */
+  int judge_redo;               /* 1 if the judge rejected the selector's step             */
 } tc_stats;
 
 typedef struct tc_ctx tc_ctx;
@@ -103,6 +121,39 @@ tc_status tc_get_cells(tc_ctx* ctx, int* begin, int* nbody, int* nchild, int* ch
                        double* X /* 3 per cell */, double* R, int* perm /* n */);
 tc_status tc_get_lists(tc_ctx* ctx, int kind, int* tgt, int* src);
 tc_status tc_get_expansions(tc_ctx* ctx, double* M, double* Md, double* L, double* Ld);
+
+/* ---- learned far-field order selector (selector = 2) ----------------------------------- */
+typedef struct {
+  int samples, iters, n_classes;
+  int class_order[6];
+  double train_loss, val_loss; /* mean squared error of predicted log10 errors            */
+  double seconds;
+} tc_train_report;
+
+/* Train the selector's network on pairs from this input: one fixed-order evaluation builds
+ * the tree and lists, `nsamples` M2L pairs are drawn (seeded), each is evaluated at every
+ * order class against exact P2P, and the 3x32 MLP is fitted with Adam for `iters` steps on
+ * the GPU.  The weights stay in the context (tc_get/set_selector_weights). */
+tc_status tc_train_selector(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz, const double* m,
+                            int mem, int nsamples, int iters, unsigned long long seed,
+                            tc_train_report* rep);
+/* Change the selector mode and tolerance of an existing context (tc_params.selector/_tol). */
+tc_status tc_set_selector(tc_ctx* ctx, int selector, double tol);
+/* Training data of the last tc_train_selector (host copies): features [n x 8] and labels
+ * [n x n_classes] (log10 relative errors).  Pass NULL to query *n. */
+tc_status tc_get_selector_data(tc_ctx* ctx, float* feat, float* labels, int* n, int* n_classes);
+/* Network parameters + standardisation (8 means, 8 inverse deviations, output offset):
+ * `w` holds tc_selector_nparam() floats, `norm` 17 floats. */
+int tc_selector_nparam(tc_ctx* ctx);
+tc_status tc_get_selector_weights(tc_ctx* ctx, float* w, float* norm);
+tc_status tc_set_selector_weights(tc_ctx* ctx, const float* w, const float* norm);
+/* One evaluation of the training loss and its gradient on the current device (host arrays),
+ * for checking the hand-written backward pass. */
+tc_status tc_mlp_loss_grad(int ns, int n_out, const float* feat, const float* labels, const float* w,
+                           const float* norm, float* grad, float* loss);
+/* Predicted log10 errors [ns x n_out] of the network for given features (host arrays). */
+tc_status tc_mlp_predict(int ns, int n_out, const float* feat, const float* w, const float* norm, float* pred);
 
 /* FP64 leapfrog update on device arrays (the integrator step around each evaluation):
  *   v += a * dt_kick;  x += v * dt_drift

@@ -20,7 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libtaichi_b200.so")
 
 VARIANT_TOP, VARIANT_JERKS = 0, 1
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_MIXED_M2L = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "capacity exceeded", 4: "non-finite input",
@@ -34,7 +34,9 @@ _u8p = C.POINTER(C.c_ubyte)
 class Params(C.Structure):
     _fields_ = [("p", C.c_int), ("ncrit", C.c_int), ("theta", C.c_double), ("variant", C.c_int),
                 ("precision", C.c_int), ("use_shift", C.c_int), ("shift_u", C.c_double * 3),
-                ("direct_below", C.c_int), ("device", C.c_int)]
+                ("direct_below", C.c_int), ("device", C.c_int), ("selector", C.c_int),
+                ("selector_tol", C.c_double), ("judge_n", C.c_int), ("judge_tol", C.c_double),
+                ("judge_seed", C.c_ulonglong)]
 
 
 class Stats(C.Structure):
@@ -43,12 +45,21 @@ class Stats(C.Structure):
                 ("max_level", C.c_int), ("ms_total", C.c_double), ("ms_tree", C.c_double),
                 ("ms_upward", C.c_double), ("ms_traverse", C.c_double), ("ms_m2l", C.c_double),
                 ("ms_p2p", C.c_double), ("ms_downward", C.c_double), ("n_launches", C.c_longlong),
-                ("flags", C.c_longlong)]
+                ("flags", C.c_longlong), ("n_classes", C.c_int), ("class_order", C.c_int * 6),
+                ("class_pairs", C.c_longlong * 6), ("m2l_flop_fraction", C.c_double), ("judge_rms", C.c_double),
+                ("judge_redo", C.c_int)]
+
+
+class TrainReport(C.Structure):
+    _fields_ = [("samples", C.c_int), ("iters", C.c_int), ("n_classes", C.c_int), ("class_order", C.c_int * 6),
+                ("train_loss", C.c_double), ("val_loss", C.c_double), ("seconds", C.c_double)]
 
 
 EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_evaluate", "tc_get_stats",
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
-           "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc"]
+           "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
+           "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -96,6 +107,24 @@ def load_library(path=LIB_PATH):
     L.tc_probe_peak.restype = C.c_double
     L.tc_evaluate_direct_noalloc.argtypes = [C.c_int] + [C.c_void_p] * 8 + [C.c_void_p] * 7 + [C.c_int, C.c_void_p]
     L.tc_evaluate_direct_noalloc.restype = C.c_int
+    _fp = C.POINTER(C.c_float)
+    L.tc_train_selector.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 7 + [C.c_int, C.c_int, C.c_int,
+                                                                               C.c_ulonglong, C.POINTER(TrainReport)]
+    L.tc_train_selector.restype = C.c_int
+    L.tc_get_selector_data.argtypes = [C.c_void_p, _fp, _fp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.tc_get_selector_data.restype = C.c_int
+    L.tc_selector_nparam.argtypes = [C.c_void_p]
+    L.tc_selector_nparam.restype = C.c_int
+    L.tc_get_selector_weights.argtypes = [C.c_void_p, _fp, _fp]
+    L.tc_get_selector_weights.restype = C.c_int
+    L.tc_set_selector_weights.argtypes = [C.c_void_p, _fp, _fp]
+    L.tc_set_selector_weights.restype = C.c_int
+    L.tc_mlp_loss_grad.argtypes = [C.c_int, C.c_int, _fp, _fp, _fp, _fp, _fp, _fp]
+    L.tc_mlp_loss_grad.restype = C.c_int
+    L.tc_mlp_predict.argtypes = [C.c_int, C.c_int, _fp, _fp, _fp, _fp]
+    L.tc_mlp_predict.restype = C.c_int
+    L.tc_set_selector.argtypes = [C.c_void_p, C.c_int, C.c_double]
+    L.tc_set_selector.restype = C.c_int
     _lib = L
     return L
 
@@ -133,10 +162,13 @@ class Gravity:
     """
 
     def __init__(self, p=12, ncrit=64, theta=0.4, variant=VARIANT_JERKS, precision=PREC_FP64, shift_u=None,
-                 direct_below=-1, device=0):
+                 direct_below=-1, device=0, selector=0, selector_tol=1e-9, judge_n=0, judge_tol=0.0,
+                 judge_seed=12345):
         self._L = load_library()
         self.params = default_params(p=p, ncrit=ncrit, theta=theta, variant=variant, precision=precision,
-                                     shift_u=shift_u, direct_below=direct_below, device=device)
+                                     shift_u=shift_u, direct_below=direct_below, device=device, selector=selector,
+                                     selector_tol=selector_tol, judge_n=judge_n, judge_tol=judge_tol,
+                                     judge_seed=judge_seed)
         h = C.c_void_p()
         rc = self._L.tc_create(C.byref(self.params), C.byref(h))
         if rc != 0:
@@ -198,10 +230,60 @@ class Gravity:
         """Measured FMA throughput of this GPU in GFLOP/s (0: FP64, 1: FP32)."""
         return self._L.tc_probe_peak(self._h, kind)
 
+    def train_selector(self, x, y, z, m, vx=None, vy=None, vz=None, nsamples=16384, iters=2000, seed=1):
+        """Fit the learned order selector on pairs of this input (tc_train_selector)."""
+        dev = hasattr(x, "data_ptr")
+        if not dev:
+            x, y, z, m = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, m))
+            if vx is not None:
+                vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64) for a in (vx, vy, vz))
+        rep = TrainReport()
+        rc = self._L.tc_train_selector(self._h, len(x), _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy), _ptr(vz),
+                                       _ptr(m), MEM_DEVICE if dev else MEM_HOST, int(nsamples), int(iters),
+                                       int(seed), C.byref(rep))
+        self._check(rc, "tc_train_selector")
+        out = {f: getattr(rep, f) for f, _ in TrainReport._fields_}
+        out["class_order"] = list(rep.class_order)[:rep.n_classes]
+        return out
+
+    def selector_data(self):
+        n, nc = C.c_int(), C.c_int()
+        self._L.tc_get_selector_data(self._h, None, None, C.byref(n), C.byref(nc))
+        f = np.zeros((n.value, 8), dtype=np.float32)
+        lab = np.zeros((n.value, nc.value), dtype=np.float32)
+        fp = C.POINTER(C.c_float)
+        self._L.tc_get_selector_data(self._h, f.ctypes.data_as(fp), lab.ctypes.data_as(fp), C.byref(n), C.byref(nc))
+        return f, lab
+
+    def selector_weights(self):
+        npar = self._L.tc_selector_nparam(self._h)
+        w = np.zeros(npar, dtype=np.float32)
+        norm = np.zeros(17, dtype=np.float32)
+        fp = C.POINTER(C.c_float)
+        self._check(self._L.tc_get_selector_weights(self._h, w.ctypes.data_as(fp), norm.ctypes.data_as(fp)),
+                    "tc_get_selector_weights")
+        return w, norm
+
+    def set_selector_weights(self, w, norm):
+        fp = C.POINTER(C.c_float)
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        norm = np.ascontiguousarray(norm, dtype=np.float32)
+        self._check(self._L.tc_set_selector_weights(self._h, w.ctypes.data_as(fp), norm.ctypes.data_as(fp)),
+                    "tc_set_selector_weights")
+
+    def set_selector(self, selector, tol):
+        """Switch the far-field order selector of this context (0 fixed, 1 analytic, 2 learned)."""
+        self._check(self._L.tc_set_selector(self._h, int(selector), float(tol)), "tc_set_selector")
+        self.params.selector = selector
+        self.params.selector_tol = tol
+
     def stats(self):
         st = Stats()
         self._L.tc_get_stats(self._h, C.byref(st))
-        return {f: getattr(st, f) for f, _ in Stats._fields_}
+        out = {f: getattr(st, f) for f, _ in Stats._fields_}
+        out["class_order"] = list(st.class_order)[:st.n_classes]
+        out["class_pairs"] = list(st.class_pairs)[:st.n_classes]
+        return out
 
     def cells(self):
         st = self.stats()

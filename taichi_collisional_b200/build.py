@@ -7,7 +7,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtaichi_b200.so")
 SOURCES = ["tc_lib.cu", "tc_common.cuh", "tc_tree.cuh", "tc_upward.cuh", "tc_traverse.cuh", "tc_m2l.cuh", "tc_m2l_mixed.cuh",
-           "tc_down.cuh", "tc_p2p.cuh", "tc_harmonics.cuh", "swap_tables.h", "tdesign.h", "m2l_schedule.h"]
+           "tc_down.cuh", "tc_p2p.cuh", "tc_harmonics.cuh", "swap_tables.h", "tdesign.h", "m2l_schedule.h", "tc_select.cuh", "tc_mlp.cuh", "tc_train.cuh"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 

@@ -59,6 +59,38 @@ struct TcOut {
   double *pot, *ax, *ay, *az, *jx, *jy, *jz;  // Morton order
 };
 
+// acceleration of one body from a local expansion held as complex full storage `sl`
+// (dX = cell centre - body), the non-jerk part of the L2P below
+template <int P>
+__device__ __forceinline__ void tc_l2p_acc(const cd* sl, double dx, double dy, double dz, double* a) {
+  double r2 = dx * dx + dy * dy + dz * dz;
+  cd p10 = mk(0, 0), p11 = mk(0, 0);
+  for (int m = 0; m <= P; m++) {
+    double sgn = (m & 1) ? -1.0 : 1.0;
+    cd d0 = mk(1, 0);
+    for (int j = 1; j <= m; j++) d0 = d0 * mk(dx / (2 * j), dy / (2 * j));
+    TcCol col;
+    col.init(m, d0);
+#pragma unroll
+    for (int n = 0; n <= P; n++) {
+      cd gb = col.step(n, dz, r2);
+      if (n >= m && n <= P - 1) {
+        cd cgp = conj(gb), cgn = sgn * gb;
+        int k1 = (n + 1) * (n + 1) + (n + 1);
+        p10 += sl[k1 + m] * cgp;
+        p11 += sl[k1 + 1 + m] * cgp;
+        if (m > 0) {
+          p10 += sl[k1 - m] * cgn;
+          p11 += sl[k1 + 1 - m] * cgn;
+        }
+      }
+    }
+  }
+  a[0] = -p11.x;
+  a[1] = -p11.y;
+  a[2] = -p10.x;
+}
+
 // L2P for every leaf; one warp per leaf, one lane per body
 template <int P, bool JERK>
 __global__ void __launch_bounds__(kUpWarps * 32) k_l2p(const int* __restrict__ leaves, int nleaf, const TcBodies b,

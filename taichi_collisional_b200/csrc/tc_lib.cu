@@ -14,6 +14,9 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
+#include <chrono>
+#include <random>
 #include <string>
 #include <vector>
 
@@ -25,6 +28,9 @@
 #include "tc_m2l_mixed.cuh"
 #include "tc_down.cuh"
 #include "tc_p2p.cuh"
+#include "tc_select.cuh"
+#include "tc_mlp.cuh"
+#include "tc_train.cuh"
 #include "tdesign.h"
 
 using namespace tc;
@@ -86,6 +92,22 @@ struct tc_ctx {
   DBuf<int2> front[2];
   DBuf<unsigned long long> m2l, m2l_alt, p2p, p2p_alt;
   DBuf<int> m2l_start, m2l_src, p2p_start, p2p_src, m2l_tl, p2p_tl, leaves;
+  DBuf<double> cell_pn;
+  DBuf<int> cls_start, cls_tl;  // per order class: per-target offsets and target lists
+  int n_classes = 0, class_order[TC_MAX_CLASSES];
+  long long class_pairs[TC_MAX_CLASSES];
+  double flop_frac = 1.0;
+  // learned selector
+  bool mlp_ready = false;
+  int mlp_nout = 0;
+  DBuf<float> mlp_w;
+  TcMlpNorm mlp_norm;
+  std::vector<float> train_feat, train_lab;
+  int train_n = 0;
+  double judge_rms = 0.0;
+  int judge_redo = 0;
+  DBuf<int> judge_idx;
+  DBuf<double> judge_out;
   size_t fcap = 0, mcap = 0, pcap = 0;
   // small device structs
   TcRootInfo* d_root = nullptr;
@@ -241,6 +263,243 @@ __global__ void k_p2p_count(const unsigned long long* __restrict__ keys, unsigne
 }
 
 // ----------------------------------------------------------------------------------------
+// far field with a per-pair order (tc_select.cuh): classify, re-sort by class, one launch per
+// class
+// ----------------------------------------------------------------------------------------
+template <int P, int I, bool JERK>
+struct TcClassLaunch {
+  static void run(int cls, int ntl, const int* tl, const int* tstart, const int* src, TcCells cv, cudaStream_t st) {
+    if constexpr (I < TcOrderClasses<P>::n) {
+      if (cls == I) {
+        constexpr int Q = TcOrderClasses<P>::q[I];
+        size_t smem = (size_t)TcM2LSmem<Q>::TOTAL * sizeof(double);
+        k_m2l<P, Q, JERK><<<ntl, tc_m2l_threads<Q>(), smem, st>>>(tl, ntl, tstart, src, cv);
+      } else {
+        TcClassLaunch<P, I + 1, JERK>::run(cls, ntl, tl, tstart, src, cv, st);
+      }
+    }
+  }
+  static void attrs() {
+    if constexpr (I < TcOrderClasses<P>::n) {
+      constexpr int Q = TcOrderClasses<P>::q[I];
+      size_t smem = (size_t)TcM2LSmem<Q>::TOTAL * sizeof(double);
+      cudaFuncSetAttribute(k_m2l<P, Q, JERK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      TcClassLaunch<P, I + 1, JERK>::attrs();
+    }
+  }
+};
+
+template <int P, bool JERK>
+static cudaError_t run_m2l_classes(tc_ctx* ctx, TcCells cv) {
+  using OC = TcOrderClasses<P>;
+  cudaStream_t st = ctx->stream;
+  const int nc = ctx->ncell, sbits = ctx->sbits;
+  const unsigned long long nm = ctx->n_m2l;
+  cudaError_t e;
+  if ((e = ctx->cell_pn.ensure((size_t)nc * (P + 1))) != cudaSuccess) return e;
+  if ((e = ctx->cls_start.ensure((size_t)OC::n * (nc + 1))) != cudaSuccess) return e;
+  if ((e = ctx->cls_tl.ensure((size_t)OC::n * nc)) != cudaSuccess) return e;
+  k_cell_pn<P><<<nblocks(nc, 128), 128, 0, st>>>(nc, cv.M, ctx->cell_pn.p);
+  if ((e = cudaMemsetAsync(ctx->d_small, 0, 4 * sizeof(unsigned) * 2, st)) != cudaSuccess) return e;
+  unsigned* d_hist = ctx->d_small;  // TC_MAX_CLASSES counters (d_small holds 8)
+  if (ctx->prm.selector == 2) {
+    if (!ctx->mlp_ready || ctx->mlp_nout != OC::n) return cudaErrorInvalidValue;
+    k_select_mlp<P><<<148 * 8, 256, 0, st>>>(ctx->m2l.p, nm, sbits, cv, ctx->cell_pn.p, ctx->mlp_w.p, ctx->mlp_norm,
+                                             (float)log10(ctx->prm.selector_tol), ctx->m2l_alt.p, d_hist);
+  } else {
+    k_select_analytic<P><<<148 * 8, 256, 0, st>>>(ctx->m2l.p, nm, sbits, cv, ctx->cell_pn.p, ctx->prm.selector_tol,
+                                                  ctx->m2l_alt.p, d_hist);
+  }
+  // stable sort by class: one radix pass over the class bits keeps (target, source) order
+  ctx->launches += 2 + radix_sort(ctx->m2l_alt.p, nullptr, ctx->m2l.p, nullptr, (int)nm, 2 * sbits + 8,
+                                  ctx->hist.p, st, 2 * sbits);
+  unsigned hcnt[8];
+  if ((e = cudaMemcpyAsync(hcnt, d_hist, sizeof(hcnt), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+  k_strip_class<<<148 * 8, 256, 0, st>>>(ctx->m2l_alt.p, nm, sbits);
+  ctx->n_classes = OC::n;
+  unsigned long long off = 0;
+  double ff = 0.0;
+  for (int i = 0; i < OC::n; i++) {
+    ctx->class_order[i] = OC::q[i];
+    ctx->class_pairs[i] = hcnt[i];
+    double q1 = OC::q[i] + 1.0, p1 = P + 1.0;
+    ff += hcnt[i] * (q1 * q1 * q1) / (p1 * p1 * p1);
+    int* cs = ctx->cls_start.p + (size_t)i * (nc + 1);
+    int* tl = ctx->cls_tl.p + (size_t)i * nc;
+    if (hcnt[i] == 0) {
+      off += hcnt[i];
+      continue;
+    }
+    k_list_csr<<<148 * 8, 256, 0, st>>>(ctx->m2l_alt.p + off, hcnt[i], nc, sbits, cs, ctx->m2l_src.p + off);
+    if ((e = cudaMemsetAsync(ctx->d_small + 7, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
+    k_list_targets<<<nblocks(nc, 256), 256, 0, st>>>(cs, nc, tl, ctx->d_small + 7);
+    unsigned ntl = 0;
+    if ((e = cudaMemcpyAsync(&ntl, ctx->d_small + 7, sizeof(unsigned), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+      return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    if (ntl) TcClassLaunch<P, 0, JERK>::run(i, (int)ntl, tl, cs, ctx->m2l_src.p + off, cv, st);
+    ctx->launches += 3;
+    off += hcnt[i];
+  }
+  ctx->flop_frac = nm ? ff / (double)nm : 1.0;
+  // the class-ordered list stays in m2l_alt; restore the (target, source) order for inspection
+  return cudaGetLastError();
+}
+
+// ----------------------------------------------------------------------------------------
+// learned selector: training data from the FMM, then Adam on the GPU
+// ----------------------------------------------------------------------------------------
+template <int P, int I>
+struct TcClassPairs {
+  static void run(int K, const int* pt, const int* ps, TcCells cv, double* Lcls, cudaStream_t st) {
+    if constexpr (I < TcOrderClasses<P>::n) {
+      constexpr int Q = TcOrderClasses<P>::q[I];
+      constexpr int NTQ = (Q + 1) * (Q + 1), G = TcM2LGroups<Q>::G;
+      size_t smem = (size_t)(NTQ * 32 + NTQ * 32 * G) * sizeof(double);
+      cudaFuncSetAttribute(k_m2l_pairs<P, Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_m2l_pairs<P, Q><<<(K + 31) / 32, 128, smem, st>>>(K, pt, ps, cv, Lcls + (size_t)I * K * (P + 1) * (P + 1));
+      TcClassPairs<P, I + 1>::run(K, pt, ps, cv, Lcls, st);
+    }
+  }
+};
+
+static void mlp_init_weights(std::vector<float>& w, int nout, unsigned long long seed) {
+  std::mt19937_64 rng(seed);
+  auto fill = [&](float* a, int fan_out, int fan_in) {
+    float lim = sqrtf(6.f / (float)(fan_in + fan_out));
+    std::uniform_real_distribution<float> U(-lim, lim);
+    for (int i = 0; i < fan_out * fan_in; i++) a[i] = U(rng);
+    for (int i = 0; i < fan_out; i++) a[fan_out * fan_in + i] = 0.f;
+  };
+  w.assign(tc_mlp_nparam(nout), 0.f);
+  float* p = w.data();
+  fill(p, kMlpH, kMlpIn);
+  p += kMlpH * kMlpIn + kMlpH;
+  fill(p, kMlpH, kMlpH);
+  p += kMlpH * kMlpH + kMlpH;
+  fill(p, kMlpH, kMlpH);
+  p += kMlpH * kMlpH + kMlpH;
+  fill(p, nout, kMlpH);
+}
+
+// gradient descent on (feat, lab) resident on the device; returns final losses
+static cudaError_t mlp_fit(int ntrain, int nval, int nout, const float* d_feat, const float* d_lab, float* d_w,
+                           const TcMlpNorm& norm, int iters, cudaStream_t st, double* train_loss, double* val_loss) {
+  const int np = tc_mlp_nparam(nout);
+  float *g = nullptr, *m1 = nullptr, *m2 = nullptr, *loss = nullptr, *gs = nullptr;
+  cudaError_t e = cudaMalloc((void**)&g, np * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&gs, np * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&m1, np * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&m2, np * sizeof(float));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&loss, 2 * sizeof(float));
+  if (e == cudaSuccess) {
+    cudaMemsetAsync(g, 0, np * sizeof(float), st);
+    cudaMemsetAsync(m1, 0, np * sizeof(float), st);
+    cudaMemsetAsync(m2, 0, np * sizeof(float), st);
+    int blocks = std::min(148 * 2, (ntrain + 255) / 256);
+    for (int it = 1; it <= iters; it++) {
+      float lr = 3e-3f * (it < iters / 2 ? 1.f : (it < 3 * iters / 4 ? 0.3f : 0.1f));
+      k_mlp_grad<<<blocks, 256, 0, st>>>(ntrain, nout, d_feat, d_lab, d_w, norm, g, loss);
+      k_mlp_adam<<<(np + 255) / 256, 256, 0, st>>>(np, d_w, g, m1, m2, lr, 0.9f, 0.999f, 1e-8f, it);
+    }
+    cudaMemsetAsync(loss, 0, 2 * sizeof(float), st);
+    cudaMemsetAsync(gs, 0, np * sizeof(float), st);
+    k_mlp_grad<<<blocks, 256, 0, st>>>(ntrain, nout, d_feat, d_lab, d_w, norm, gs, loss);
+    if (nval > 0)
+      k_mlp_grad<<<std::min(148, (nval + 255) / 256), 256, 0, st>>>(nval, nout, d_feat + (size_t)ntrain * kMlpIn,
+                                                                     d_lab + (size_t)ntrain * nout, d_w, norm, gs,
+                                                                     loss + 1);
+    float hl[2] = {0, 0};
+    e = cudaMemcpyAsync(hl, loss, sizeof(hl), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    *train_loss = hl[0];
+    *val_loss = hl[1];
+  }
+  cudaFree(g); cudaFree(gs); cudaFree(m1); cudaFree(m2); cudaFree(loss);
+  return e == cudaSuccess ? cudaGetLastError() : e;
+}
+
+template <int P>
+static tc_status train_selector(tc_ctx* ctx, int nsamples, int iters, unsigned long long seed, tc_train_report* rep) {
+  using OC = TcOrderClasses<P>;
+  constexpr int NTP = (P + 1) * (P + 1);
+  cudaStream_t st = ctx->stream;
+  const bool jerk = ctx->prm.variant == TC_VARIANT_JERKS;
+  TcCells cv = cells_view(ctx, NTP);
+  TcBodies b = bodies_view(ctx, ctx->n, jerk);
+  const int K = (int)std::min<unsigned long long>((unsigned long long)nsamples, ctx->n_m2l);
+  if (K < 16) return TC_ERR_ARG;
+  // the fixed-order evaluation left the sorted (target, source) list in m2l
+  std::vector<long long> idx(K);
+  std::mt19937_64 rng(seed);
+  std::uniform_int_distribution<unsigned long long> U(0, ctx->n_m2l - 1);
+  for (int k = 0; k < K; k++) idx[k] = (long long)U(rng);
+  long long* d_idx = nullptr;
+  int *pt = nullptr, *ps = nullptr;
+  double* Lcls = nullptr;
+  float *d_feat = nullptr, *d_lab = nullptr;
+  const int nc = ctx->ncell;
+  TC_CK(ctx->cell_pn.ensure((size_t)nc * (P + 1)));
+  TC_CK(cudaMalloc((void**)&d_idx, K * sizeof(long long)));
+  TC_CK(cudaMalloc((void**)&pt, K * sizeof(int)));
+  TC_CK(cudaMalloc((void**)&ps, K * sizeof(int)));
+  TC_CK(cudaMalloc((void**)&Lcls, (size_t)OC::n * K * NTP * sizeof(double)));
+  TC_CK(cudaMalloc((void**)&d_feat, (size_t)K * kMlpIn * sizeof(float)));
+  TC_CK(cudaMalloc((void**)&d_lab, (size_t)K * OC::n * sizeof(float)));
+  TC_CK(cudaMemcpyAsync(d_idx, idx.data(), K * sizeof(long long), cudaMemcpyHostToDevice, st));
+  k_gather_pairs<<<(K + 255) / 256, 256, 0, st>>>(K, ctx->m2l.p, d_idx, ctx->sbits, pt, ps);
+  k_cell_pn<P><<<nblocks(nc, 128), 128, 0, st>>>(nc, cv.M, ctx->cell_pn.p);
+  TcClassPairs<P, 0>::run(K, pt, ps, cv, Lcls, st);
+  k_pair_eval<P><<<K, 128, 0, st>>>(K, OC::n, pt, ps, b, cv, ctx->cell_pn.p, Lcls, d_lab);
+  k_pair_features<P><<<(K + 255) / 256, 256, 0, st>>>(K, pt, ps, cv, ctx->cell_pn.p, d_feat);
+  ctx->train_feat.resize((size_t)K * kMlpIn);
+  ctx->train_lab.resize((size_t)K * OC::n);
+  TC_CK(cudaMemcpyAsync(ctx->train_feat.data(), d_feat, ctx->train_feat.size() * sizeof(float),
+                        cudaMemcpyDeviceToHost, st));
+  TC_CK(cudaMemcpyAsync(ctx->train_lab.data(), d_lab, ctx->train_lab.size() * sizeof(float), cudaMemcpyDeviceToHost,
+                        st));
+  TC_CK(cudaStreamSynchronize(st));
+  ctx->train_n = K;
+  // standardisation from the training part
+  const int ntrain = (K * 4) / 5, nval = K - ntrain;
+  TcMlpNorm norm;
+  double lab_mean = 0;
+  for (int i = 0; i < kMlpIn; i++) {
+    double s1 = 0, s2 = 0;
+    for (int k = 0; k < ntrain; k++) {
+      double v = ctx->train_feat[(size_t)k * kMlpIn + i];
+      s1 += v;
+      s2 += v * v;
+    }
+    double mu = s1 / ntrain, var = std::max(s2 / ntrain - mu * mu, 1e-12);
+    norm.mean[i] = (float)mu;
+    norm.inv_std[i] = (float)(1.0 / sqrt(var));
+  }
+  for (int k = 0; k < ntrain * OC::n; k++) lab_mean += ctx->train_lab[k];
+  norm.out_mean = (float)(lab_mean / (ntrain * OC::n));
+  std::vector<float> w;
+  mlp_init_weights(w, OC::n, seed ^ 0x9e3779b97f4a7c15ull);
+  TC_CK(ctx->mlp_w.ensure(w.size()));
+  TC_CK(cudaMemcpyAsync(ctx->mlp_w.p, w.data(), w.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  double tl = 0, vl = 0;
+  TC_CK(mlp_fit(ntrain, nval, OC::n, d_feat, d_lab, ctx->mlp_w.p, norm, iters, st, &tl, &vl));
+  ctx->mlp_norm = norm;
+  ctx->mlp_nout = OC::n;
+  ctx->mlp_ready = true;
+  cudaFree(d_idx); cudaFree(pt); cudaFree(ps); cudaFree(Lcls); cudaFree(d_feat); cudaFree(d_lab);
+  if (rep) {
+    rep->samples = K;
+    rep->iters = iters;
+    rep->n_classes = OC::n;
+    for (int i = 0; i < 6; i++) rep->class_order[i] = i < OC::n ? OC::at(i) : 0;
+    rep->train_loss = tl;
+    rep->val_loss = vl;
+  }
+  return TC_OK;
+}
+
+// ----------------------------------------------------------------------------------------
 // per-order evaluation body
 // ----------------------------------------------------------------------------------------
 template <int P, bool JERK>
@@ -370,23 +629,31 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   // ---- far field and near field
   TcOut o = out_view(ctx, n, JERK);
   TC_CK(cudaMemsetAsync(ctx->outs.p, 0, sizeof(double) * (size_t)n * (JERK ? 7 : 4), st));
-  const bool mixed = prm.precision == TC_PREC_MIXED;
-  if (hs[0] > 0) {
+  const bool mixed = prm.precision == TC_PREC_MIXED_M2L;              // FP32 far field
+  const bool mixed_p2p = prm.precision != TC_PREC_FP64;               // FP32 near field
+  ctx->n_classes = 1;
+  ctx->class_order[0] = P;
+  ctx->class_pairs[0] = (long long)ctx->n_m2l;
+  ctx->flop_frac = 1.0;
+  if (hs[0] > 0 && prm.selector > 0 && !mixed && TcOrderClasses<P>::n > 1) {
+    cudaError_t ce = run_m2l_classes<P, JERK>(ctx, cv);
+    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "far field by order class");
+  } else if (hs[0] > 0) {
     if (mixed) {
       size_t smem = (size_t)TcM2LMixSmem<P>::BYTES;
       k_m2l_mixed<P, JERK><<<hs[0], tc_m2lx_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
                                                                         ctx->m2l_src.p, cv);
     } else {
       size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
-      k_m2l<P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
-                                                                  ctx->m2l_src.p, cv);
+      k_m2l<P, P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
+                                                                     ctx->m2l_src.p, cv);
     }
     ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[4], st);
   if (hs[1] > 0) {
     int g = nblocks(hs[1], kP2PWarps);
-    if (mixed)
+    if (mixed_p2p)
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b,
                                                        cv, o);
     else
@@ -413,11 +680,42 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
 
 typedef tc_status (*run_fn)(tc_ctx*, int);
 
+// RMS relative acceleration error of the last evaluation (Morton-order outputs) at nt seeded
+// bodies against FP64 direct sums
+static tc_status judge(tc_ctx* ctx, int n, int nt, bool jerk, double* rms) {
+  cudaStream_t st = ctx->stream;
+  std::vector<int> idx(nt);
+  std::mt19937_64 rng(ctx->prm.judge_seed);
+  std::uniform_int_distribution<int> U(0, n - 1);
+  for (int k = 0; k < nt; k++) idx[k] = U(rng);
+  TC_CK(ctx->judge_idx.ensure(nt));
+  TC_CK(ctx->judge_out.ensure(7 * (size_t)nt));
+  TC_CK(cudaMemcpyAsync(ctx->judge_idx.p, idx.data(), nt * sizeof(int), cudaMemcpyHostToDevice, st));
+  TcBodies b = bodies_view(ctx, n, jerk);
+  TcOut o = out_view(ctx, n, jerk);
+  k_direct_targets<<<nt, 256, 0, st>>>(n, nt, ctx->judge_idx.p, b, o, ctx->judge_out.p);
+  ctx->launches++;
+  std::vector<double> ref(7 * (size_t)nt);
+  TC_CK(cudaMemcpyAsync(ref.data(), ctx->judge_out.p, ref.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  TC_CK(cudaStreamSynchronize(st));
+  double s = 0.0;
+  for (int k = 0; k < nt; k++) {
+    const double* r = &ref[7 * (size_t)k];
+    double ex = r[4] - r[1], ey = r[5] - r[2], ez = r[6] - r[3];
+    double an = r[1] * r[1] + r[2] * r[2] + r[3] * r[3];
+    s += (ex * ex + ey * ey + ez * ez) / (an > 0 ? an : 1.0);
+  }
+  *rms = sqrt(s / nt);
+  return TC_OK;
+}
+
 template <int P>
 static void set_m2l_attrs() {
+  TcClassLaunch<P, 0, true>::attrs();
+  TcClassLaunch<P, 0, false>::attrs();
   size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
-  cudaFuncSetAttribute(k_m2l<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  cudaFuncSetAttribute(k_m2l<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_m2l<P, P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaFuncSetAttribute(k_m2l<P, P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   size_t smx = (size_t)TcM2LMixSmem<P>::BYTES;
   cudaFuncSetAttribute(k_m2l_mixed<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
   cudaFuncSetAttribute(k_m2l_mixed<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
@@ -505,6 +803,11 @@ void tc_default_params(tc_params* prm) {
   prm->precision = TC_PREC_FP64;
   prm->direct_below = -1;
   prm->device = 0;
+  prm->selector = 0;
+  prm->selector_tol = 1e-9;
+  prm->judge_n = 0;
+  prm->judge_tol = 0.0;
+  prm->judge_seed = 12345;
 }
 
 int tc_pmax(void) { return TC_PMAX; }
@@ -532,7 +835,8 @@ tc_status tc_create(const tc_params* prm, tc_ctx** out) {
   if (prm->p < 1 || prm->p > TC_PMAX || !tc_order_supported(prm->p)) return TC_ERR_UNSUPPORTED;
   if (prm->ncrit < 1 || !(prm->theta > 0.0) || (prm->variant != TC_VARIANT_TOP && prm->variant != TC_VARIANT_JERKS))
     return TC_ERR_ARG;
-  if (prm->precision != TC_PREC_FP64 && prm->precision != TC_PREC_MIXED) return TC_ERR_ARG;
+  if (prm->precision != TC_PREC_FP64 && prm->precision != TC_PREC_MIXED && prm->precision != TC_PREC_MIXED_M2L)
+    return TC_ERR_ARG;
   tc_ctx* ctx = new tc_ctx();
   ctx->prm = *prm;
   memset(&ctx->stats, 0, sizeof(ctx->stats));
@@ -542,7 +846,7 @@ tc_status tc_create(const tc_params* prm, tc_ctx** out) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_lv, sizeof(TcLevels));
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_cnt, sizeof(TcTravCounters));
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_err, sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_small, 4 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_small, 16 * sizeof(unsigned));
   if (e == cudaSuccess) {
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
     ctx->events = e == cudaSuccess;
@@ -567,6 +871,8 @@ tc_status tc_destroy(tc_ctx* ctx) {
   ctx->m2l.release(); ctx->m2l_alt.release(); ctx->p2p.release(); ctx->p2p_alt.release();
   ctx->m2l_start.release(); ctx->m2l_src.release(); ctx->p2p_start.release(); ctx->p2p_src.release();
   ctx->m2l_tl.release(); ctx->p2p_tl.release(); ctx->leaves.release(); ctx->bpart.release();
+  ctx->cell_pn.release(); ctx->cls_start.release(); ctx->cls_tl.release(); ctx->mlp_w.release();
+  ctx->judge_idx.release(); ctx->judge_out.release();
   if (ctx->d_root) cudaFree(ctx->d_root);
   if (ctx->d_lv) cudaFree(ctx->d_lv);
   if (ctx->d_cnt) cudaFree(ctx->d_cnt);
@@ -672,6 +978,28 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
     }
     if (rs != TC_OK) return rs;
   }
+  // ---- judge: FP64 direct sums at seeded bodies; a rejected selector step is redone at fixed p
+  ctx->judge_rms = 0.0;
+  ctx->judge_redo = 0;
+  if (ctx->prm.judge_n > 0) {
+    int nt = std::min(ctx->prm.judge_n, n);
+    double rms = 0.0;
+    tc_status js = judge(ctx, n, nt, jerk, &rms);
+    if (js != TC_OK) return js;
+    ctx->judge_rms = rms;
+    if (!ctx->direct && ctx->prm.selector > 0 && ctx->prm.judge_tol > 0 && rms > ctx->prm.judge_tol) {
+      int sel = ctx->prm.selector;
+      ctx->prm.selector = 0;
+      run_fn f = pick(ctx->prm.p, jerk);
+      rs = f(ctx, n);
+      ctx->prm.selector = sel;
+      if (rs != TC_OK) return rs;
+      js = judge(ctx, n, nt, jerk, &rms);
+      if (js != TC_OK) return js;
+      ctx->judge_rms = rms;
+      ctx->judge_redo = 1;
+    }
+  }
   // ---- outputs to the caller's order
   double *opot = pot, *oax = ax, *oay = ay, *oaz = az, *ojx = jx, *ojy = jy, *ojz = jz;
   if (mem == TC_MEM_HOST) {
@@ -706,6 +1034,14 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   S.n_p2p_inter = ctx->direct ? (long long)n * n : (long long)ctx->n_inter;
   S.n_launches = ctx->launches;
   S.flags = herr | ctx->tree_flags;
+  S.n_classes = ctx->n_classes;
+  for (int i = 0; i < 6; i++) {
+    S.class_order[i] = i < ctx->n_classes ? ctx->class_order[i] : 0;
+    S.class_pairs[i] = i < ctx->n_classes ? ctx->class_pairs[i] : 0;
+  }
+  S.m2l_flop_fraction = ctx->flop_frac;
+  S.judge_rms = ctx->judge_rms;
+  S.judge_redo = ctx->judge_redo;
   if (ctx->events) {
     float t[8];
     for (int i = 1; i < 8; i++) cudaEventElapsedTime(&t[i], ctx->ev[i - 1], ctx->ev[i]);
@@ -802,6 +1138,153 @@ tc_status tc_evaluate_direct_noalloc(int n, const double* x, const double* y, co
   return cudaGetLastError() == cudaSuccess ? TC_OK : TC_ERR_CUDA;
 }
 
+tc_status tc_train_selector(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
+                            const double* vy, const double* vz, const double* m, int mem, int nsamples, int iters,
+                            unsigned long long seed, tc_train_report* rep) {
+  if (!ctx || n <= 0 || nsamples <= 0 || iters < 0) return TC_ERR_ARG;
+  if (ctx->prm.p != 12 && ctx->prm.p != 16) return TC_ERR_UNSUPPORTED;
+  auto t0 = std::chrono::steady_clock::now();
+  const bool jerk = ctx->prm.variant == TC_VARIANT_JERKS;
+  // a fixed-order evaluation builds the tree, the expansions and the lists
+  int sel = ctx->prm.selector;
+  int db = ctx->prm.direct_below;
+  ctx->prm.selector = 0;
+  ctx->prm.direct_below = 0;
+  size_t N = (size_t)n;
+  tc_status rs;
+  if (mem == TC_MEM_HOST) {
+    std::vector<double> o(7 * N);
+    rs = tc_evaluate(ctx, n, x, y, z, vx, vy, vz, m, nullptr, o.data(), o.data() + N, o.data() + 2 * N,
+                     o.data() + 3 * N, jerk ? o.data() + 4 * N : nullptr, jerk ? o.data() + 5 * N : nullptr,
+                     jerk ? o.data() + 6 * N : nullptr, mem);
+  } else {
+    double* o = nullptr;
+    if (cudaMalloc((void**)&o, 7 * N * sizeof(double)) != cudaSuccess) {
+      ctx->prm.selector = sel;
+      ctx->prm.direct_below = db;
+      return TC_ERR_CUDA;
+    }
+    rs = tc_evaluate(ctx, n, x, y, z, vx, vy, vz, m, nullptr, o, o + N, o + 2 * N, o + 3 * N, jerk ? o + 4 * N : nullptr,
+                     jerk ? o + 5 * N : nullptr, jerk ? o + 6 * N : nullptr, mem);
+    cudaFree(o);
+  }
+  ctx->prm.selector = sel;
+  ctx->prm.direct_below = db;
+  if (rs != TC_OK) return rs;
+  tc_status r2 = ctx->prm.p == 12 ? train_selector<12>(ctx, nsamples, iters, seed, rep)
+                                  : train_selector<16>(ctx, nsamples, iters, seed, rep);
+  if (rep) rep->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  return r2;
+}
+
+tc_status tc_set_selector(tc_ctx* ctx, int selector, double tol) {
+  if (!ctx || selector < 0 || selector > 2 || !(tol > 0.0)) return TC_ERR_ARG;
+  if (selector == 2 && !ctx->mlp_ready) return TC_ERR_ARG;
+  ctx->prm.selector = selector;
+  ctx->prm.selector_tol = tol;
+  return TC_OK;
+}
+
+tc_status tc_get_selector_data(tc_ctx* ctx, float* feat, float* labels, int* n, int* n_classes) {
+  if (!ctx || !n) return TC_ERR_ARG;
+  *n = ctx->train_n;
+  if (n_classes) *n_classes = ctx->mlp_nout;
+  if (feat && !ctx->train_feat.empty()) memcpy(feat, ctx->train_feat.data(), ctx->train_feat.size() * sizeof(float));
+  if (labels && !ctx->train_lab.empty()) memcpy(labels, ctx->train_lab.data(), ctx->train_lab.size() * sizeof(float));
+  return TC_OK;
+}
+
+int tc_selector_nparam(tc_ctx* ctx) {
+  if (!ctx) return -1;
+  int nout = ctx->prm.p == 12 ? TcOrderClasses<12>::n : ctx->prm.p == 16 ? TcOrderClasses<16>::n : 0;
+  return nout ? tc_mlp_nparam(nout) : 0;
+}
+
+tc_status tc_get_selector_weights(tc_ctx* ctx, float* w, float* norm) {
+  if (!ctx || !ctx->mlp_ready) return TC_ERR_ARG;
+  if (w) TC_CK(cudaMemcpy(w, ctx->mlp_w.p, tc_mlp_nparam(ctx->mlp_nout) * sizeof(float), cudaMemcpyDeviceToHost));
+  if (norm) {
+    memcpy(norm, ctx->mlp_norm.mean, kMlpIn * sizeof(float));
+    memcpy(norm + kMlpIn, ctx->mlp_norm.inv_std, kMlpIn * sizeof(float));
+    norm[2 * kMlpIn] = ctx->mlp_norm.out_mean;
+  }
+  return TC_OK;
+}
+
+tc_status tc_set_selector_weights(tc_ctx* ctx, const float* w, const float* norm) {
+  int np = tc_selector_nparam(ctx);
+  if (!ctx || !w || !norm || np <= 0) return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  TC_CK(ctx->mlp_w.ensure(np));
+  TC_CK(cudaMemcpy(ctx->mlp_w.p, w, np * sizeof(float), cudaMemcpyHostToDevice));
+  memcpy(ctx->mlp_norm.mean, norm, kMlpIn * sizeof(float));
+  memcpy(ctx->mlp_norm.inv_std, norm + kMlpIn, kMlpIn * sizeof(float));
+  ctx->mlp_norm.out_mean = norm[2 * kMlpIn];
+  ctx->mlp_nout = ctx->prm.p == 12 ? TcOrderClasses<12>::n : TcOrderClasses<16>::n;
+  ctx->mlp_ready = true;
+  return TC_OK;
+}
+
+tc_status tc_mlp_loss_grad(int ns, int n_out, const float* feat, const float* labels, const float* w,
+                           const float* norm, float* grad, float* loss) {
+  if (ns <= 0 || n_out <= 0 || n_out > kMlpOutMax || !feat || !labels || !w || !norm || !grad || !loss)
+    return TC_ERR_ARG;
+  tc_ctx* ctx = nullptr;
+  const int np = tc_mlp_nparam(n_out);
+  float *df = nullptr, *dl = nullptr, *dw = nullptr, *dg = nullptr, *dloss = nullptr;
+  TcMlpNorm nm;
+  memcpy(nm.mean, norm, kMlpIn * sizeof(float));
+  memcpy(nm.inv_std, norm + kMlpIn, kMlpIn * sizeof(float));
+  nm.out_mean = norm[2 * kMlpIn];
+  TC_CK(cudaMalloc((void**)&df, (size_t)ns * kMlpIn * sizeof(float)));
+  TC_CK(cudaMalloc((void**)&dl, (size_t)ns * n_out * sizeof(float)));
+  TC_CK(cudaMalloc((void**)&dw, np * sizeof(float)));
+  TC_CK(cudaMalloc((void**)&dg, np * sizeof(float)));
+  TC_CK(cudaMalloc((void**)&dloss, sizeof(float)));
+  TC_CK(cudaMemcpy(df, feat, (size_t)ns * kMlpIn * sizeof(float), cudaMemcpyHostToDevice));
+  TC_CK(cudaMemcpy(dl, labels, (size_t)ns * n_out * sizeof(float), cudaMemcpyHostToDevice));
+  TC_CK(cudaMemcpy(dw, w, np * sizeof(float), cudaMemcpyHostToDevice));
+  TC_CK(cudaMemset(dg, 0, np * sizeof(float)));
+  TC_CK(cudaMemset(dloss, 0, sizeof(float)));
+  k_mlp_grad<<<std::min(148, (ns + 255) / 256), 256>>>(ns, n_out, df, dl, dw, nm, dg, dloss);
+  TC_CK(cudaGetLastError());
+  TC_CK(cudaMemcpy(grad, dg, np * sizeof(float), cudaMemcpyDeviceToHost));
+  TC_CK(cudaMemcpy(loss, dloss, sizeof(float), cudaMemcpyDeviceToHost));
+  cudaFree(df); cudaFree(dl); cudaFree(dw); cudaFree(dg); cudaFree(dloss);
+  return TC_OK;
+}
+
+__global__ void k_mlp_predict(int ns, int nout, const float* __restrict__ feat, const float* __restrict__ w,
+                              TcMlpNorm norm, float* __restrict__ pred) {
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  float x[kMlpIn], a1[kMlpH], a2[kMlpH], a3[kMlpH], y[kMlpOutMax];
+  for (int i = 0; i < kMlpIn; i++) x[i] = (feat[(size_t)k * kMlpIn + i] - norm.mean[i]) * norm.inv_std[i];
+  tc_mlp_forward(w, nout, x, a1, a2, a3, y);
+  for (int j = 0; j < nout; j++) pred[(size_t)k * nout + j] = y[j] + norm.out_mean;
+}
+
+tc_status tc_mlp_predict(int ns, int n_out, const float* feat, const float* w, const float* norm, float* pred) {
+  if (ns <= 0 || n_out <= 0 || n_out > kMlpOutMax || !feat || !w || !norm || !pred) return TC_ERR_ARG;
+  tc_ctx* ctx = nullptr;
+  const int np = tc_mlp_nparam(n_out);
+  float *df = nullptr, *dw = nullptr, *dp = nullptr;
+  TcMlpNorm nm;
+  memcpy(nm.mean, norm, kMlpIn * sizeof(float));
+  memcpy(nm.inv_std, norm + kMlpIn, kMlpIn * sizeof(float));
+  nm.out_mean = norm[2 * kMlpIn];
+  TC_CK(cudaMalloc((void**)&df, (size_t)ns * kMlpIn * sizeof(float)));
+  TC_CK(cudaMalloc((void**)&dw, np * sizeof(float)));
+  TC_CK(cudaMalloc((void**)&dp, (size_t)ns * n_out * sizeof(float)));
+  TC_CK(cudaMemcpy(df, feat, (size_t)ns * kMlpIn * sizeof(float), cudaMemcpyHostToDevice));
+  TC_CK(cudaMemcpy(dw, w, np * sizeof(float), cudaMemcpyHostToDevice));
+  k_mlp_predict<<<(ns + 127) / 128, 128>>>(ns, n_out, df, dw, nm, dp);
+  TC_CK(cudaGetLastError());
+  TC_CK(cudaMemcpy(pred, dp, (size_t)ns * n_out * sizeof(float), cudaMemcpyDeviceToHost));
+  cudaFree(df); cudaFree(dw); cudaFree(dp);
+  return TC_OK;
+}
+
 tc_status tc_get_stats(tc_ctx* ctx, tc_stats* st) {
   if (!ctx || !st) return TC_ERR_ARG;
   *st = ctx->stats;
@@ -840,6 +1323,9 @@ tc_status tc_get_lists(tc_ctx* ctx, int kind, int* tgt, int* src) {
   TC_CK(cudaMemcpy(k.data(), kind ? ctx->p2p.p : ctx->m2l.p, cnt * sizeof(unsigned long long),
                    cudaMemcpyDeviceToHost));
   unsigned long long mask = (1ull << ctx->sbits) - 1ull;
+  unsigned long long kmask = (1ull << (2 * ctx->sbits)) - 1ull;  // drop an order-class prefix
+  for (auto& v : k) v &= kmask;
+  std::sort(k.begin(), k.end());
   for (unsigned long long i = 0; i < cnt; i++) {
     if (tgt) tgt[i] = (int)(k[i] >> ctx->sbits);
     if (src) src[i] = (int)(k[i] & mask);

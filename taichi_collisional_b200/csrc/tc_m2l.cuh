@@ -71,13 +71,15 @@ __device__ __forceinline__ TcPairGeo tc_pair_geo(double dx, double dy, double dz
   return g;
 }
 
-// forward half for degree D: scaled, rotated into the pair frame, unscaled -> smem
-template <int P, int D>
+// forward half for degree D of an order-Q M2L: scaled, rotated into the pair frame, unscaled
+// -> smem.  QUIRK: Q is the expansion order itself, so the (Q, +-Q) entries vanish as in the
+// reference.
+template <int Q, int D, bool QUIRK>
 __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1, cd ex1, double* buf, int lane) {
   double v[2 * D + 1], o[2 * D + 1];
 #pragma unroll
   for (int k = 0; k < 2 * D + 1; k++) v[k] = __ldg(Ms + D * D + k) * c_fc[D * D + k];
-  if (D == P) {
+  if (QUIRK && D == Q) {
     v[0] = 0.0;
     v[2 * D] = 0.0;
   }
@@ -156,54 +158,57 @@ struct TcM2LSmem {
 // Warp w of each 4-warp group owns the degrees TcDegSets<P>::d[w][*] (balanced by a
 // per-degree cost model) for the group's 32 pairs; warps w and w + 4 run the same degree code,
 // which keeps each SM sub-partition's instruction working set to one degree set.
-template <int P, int W, int I>
+template <int Q, bool QUIRK, int W, int I>
 struct TcDegSeq {
-  static constexpr int D = TcDegSets<P>::d[W][I];
+  static constexpr int D = TcDegSets<Q>::d[W][I];
   static __device__ __forceinline__ void fwd(const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
     if constexpr (D >= 0) {
-      tc_m2l_fwd<P, D>(Ms, ez1, ex1, buf, lane);
-      TcDegSeq<P, W, I + 1>::fwd(Ms, ez1, ex1, buf, lane);
+      tc_m2l_fwd<Q, D, QUIRK>(Ms, ez1, ex1, buf, lane);
+      TcDegSeq<Q, QUIRK, W, I + 1>::fwd(Ms, ez1, ex1, buf, lane);
     }
   }
   static __device__ __forceinline__ void back(const double* buf, double rinv, int lane, cd ez1, cd ex1, double* acc,
                                               int acol, bool valid) {
     if constexpr (D >= 0) {
-      tc_m2l_back<P, D>(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-      TcDegSeq<P, W, I + 1>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+      tc_m2l_back<Q, D>(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+      TcDegSeq<Q, QUIRK, W, I + 1>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
     }
   }
 };
 
-template <int P>
+template <int Q, bool QUIRK>
 __device__ __forceinline__ void tc_m2l_fwd_warp(int w, const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
-  if (w == 0) TcDegSeq<P, 0, 0>::fwd(Ms, ez1, ex1, buf, lane);
-  else if (w == 1) TcDegSeq<P, 1, 0>::fwd(Ms, ez1, ex1, buf, lane);
-  else if (w == 2) TcDegSeq<P, 2, 0>::fwd(Ms, ez1, ex1, buf, lane);
-  else TcDegSeq<P, 3, 0>::fwd(Ms, ez1, ex1, buf, lane);
+  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::fwd(Ms, ez1, ex1, buf, lane);
+  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::fwd(Ms, ez1, ex1, buf, lane);
+  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::fwd(Ms, ez1, ex1, buf, lane);
+  else TcDegSeq<Q, QUIRK, 3, 0>::fwd(Ms, ez1, ex1, buf, lane);
 }
-template <int P>
+template <int Q, bool QUIRK>
 __device__ __forceinline__ void tc_m2l_back_warp(int w, const double* buf, double rinv, int lane, cd ez1, cd ex1,
                                                  double* acc, int acol, bool valid) {
-  if (w == 0) TcDegSeq<P, 0, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-  else if (w == 1) TcDegSeq<P, 1, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-  else if (w == 2) TcDegSeq<P, 2, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-  else TcDegSeq<P, 3, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+  else TcDegSeq<Q, QUIRK, 3, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
 }
 
 __device__ __forceinline__ void tc_bar_group(int grp) {
   asm volatile("bar.sync %0, 128;" ::"r"(2 + grp) : "memory");
 }
 
-template <int P>
-constexpr int tc_m2l_threads() { return 128 * TcM2LGroups<P>::G; }
+template <int Q>
+constexpr int tc_m2l_threads() { return 128 * TcM2LGroups<Q>::G; }
 
-template <int P, bool JERK>
-__global__ void __launch_bounds__(tc_m2l_threads<P>(), 1) k_m2l(const int* __restrict__ tlist, int ntl,
-                                               const int* __restrict__ tstart,
-                                               const int* __restrict__ src, TcCells c) {
-  using SM = TcM2LSmem<P>;
-  constexpr int NT = SM::NT;
+// M2L of order Q <= P over a per-target list; expansions are stored with order P.  Adds
+// into L (zeroed before the first M2L launch of an evaluation).
+template <int P, int Q, bool JERK>
+__global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __restrict__ tlist, int ntl,
+                                                               const int* __restrict__ tstart,
+                                                               const int* __restrict__ src, TcCells c) {
+  using SM = TcM2LSmem<Q>;
+  constexpr int NTQ = SM::NT, NTP = (P + 1) * (P + 1);
   constexpr int G = SM::G;
+  constexpr bool QUIRK = Q == P;
   extern __shared__ double tc_m2l_smem[];
   double* acc = tc_m2l_smem + SM::ACC;
   int ti = blockIdx.x;
@@ -212,30 +217,30 @@ __global__ void __launch_bounds__(tc_m2l_threads<P>(), 1) k_m2l(const int* __res
   if (!c.has_sink[t]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = warp >> 2, w = warp & 3, acol = grp * 32 + lane;
-  double* buf = tc_m2l_smem + SM::BUF + grp * NT * 32;
+  double* buf = tc_m2l_smem + SM::BUF + grp * NTQ * 32;
   const int s_beg = tstart[t], s_end = tstart[t + 1];
   const double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
   for (int arr = 0; arr < (JERK ? 2 : 1); arr++) {
     const double* Mbase = arr ? c.Md : c.M;
-    for (int i = threadIdx.x; i < NT * 32 * G; i += blockDim.x) acc[i] = 0.0;
+    for (int i = threadIdx.x; i < NTQ * 32 * G; i += blockDim.x) acc[i] = 0.0;
     tc_bar_cta();
     for (int b0 = s_beg + grp * 32; b0 < s_end; b0 += 32 * G) {
       int idx = b0 + lane;
       bool valid = idx < s_end;
       int s = src[valid ? idx : s_beg];
       TcPairGeo pg = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
-      tc_m2l_fwd_warp<P>(w, Mbase + (size_t)s * NT, pg.ez1, pg.ex1, buf, lane);
+      tc_m2l_fwd_warp<Q, QUIRK>(w, Mbase + (size_t)s * NTP, pg.ez1, pg.ex1, buf, lane);
       tc_bar_group(grp);
-      tc_m2l_back_warp<P>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, acc, acol, valid);
+      tc_m2l_back_warp<Q, QUIRK>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, acc, acol, valid);
       tc_bar_group(grp);
     }
     tc_bar_cta();
-    double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NT;
-    for (int r = threadIdx.x; r < NT; r += blockDim.x) {
+    double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NTP;
+    for (int r = threadIdx.x; r < NTQ; r += blockDim.x) {
       double v = 0.0;
 #pragma unroll 8
       for (int q = 0; q < 32 * G; q++) v += acc[r * (32 * G) + q];
-      Lt[r] = v;
+      Lt[r] += v;
     }
     tc_bar_cta();
   }

@@ -1,0 +1,214 @@
+// Learned far-field order selector: a 3 x 32 tanh MLP (FP32 weights) that predicts, for an
+// M2L pair, log10 of the relative acceleration error of an order-q M2L for every order class q
+// (error relative to the source's monopole acceleration M_s / r^2).
+//
+// Features (TC_NFEAT = 8, standardised with the training set's mean and deviation):
+//   log(Rt/r), log(Rs/r), log(Pn_s[2] / (Pn_s[0] Rs^2)), log(Pn_s[4] / (Pn_s[0] Rs^4)),
+//   log(Pn_s[6] / (Pn_s[0] Rs^6)), log(Pn_s[8] / (Pn_s[0] Rs^8)), log(N_s), log(N_t)
+// i.e. distance over cell radii, the per-degree multipole power of the source and the two
+// cells' particle counts.  Training data come from the FMM itself (tc_train.cuh): M2L at each
+// order class against exact P2P for pairs drawn from a real interaction list.
+//
+// Forward, backward (mean-squared error on the log errors) and Adam are hand-written kernels;
+// one thread per sample, weights staged in shared memory.
+#pragma once
+#include "tc_select.cuh"
+
+namespace tc {
+
+constexpr int kMlpIn = TC_NFEAT, kMlpH = 32, kMlpOutMax = TC_MAX_CLASSES;
+// parameter layout: W1[H][IN] b1[H] W2[H][H] b2[H] W3[H][H] b3[H] W4[OUT][H] b4[OUT]
+__host__ __device__ constexpr int tc_mlp_nparam(int nout) {
+  return kMlpH * kMlpIn + kMlpH + 2 * (kMlpH * kMlpH + kMlpH) + nout * kMlpH + nout;
+}
+constexpr int kMlpParamMax = kMlpH * kMlpIn + kMlpH + 2 * (kMlpH * kMlpH + kMlpH) + kMlpOutMax * kMlpH + kMlpOutMax;
+
+struct TcMlpNorm {
+  float mean[kMlpIn], inv_std[kMlpIn];
+  float out_mean;  // outputs are learned as offsets from this value
+};
+
+__device__ __forceinline__ float tc_clampf(float v, float lo, float hi) { return fminf(fmaxf(v, lo), hi); }
+
+// hardware tanh approximation (one MUFU op), used for inference over every pair
+__device__ __forceinline__ float tc_tanh_fast(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// raw features of one pair (before standardisation)
+__device__ __forceinline__ void tc_pair_features(const TcCells& c, int t, int s, const double* pn, int P, float* f) {
+  double dx = c.X[t] - c.X[s], dy = c.Y[t] - c.Y[s], dz = c.Z[t] - c.Z[s];
+  double r = sqrt(dx * dx + dy * dy + dz * dz);
+  double rt = c.R[t], rs = c.R[s];
+  const double* ps = pn + (size_t)s * (P + 1);
+  double p0 = fmax(ps[0], 1e-300);
+  f[0] = (float)log(rt / r);
+  f[1] = (float)log(rs / r);
+  for (int j = 0; j < 4; j++) {
+    int deg = 2 * (j + 1);
+    double v = deg <= P ? ps[deg] / (p0 * pow(rs, (double)deg)) : 0.0;
+    f[2 + j] = tc_clampf((float)log(fmax(v, 1e-30)), -69.f, 10.f);
+  }
+  f[6] = (float)log((double)c.nbody[s]);
+  f[7] = (float)log((double)c.nbody[t]);
+}
+
+// forward pass; a1..a3 hold the hidden activations (for the backward pass).  FAST uses the
+// hardware tanh approximation (inference only; training uses tanhf).
+template <bool FAST = false>
+__device__ __forceinline__ void tc_mlp_forward(const float* __restrict__ w, int nout, const float* x, float* a1,
+                                               float* a2, float* a3, float* y) {
+  const float* W1 = w;
+  const float* b1 = W1 + kMlpH * kMlpIn;
+  const float* W2 = b1 + kMlpH;
+  const float* b2 = W2 + kMlpH * kMlpH;
+  const float* W3 = b2 + kMlpH;
+  const float* b3 = W3 + kMlpH * kMlpH;
+  const float* W4 = b3 + kMlpH;
+  const float* b4 = W4 + nout * kMlpH;
+  for (int j = 0; j < kMlpH; j++) {
+    float s = b1[j];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) s += W1[j * kMlpIn + i] * x[i];
+    a1[j] = FAST ? tc_tanh_fast(s) : tanhf(s);
+  }
+  for (int j = 0; j < kMlpH; j++) {
+    float s = b2[j];
+#pragma unroll 8
+    for (int i = 0; i < kMlpH; i++) s += W2[j * kMlpH + i] * a1[i];
+    a2[j] = FAST ? tc_tanh_fast(s) : tanhf(s);
+  }
+  for (int j = 0; j < kMlpH; j++) {
+    float s = b3[j];
+#pragma unroll 8
+    for (int i = 0; i < kMlpH; i++) s += W3[j * kMlpH + i] * a2[i];
+    a3[j] = FAST ? tc_tanh_fast(s) : tanhf(s);
+  }
+  for (int j = 0; j < nout; j++) {
+    float s = b4[j];
+#pragma unroll 8
+    for (int i = 0; i < kMlpH; i++) s += W4[j * kMlpH + i] * a3[i];
+    y[j] = s;
+  }
+}
+
+// loss = mean over samples and outputs of (y - target)^2; gradients accumulated into g
+__global__ void k_mlp_grad(int ns, int nout, const float* __restrict__ feat, const float* __restrict__ target,
+                           const float* __restrict__ w, TcMlpNorm norm, float* __restrict__ g,
+                           float* __restrict__ loss) {
+  __shared__ float sw[kMlpParamMax];
+  __shared__ float sg[kMlpParamMax];
+  __shared__ float sloss;
+  const int np = tc_mlp_nparam(nout);
+  for (int i = threadIdx.x; i < np; i += blockDim.x) {
+    sw[i] = w[i];
+    sg[i] = 0.f;
+  }
+  if (threadIdx.x == 0) sloss = 0.f;
+  __syncthreads();
+  const float* W2 = sw + kMlpH * kMlpIn + kMlpH;
+  const float* W3 = W2 + kMlpH * kMlpH + kMlpH;
+  const float* W4 = W3 + kMlpH * kMlpH + kMlpH;
+  float* gW1 = sg;
+  float* gb1 = gW1 + kMlpH * kMlpIn;
+  float* gW2 = gb1 + kMlpH;
+  float* gb2 = gW2 + kMlpH * kMlpH;
+  float* gW3 = gb2 + kMlpH;
+  float* gb3 = gW3 + kMlpH * kMlpH;
+  float* gW4 = gb3 + kMlpH;
+  float* gb4 = gW4 + nout * kMlpH;
+  const float scale = 2.f / ((float)ns * (float)nout);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ns; k += gridDim.x * blockDim.x) {
+    float x[kMlpIn], a1[kMlpH], a2[kMlpH], a3[kMlpH], y[kMlpOutMax], d4[kMlpOutMax], d3[kMlpH], d2[kMlpH];
+    for (int i = 0; i < kMlpIn; i++) x[i] = (feat[(size_t)k * kMlpIn + i] - norm.mean[i]) * norm.inv_std[i];
+    tc_mlp_forward(sw, nout, x, a1, a2, a3, y);
+    float l = 0.f;
+    for (int j = 0; j < nout; j++) {
+      float e = y[j] - (target[(size_t)k * nout + j] - norm.out_mean);
+      l += e * e;
+      d4[j] = scale * e;
+      atomicAdd(&gb4[j], d4[j]);
+      for (int i = 0; i < kMlpH; i++) atomicAdd(&gW4[j * kMlpH + i], d4[j] * a3[i]);
+    }
+    atomicAdd(&sloss, l / ((float)ns * (float)nout));
+    for (int i = 0; i < kMlpH; i++) {
+      float s = 0.f;
+      for (int j = 0; j < nout; j++) s += W4[j * kMlpH + i] * d4[j];
+      d3[i] = s * (1.f - a3[i] * a3[i]);
+      atomicAdd(&gb3[i], d3[i]);
+    }
+    for (int j = 0; j < kMlpH; j++)
+      for (int i = 0; i < kMlpH; i++) atomicAdd(&gW3[j * kMlpH + i], d3[j] * a2[i]);
+    for (int i = 0; i < kMlpH; i++) {
+      float s = 0.f;
+      for (int j = 0; j < kMlpH; j++) s += W3[j * kMlpH + i] * d3[j];
+      d2[i] = s * (1.f - a2[i] * a2[i]);
+      atomicAdd(&gb2[i], d2[i]);
+    }
+    for (int j = 0; j < kMlpH; j++)
+      for (int i = 0; i < kMlpH; i++) atomicAdd(&gW2[j * kMlpH + i], d2[j] * a1[i]);
+    for (int i = 0; i < kMlpH; i++) {
+      float s = 0.f;
+      for (int j = 0; j < kMlpH; j++) s += W2[j * kMlpH + i] * d2[j];
+      float d1 = s * (1.f - a1[i] * a1[i]);
+      atomicAdd(&gb1[i], d1);
+      for (int q = 0; q < kMlpIn; q++) atomicAdd(&gW1[i * kMlpIn + q], d1 * x[q]);
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < np; i += blockDim.x)
+    if (sg[i] != 0.f) atomicAdd(&g[i], sg[i]);
+  if (threadIdx.x == 0) atomicAdd(loss, sloss);
+}
+
+__global__ void k_mlp_adam(int np, float* __restrict__ w, float* __restrict__ g, float* __restrict__ m1,
+                           float* __restrict__ m2, float lr, float b1, float b2, float eps, int step) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= np) return;
+  float gi = g[i];
+  float a = b1 * m1[i] + (1.f - b1) * gi;
+  float b = b2 * m2[i] + (1.f - b2) * gi * gi;
+  m1[i] = a;
+  m2[i] = b;
+  float ah = a / (1.f - powf(b1, (float)step)), bh = b / (1.f - powf(b2, (float)step));
+  w[i] -= lr * ah / (sqrtf(bh) + eps);
+  g[i] = 0.f;
+}
+
+// learned selector: features -> predicted log10 errors -> smallest class under log10(tol)
+template <int P>
+__global__ void k_select_mlp(const unsigned long long* __restrict__ keys, unsigned long long n, int sbits, TcCells c,
+                             const double* __restrict__ pn, const float* __restrict__ w, TcMlpNorm norm,
+                             float log10_tol, unsigned long long* __restrict__ out, unsigned int* __restrict__ hist) {
+  using OC = TcOrderClasses<P>;
+  __shared__ float sw[kMlpParamMax];
+  __shared__ unsigned int h[TC_MAX_CLASSES];
+  const int nout = OC::n;
+  for (int i = threadIdx.x; i < tc_mlp_nparam(nout); i += blockDim.x) sw[i] = w[i];
+  if (threadIdx.x < TC_MAX_CLASSES) h[threadIdx.x] = 0;
+  __syncthreads();
+  const unsigned long long mask = (1ull << sbits) - 1ull;
+  for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (unsigned long long)gridDim.x * blockDim.x) {
+    unsigned long long key = keys[k];
+    int t = (int)(key >> sbits), s = (int)(key & mask);
+    float x[kMlpIn], a1[kMlpH], a2[kMlpH], a3[kMlpH], y[kMlpOutMax];
+    tc_pair_features(c, t, s, pn, P, x);
+    for (int i = 0; i < kMlpIn; i++) x[i] = (x[i] - norm.mean[i]) * norm.inv_std[i];
+    tc_mlp_forward<true>(sw, nout, x, a1, a2, a3, y);
+    int cls = nout - 1;
+    for (int i = 0; i < nout - 1; i++)
+      if (y[i] + norm.out_mean <= log10_tol) {
+        cls = i;
+        break;
+      }
+    out[k] = ((unsigned long long)cls << (2 * sbits)) | key;
+    atomicAdd(&h[cls], 1u);
+  }
+  __syncthreads();
+  if (threadIdx.x < TC_MAX_CLASSES && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
+}
+
+}  // namespace tc

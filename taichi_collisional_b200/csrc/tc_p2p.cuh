@@ -130,6 +130,34 @@ __global__ void k_direct(int n, const TcBodies b, TcOut out) {
   }
 }
 
+// FP64 direct sums at selected bodies (Morton positions), one 256-thread block per target;
+// also copies the evaluation's own result for that body: out[k] = {direct pot, ax, ay, az,
+// evaluated ax, ay, az}.  The judge of the selector and an accuracy probe.
+__global__ void __launch_bounds__(256) k_direct_targets(int n, int nt, const int* __restrict__ tgt, const TcBodies b,
+                                                        TcOut ev, double* __restrict__ out /* nt x 7 */) {
+  __shared__ double red[4][8];
+  int k = blockIdx.x;
+  if (k >= nt) return;
+  int i = tgt[k];
+  double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+  TcAcc<false> a;
+  a.zero();
+  for (int j = threadIdx.x; j < n; j += blockDim.x) tc_p2p_one<false>(xi, yi, zi, 0, 0, 0, b, j, a);
+  for (int o = 16; o > 0; o >>= 1) a.add_xor(o);
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) { red[0][w] = a.pot; red[1][w] = a.ax; red[2][w] = a.ay; red[3][w] = a.az; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double* o = out + 7 * (size_t)k;
+    for (int q = 0; q < 4; q++) {
+      double v = 0;
+      for (int ww = 0; ww < 8; ww++) v += red[q][ww];
+      o[q] = v;
+    }
+    o[4] = ev.ax[i]; o[5] = ev.ay[i]; o[6] = ev.az[i];
+  }
+}
+
 // Morton order -> caller order
 __global__ void k_scatter_out(int n, const int* __restrict__ perm, TcOut s, double* pot, double* ax, double* ay,
                               double* az, double* jx, double* jy, double* jz) {
@@ -145,11 +173,18 @@ __global__ void k_scatter_out(int n, const int* __restrict__ perm, TcOut s, doub
 namespace tc {
 
 // ---------------------------------------------------------------------------------------
-// Mixed-precision near field: FP32 interactions, compensated sums.
-// Positions enter relative to the target cell centre as FP32 (hi, lo) pairs formed in FP64,
-// so dx = (xj_hi - xi_hi) + (xj_lo - xi_lo) keeps ~1e-14 relative accuracy even for close
-// pairs; each 32-source tile is summed in FP32 and folded into (hi, lo) accumulators with
-// a two-sum; the final per-target sum is formed in FP64.
+// Mixed-precision near field: FP32 interactions, compensated sums, the strongest pair in FP64.
+// Positions and masses enter as FP32 (hi, lo) pairs formed in FP64 (positions relative to
+// the target cell centre), so dx = (xj_hi - xi_hi) + (xj_lo - xi_lo) carries only its final
+// FP32 rounding even for close pairs; 1/r is the hardware estimate refined by one Newton
+// step; each 32-source tile is summed in FP32 and folded into (hi, lo) accumulators with a
+// two-sum; the final per-target sum is formed in FP64.
+//
+// The FP32 error of a target's near field is dominated by its strongest interaction (a close
+// neighbour or a massive star): each lane tracks the source with the largest m / r^2 and, after
+// the loop, replaces that pair's FP32 contribution by its FP64 value.  The pair arithmetic uses
+// explicitly rounded intrinsics (no contraction), so the contribution recomputed for removal is
+// bit-identical to the one that was summed.
 // ---------------------------------------------------------------------------------------
 struct TcF2 {
   float hi, lo;
@@ -163,13 +198,58 @@ struct TcF2 {
   __device__ __forceinline__ double val() const { return (double)hi + (double)lo; }
 };
 
+// one FP32 pair: f0 = m / r (potential), f = m / r^3 (acceleration factor), g the jerk's
+// radial factor; the accumulated terms are f0, d f and dv f + d g
+struct TcPair32 {
+  float dx, dy, dz, ri, f0, f, dvx, dvy, dvz, g;
+};
+
+template <bool JERK>
+__device__ __forceinline__ TcPair32 tc_pair32(float sxh, float syh, float szh, float sxl, float syl, float szl,
+                                              float mh, float ml, float svx, float svy, float svz, float xh,
+                                              float yh, float zh, float xl, float yl, float zl, float vxi,
+                                              float vyi, float vzi) {
+  TcPair32 v;
+  v.dx = __fadd_rn(__fsub_rn(sxh, xh), __fsub_rn(sxl, xl));
+  v.dy = __fadd_rn(__fsub_rn(syh, yh), __fsub_rn(syl, yl));
+  v.dz = __fadd_rn(__fsub_rn(szh, zh), __fsub_rn(szl, zl));
+  float r2 = __fmaf_rn(v.dx, v.dx, __fmaf_rn(v.dy, v.dy, __fmul_rn(v.dz, v.dz)));
+  v.ri = 0.f;
+  if (r2 > 0.f) {
+    // one Newton step on the hardware estimate: y' = y + y (1 - r2 y^2) / 2
+    float y = rsqrtf(r2);
+    float e = __fmaf_rn(-__fmul_rn(r2, y), y, 1.f);
+    v.ri = __fmaf_rn(__fmul_rn(0.5f, y), e, y);
+  }
+  v.f0 = __fmaf_rn(ml, v.ri, __fmul_rn(mh, v.ri));
+  float ri2 = __fmul_rn(v.ri, v.ri);
+  v.f = __fmul_rn(v.f0, ri2);
+  if (JERK) {
+    v.dvx = __fsub_rn(svx, vxi);
+    v.dvy = __fsub_rn(svy, vyi);
+    v.dvz = __fsub_rn(svz, vzi);
+    float vr = __fmul_rn(3.f, __fmaf_rn(v.dx, v.dvx, __fmaf_rn(v.dy, v.dvy, __fmul_rn(v.dz, v.dvz))));
+    v.g = __fmul_rn(__fmul_rn(-v.f, ri2), vr);
+  } else {
+    v.dvx = v.dvy = v.dvz = v.g = 0.f;
+  }
+  return v;
+}
+
+// FP32 (hi, lo) split of x - c
+__device__ __forceinline__ void tc_split(double x, double c, float& h, float& l) {
+  double d = x - c;
+  h = (float)d;
+  l = (float)(d - (double)h);
+}
+
 template <bool JERK>
 __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
                                                               const int* __restrict__ tstart,
                                                               const int* __restrict__ src, const TcBodies b,
                                                               const TcCells c, TcOut out) {
-  // per warp source tile: xh yh zh xl yl zl m vx vy vz
-  __shared__ float tile[kP2PWarps][10][32];
+  // per warp source tile: xh yh zh xl yl zl mh ml vx vy vz
+  __shared__ float tile[kP2PWarps][11][32];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float(*T)[32] = tile[w];
   for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
@@ -190,13 +270,14 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
       bool vi = (t0 + ti) < nt;
       float xh = 0, yh = 0, zh = 0, xl = 0, yl = 0, zl = 0, vxi = 0, vyi = 0, vzi = 0;
       if (vi) {
-        double dx = b.x[i] - Xc, dy = b.y[i] - Yc, dz = b.z[i] - Zc;
-        xh = (float)dx; xl = (float)(dx - (double)xh);
-        yh = (float)dy; yl = (float)(dy - (double)yh);
-        zh = (float)dz; zl = (float)(dz - (double)zh);
+        tc_split(b.x[i], Xc, xh, xl);
+        tc_split(b.y[i], Yc, yh, yl);
+        tc_split(b.z[i], Zc, zh, zl);
         if (JERK) { vxi = (float)b.vx[i]; vyi = (float)b.vy[i]; vzi = (float)b.vz[i]; }
       }
       TcF2 pot = {0, 0}, ax = {0, 0}, ay = {0, 0}, az = {0, 0}, jx = {0, 0}, jy = {0, 0}, jz = {0, 0};
+      float best = 0.f;
+      int bj = -1;
       for (int q = sb; q < se; q++) {
         int s = src[q];
         int jb = c.begin[s], jn = c.nbody[s];
@@ -205,40 +286,32 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
           __syncwarp();
           if (lane < cnt) {
             int j = jb + j0 + lane;
-            double dx = b.x[j] - Xc, dy = b.y[j] - Yc, dz = b.z[j] - Zc;
-            float h;
-            h = (float)dx; T[0][lane] = h; T[3][lane] = (float)(dx - (double)h);
-            h = (float)dy; T[1][lane] = h; T[4][lane] = (float)(dy - (double)h);
-            h = (float)dz; T[2][lane] = h; T[5][lane] = (float)(dz - (double)h);
-            T[6][lane] = (b.flags[j] & 2) ? (float)b.m[j] : 0.f;
-            if (JERK) { T[7][lane] = (float)b.vx[j]; T[8][lane] = (float)b.vy[j]; T[9][lane] = (float)b.vz[j]; }
+            tc_split(b.x[j], Xc, T[0][lane], T[3][lane]);
+            tc_split(b.y[j], Yc, T[1][lane], T[4][lane]);
+            tc_split(b.z[j], Zc, T[2][lane], T[5][lane]);
+            tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, T[6][lane], T[7][lane]);
+            if (JERK) { T[8][lane] = (float)b.vx[j]; T[9][lane] = (float)b.vy[j]; T[10][lane] = (float)b.vz[j]; }
           }
           __syncwarp();
           float sp = 0, sx = 0, sy = 0, sz = 0, qx = 0, qy = 0, qz = 0;
           if (vi) {
             for (int jj = grp; jj < cnt; jj += ng) {
-              float dx = (T[0][jj] - xh) + (T[3][jj] - xl);
-              float dy = (T[1][jj] - yh) + (T[4][jj] - yl);
-              float dz = (T[2][jj] - zh) + (T[5][jj] - zl);
-              float r2 = dx * dx + dy * dy + dz * dz;
-              float ri = r2 > 0.f ? rsqrtf(r2) : 0.f;
-              float f = T[6][jj] * ri;
-              sp += f;
-              float ri2 = ri * ri;
-              f *= ri2;
-              sx += dx * f;
-              sy += dy * f;
-              sz += dz * f;
+              TcPair32 v = tc_pair32<JERK>(T[0][jj], T[1][jj], T[2][jj], T[3][jj], T[4][jj], T[5][jj], T[6][jj],
+                                           T[7][jj], JERK ? T[8][jj] : 0.f, JERK ? T[9][jj] : 0.f,
+                                           JERK ? T[10][jj] : 0.f, xh, yh, zh, xl, yl, zl, vxi, vyi, vzi);
+              sp = __fadd_rn(sp, v.f0);
+              sx = __fmaf_rn(v.dx, v.f, sx);
+              sy = __fmaf_rn(v.dy, v.f, sy);
+              sz = __fmaf_rn(v.dz, v.f, sz);
               if (JERK) {
-                float dvx = T[7][jj] - vxi, dvy = T[8][jj] - vyi, dvz = T[9][jj] - vzi;
-                float vr = 3.f * (dx * dvx + dy * dvy + dz * dvz);
-                qx += dvx * f;
-                qy += dvy * f;
-                qz += dvz * f;
-                float g = -f * ri2 * vr;
-                qx += dx * g;
-                qy += dy * g;
-                qz += dz * g;
+                qx = __fmaf_rn(v.dx, v.g, __fmaf_rn(v.dvx, v.f, qx));
+                qy = __fmaf_rn(v.dy, v.g, __fmaf_rn(v.dvy, v.f, qy));
+                qz = __fmaf_rn(v.dz, v.g, __fmaf_rn(v.dvz, v.f, qz));
+              }
+              float strength = __fmul_rn(v.f0, v.ri);  // m / r^2
+              if (strength > best) {
+                best = strength;
+                bj = jb + j0 + jj;
               }
             }
           }
@@ -249,6 +322,29 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
       TcAcc<JERK> a;
       a.pot = pot.val(); a.ax = ax.val(); a.ay = ay.val(); a.az = az.val();
       a.jx = jx.val(); a.jy = jy.val(); a.jz = jz.val();
+      if (vi && bj >= 0) {
+        // the strongest pair: remove its FP32 terms exactly, add its FP64 value
+        const int j = bj;
+        float sxh, syh, szh, sxl, syl, szl, mh, ml;
+        tc_split(b.x[j], Xc, sxh, sxl);
+        tc_split(b.y[j], Yc, syh, syl);
+        tc_split(b.z[j], Zc, szh, szl);
+        tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, mh, ml);
+        TcPair32 v = tc_pair32<JERK>(sxh, syh, szh, sxl, syl, szl, mh, ml, JERK ? (float)b.vx[j] : 0.f,
+                                     JERK ? (float)b.vy[j] : 0.f, JERK ? (float)b.vz[j] : 0.f, xh, yh, zh, xl, yl,
+                                     zl, vxi, vyi, vzi);
+        a.pot -= (double)v.f0;
+        a.ax -= (double)v.dx * (double)v.f;
+        a.ay -= (double)v.dy * (double)v.f;
+        a.az -= (double)v.dz * (double)v.f;
+        if (JERK) {
+          a.jx -= (double)v.dvx * (double)v.f + (double)v.dx * (double)v.g;
+          a.jy -= (double)v.dvy * (double)v.f + (double)v.dy * (double)v.g;
+          a.jz -= (double)v.dvz * (double)v.f + (double)v.dz * (double)v.g;
+        }
+        tc_p2p_one<JERK>(b.x[i], b.y[i], b.z[i], JERK ? b.vx[i] : 0.0, JERK ? b.vy[i] : 0.0, JERK ? b.vz[i] : 0.0,
+                         b, j, a);
+      }
       for (int o = gsz; o < 32; o <<= 1) a.add_xor(o);
       if (vi && grp == 0 && (b.flags[i] & 1)) {
         out.pot[i] += a.pot;

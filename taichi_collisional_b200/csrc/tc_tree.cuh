@@ -232,15 +232,15 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long l
 
 // Sorts (keys, vals) by key bits [0, bits).  Uses alt buffers; the result ends in keys/vals.
 inline int radix_sort(unsigned long long* keys, int* vals, unsigned long long* keys_alt, int* vals_alt, int n, int bits, uint32_t* hist,
-                      cudaStream_t st) {
+                      cudaStream_t st, int begin_bit = 0) {
   if (n <= 1) return 0;
   int launches = 0;
   int nblk = (n + kRsTile - 1) / kRsTile;
-  int passes = (bits + 7) / 8;
+  int passes = (bits - begin_bit + 7) / 8;
   unsigned long long *ka = keys, *kb = keys_alt;
   int *va = vals, *vb = vals_alt;
   for (int p = 0; p < passes; p++) {
-    int shift = 8 * p;
+    int shift = begin_bit + 8 * p;
     k_rs_hist<<<nblk, kRsThreads, 0, st>>>(ka, n, shift, hist);
     launches += 2 + excl_scan(hist, 256 * nblk, hist + 256 * (size_t)nblk, st);
     if (vals)

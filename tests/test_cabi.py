@@ -32,7 +32,7 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts_match_header():
     # tc_params: int p, int ncrit, double theta, int variant, int precision, int use_shift,
     # double shift_u[3], int direct_below, int device
-    assert C.sizeof(tcb.Params) == 4 + 4 + 8 + 4 + 4 + 4 + 4 + 24 + 4 + 4
+    assert C.sizeof(tcb.Params) == 4 + 4 + 8 + 4 + 4 + 4 + 4 + 24 + 4 + 4 + 4 + 4 + 8 + 4 + 4 + 8 + 8
     assert tcb.Params.theta.offset == 8
     assert tcb.Params.shift_u.offset == 32
 

@@ -37,13 +37,16 @@ typedef enum {
   TC_ERR_CAPACITY = 3,   /* an interaction list overflowed; the context grows and retries */
   TC_ERR_NAN_INPUT = 4,  /* a position or mass is NaN/Inf */
   TC_ERR_DEPTH = 5,      /* more than ncrit bodies share a level-21 cell (kept as one leaf) */
-  TC_ERR_UNSUPPORTED = 6 /* option not available in this build */
+  TC_ERR_UNSUPPORTED = 6, /* option not available in this build */
+  TC_ERR_TIMEOUT = 7      /* a bounded device-side wait (tensor-core far field) gave up; outputs invalid */
 } tc_status;
 
 typedef enum { TC_VARIANT_TOP = 0, TC_VARIANT_JERKS = 1 } tc_variant;
 /* TC_PREC_FP64: every stage FP64 (parity with the reference at 1e-12).
  * TC_PREC_MIXED: near field (P2P) in FP32 with compensated sums, far field FP64.
- * TC_PREC_MIXED_M2L: near field as MIXED, and the M2L rotations in FP32 as well. */
+ * TC_PREC_MIXED_M2L: near field as MIXED, and the M2L in FP32 as well: for p <= 12 the swap
+ *   and translation contractions run on the tensor cores (tcgen05, TF32 hi/lo split, FP32
+ *   accumulation), the phase rotations in FP32 on the CUDA cores. */
 typedef enum { TC_PREC_FP64 = 0, TC_PREC_MIXED = 1, TC_PREC_MIXED_M2L = 2 } tc_precision;
 typedef enum { TC_MEM_HOST = 0, TC_MEM_DEVICE = 1 } tc_memory;
 
@@ -195,6 +198,13 @@ const char* tc_last_error_string(tc_ctx* ctx);
 int tc_pmax(void);
 /* 1 if expansion order p has compiled kernels in this build. */
 int tc_order_supported(int p);
+/* Constant matrices of the tensor-core far field (TC_PREC_MIXED_M2L, order q <= 12): the
+ * swap and translation bins, TF32 hi parts then lo parts, 256 floats per 16 x 16 bin in the
+ * kernel's shared-memory layout.  Writes at most cap floats into out (may be NULL) and
+ * returns the full count, or -1 if q has no tensor-core plan.  A host-only diagnostic (no
+ * device work), used to check the plan against the FP64 rotation M2L.  No counterpart in
+ * the reference. */
+int tc_tc_bins(int q, float* out, int cap);
 
 #ifdef __cplusplus
 }

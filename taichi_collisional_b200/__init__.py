@@ -24,7 +24,7 @@ PREC_FP64, PREC_MIXED, PREC_MIXED_M2L = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "capacity exceeded", 4: "non-finite input",
-          5: "tree depth limit reached", 6: "unsupported option"}
+          5: "tree depth limit reached", 6: "unsupported option", 7: "device-side wait timed out"}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -59,7 +59,7 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
-           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector"]
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -125,6 +125,8 @@ def load_library(path=LIB_PATH):
     L.tc_mlp_predict.restype = C.c_int
     L.tc_set_selector.argtypes = [C.c_void_p, C.c_int, C.c_double]
     L.tc_set_selector.restype = C.c_int
+    L.tc_tc_bins.argtypes = [C.c_int, _fp, C.c_int]
+    L.tc_tc_bins.restype = C.c_int
     _lib = L
     return L
 
@@ -321,6 +323,18 @@ class Gravity:
                                        L.ctypes.data_as(_dp), None if Ld is None else Ld.ctypes.data_as(_dp))
         self._check(rc, "tc_get_expansions")
         return M, Md, L, Ld
+
+
+def tc_bins(q):
+    """Constant matrices of the tensor-core far field at order q: (hi, lo) arrays of shape
+    (bins, 256) in the kernel's layout (see include/taichi_b200.h, tc_tc_bins)."""
+    L = load_library()
+    n = L.tc_tc_bins(q, None, 0)
+    if n < 0:
+        raise TaichiError("no tensor-core plan for order %d" % q)
+    buf = np.zeros(n, dtype=np.float32)
+    L.tc_tc_bins(q, buf.ctypes.data_as(C.POINTER(C.c_float)), n)
+    return buf[: n // 2].reshape(-1, 256), buf[n // 2:].reshape(-1, 256)
 
 
 def evaluate_direct_noalloc(x, y, z, m, vx=None, vy=None, vz=None, flags=None, out=None, stream=0):

@@ -6,8 +6,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libtaichi_b200.so")
-SOURCES = ["tc_lib.cu", "tc_common.cuh", "tc_tree.cuh", "tc_upward.cuh", "tc_traverse.cuh", "tc_m2l.cuh", "tc_m2l_mixed.cuh",
-           "tc_down.cuh", "tc_p2p.cuh", "tc_harmonics.cuh", "swap_tables.h", "tdesign.h", "m2l_schedule.h", "tc_select.cuh", "tc_mlp.cuh", "tc_train.cuh"]
+# every source of the single translation unit (tc_lib.cu includes the rest)
+SOURCE_EXT = (".cu", ".cuh", ".h")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared"]
 
@@ -16,7 +16,8 @@ def _stale():
     if not os.path.exists(LIB):
         return True
     t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, s) for s in SOURCES] + [os.path.join(HERE, "..", "include", "taichi_b200.h")]
+    deps = [os.path.join(CSRC, s) for s in os.listdir(CSRC) if s.endswith(SOURCE_EXT)]
+    deps.append(os.path.join(HERE, "..", "include", "taichi_b200.h"))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 

@@ -18,6 +18,7 @@
 #define TC_EBIT_MINIBALL 16u
 #define TC_EBIT_NAN 32u
 #define TC_EBIT_CELL_CAP 64u
+#define TC_EBIT_TIMEOUT 128u
 
 // Sorted-body structure of arrays (Morton order).
 struct TcBodies {

@@ -26,6 +26,7 @@
 #include "tc_traverse.cuh"
 #include "tc_m2l.cuh"
 #include "tc_m2l_mixed.cuh"
+#include "tc_m2l_tc.cuh"
 #include "tc_down.cuh"
 #include "tc_p2p.cuh"
 #include "tc_select.cuh"
@@ -114,7 +115,10 @@ struct tc_ctx {
   TcLevels* d_lv = nullptr;
   TcTravCounters* d_cnt = nullptr;
   unsigned int* d_err = nullptr;
-  unsigned int* d_small = nullptr;  // [0] m2l targets, [1] p2p targets, [2] leaves
+  unsigned int* d_small = nullptr;  // [0] m2l targets, [1] p2p targets, [2] leaves, [9] tensor M2L counter
+  DBuf<float> tc_bins;  // tensor-core M2L bin matrices (hi, lo) of order tc_bins_q
+  int tc_bins_q = -1;
+  int nsm = 0;
   DBuf<double> bpart;
   // last evaluation
   TcLevels lv;
@@ -184,6 +188,78 @@ static cudaError_t init_constants(int dev) {
   if ((e = cudaMemcpyToSymbol(c_mC, mC, sizeof(mC))) != cudaSuccess) return e;
   if (dev >= 0 && dev < 64) g_const_init[dev] = true;
   return cudaSuccess;
+}
+
+// bin matrices of the tensor-core M2L at order Q (tc_m2l_tc.cuh): the orthogonal swap
+// T_n = E S_n E^-1 of every degree (S from the exact tables of swap_tables.h,
+// E_k = c_m / sqrt((n+|m|)!(n-|m|)!)) and the translation C[n,k,m] = (-1)^m (n+k)! /
+// sqrt((n+m)!(n-m)!(k+m)!(k-m)!) for n + k <= Q, each rounded to TF32 as hi + lo
+static float tc_tf32_host(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x1000u) & 0xffffe000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+template <int Q>
+static void tc_build_bins(std::vector<float>& img) {
+  using PL = TcTcPlan<Q>;
+  const int NB = PL::NH + PL::NTB;
+  std::vector<double> full((size_t)NB * 256, 0.0);
+  double fact[2 * TC_TC_QMAX + 2];
+  fact[0] = 1.0;
+  for (int i = 1; i < 2 * TC_TC_QMAX + 2; i++) fact[i] = fact[i - 1] * (double)i;
+  auto deg = [](int i) { int n = 0; while ((n + 1) * (n + 1) <= i) n++; return n; };
+  auto E = [&](int n, int m) {
+    int a = m < 0 ? -m : m;
+    return (a ? sqrt(2.0) : 1.0) / sqrt(fact[n + a] * fact[n - a]);
+  };
+  // swap halves: out position o, in position k of the same half (same degree only)
+  for (int h = 0; h < PL::NH; h++)
+    for (int o = 0; o < 16; o++)
+      for (int k = 0; k < 16; k++) {
+        int no = PL::half_nat[h][o], ni = PL::half_nat[h][k];
+        if (no < 0 || ni < 0) continue;
+        int n = deg(no);
+        if (deg(ni) != n) continue;
+        double sv = 0.0;
+        for (int r = tc_swap_rowptr[no]; r < tc_swap_rowptr[no + 1]; r++)
+          if (tc_swap_col[r] == ni) sv = tc_swap_val[r];
+        full[(size_t)h * 256 + tc_tc_bin_index(o, k)] = sv * E(n, no - n * n - n) / E(n, ni - n * n - n);
+      }
+  // translation bins (real arrangement; the imaginary parts use the same matrix)
+  for (int b = 0; b < PL::NTB; b++)
+    for (int o = 0; o < 16; o++)
+      for (int k = 0; k < 16; k++) {
+        int no = PL::trans_nat[b][o], ni = PL::trans_nat[b][k];
+        if (no < 0 || ni < 0) continue;
+        int N = deg(no), K = deg(ni);
+        int mo = no - N * N - N, mi = ni - K * K - K;
+        if (mo != mi || N + K > Q) continue;
+        int m = mo < 0 ? -mo : mo;
+        double v = ((m & 1) ? -1.0 : 1.0) * fact[N + K] / sqrt(fact[N + m] * fact[N - m] * fact[K + m] * fact[K - m]);
+        full[(size_t)(PL::NH + b) * 256 + tc_tc_bin_index(o, k)] = v;
+      }
+  img.assign((size_t)2 * NB * 256, 0.f);
+  for (size_t i = 0; i < full.size(); i++) {
+    float hi = tc_tf32_host((float)full[i]);
+    img[i] = hi;
+    img[full.size() + i] = tc_tf32_host((float)(full[i] - (double)hi));
+  }
+}
+
+template <int Q>
+static cudaError_t tc_ensure_bins(tc_ctx* ctx) {
+  if (ctx->tc_bins_q == Q) return cudaSuccess;
+  std::vector<float> img;
+  tc_build_bins<Q>(img);
+  cudaError_t e = ctx->tc_bins.ensure(img.size());
+  if (e != cudaSuccess) return e;
+  e = cudaMemcpy(ctx->tc_bins.p, img.data(), img.size() * sizeof(float), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) ctx->tc_bins_q = Q;
+  return e;
 }
 
 static inline int nblocks(long long n, int t) { return (int)((n + t - 1) / t); }
@@ -639,7 +715,16 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     cudaError_t ce = run_m2l_classes<P, JERK>(ctx, cv);
     if (ce != cudaSuccess) return cuda_fail(ctx, ce, "far field by order class");
   } else if (hs[0] > 0) {
-    if (mixed) {
+    if (mixed && P <= TC_TC_QMAX) {
+      if constexpr (P <= TC_TC_QMAX) {
+        TC_CK(tc_ensure_bins<P>(ctx));
+        TC_CK(cudaMemsetAsync(ctx->d_small + 9, 0, sizeof(unsigned), st));
+        int grid = std::min((int)hs[0], ctx->nsm);
+        k_m2l_tc<P, P, JERK><<<grid, 128, TcTcSmem<P>::TOTAL, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
+                                                                     ctx->m2l_src.p, cv, ctx->tc_bins.p,
+                                                                     ctx->d_small + 9, ctx->d_err);
+      }
+    } else if (mixed) {
       size_t smem = (size_t)TcM2LMixSmem<P>::BYTES;
       k_m2l_mixed<P, JERK><<<hs[0], tc_m2lx_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
                                                                         ctx->m2l_src.p, cv);
@@ -716,6 +801,10 @@ static void set_m2l_attrs() {
   size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
   cudaFuncSetAttribute(k_m2l<P, P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_m2l<P, P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if constexpr (P <= TC_TC_QMAX) {
+    cudaFuncSetAttribute(k_m2l_tc<P, P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcTcSmem<P>::TOTAL);
+    cudaFuncSetAttribute(k_m2l_tc<P, P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, TcTcSmem<P>::TOTAL);
+  }
   size_t smx = (size_t)TcM2LMixSmem<P>::BYTES;
   cudaFuncSetAttribute(k_m2l_mixed<P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
   cudaFuncSetAttribute(k_m2l_mixed<P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smx);
@@ -814,6 +903,20 @@ int tc_pmax(void) { return TC_PMAX; }
 
 int tc_order_supported(int p) { return pick(p, false) != nullptr; }
 
+int tc_tc_bins(int q, float* out, int cap) {
+  std::vector<float> img;
+  switch (q) {
+    case 4: tc_build_bins<4>(img); break;
+    case 6: tc_build_bins<6>(img); break;
+    case 8: tc_build_bins<8>(img); break;
+    case 10: tc_build_bins<10>(img); break;
+    case 12: tc_build_bins<12>(img); break;
+    default: return -1;
+  }
+  if (out) memcpy(out, img.data(), sizeof(float) * std::min((size_t)std::max(cap, 0), img.size()));
+  return (int)img.size();
+}
+
 const char* tc_status_string(tc_status s) {
   switch (s) {
     case TC_OK: return "ok";
@@ -823,6 +926,7 @@ const char* tc_status_string(tc_status s) {
     case TC_ERR_NAN_INPUT: return "non-finite position or mass";
     case TC_ERR_DEPTH: return "tree depth limit reached";
     case TC_ERR_UNSUPPORTED: return "unsupported option";
+    case TC_ERR_TIMEOUT: return "device-side wait timed out";
   }
   return "unknown status";
 }
@@ -847,6 +951,7 @@ tc_status tc_create(const tc_params* prm, tc_ctx** out) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_cnt, sizeof(TcTravCounters));
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_small, 16 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->prm.device);
   if (e == cudaSuccess) {
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
     ctx->events = e == cudaSuccess;
@@ -1048,6 +1153,10 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
     cudaEventElapsedTime(&t[0], ctx->ev[0], ctx->ev[7]);
     S.ms_total = t[0]; S.ms_tree = t[1]; S.ms_upward = t[2]; S.ms_traverse = t[3]; S.ms_m2l = t[4];
     S.ms_p2p = t[5]; S.ms_downward = t[6];
+  }
+  if (herr & TC_EBIT_TIMEOUT) {
+    ctx->err = "a device-side wait of the tensor-core far field gave up";
+    return TC_ERR_TIMEOUT;
   }
   if ((herr | ctx->tree_flags) & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
   if ((herr | ctx->tree_flags) & TC_EBIT_DEPTH) return TC_ERR_DEPTH;

@@ -8,14 +8,17 @@
 // The reference's factorial table stops at (2P-1)! (kernel_fast_lean.h:127), so the scaled
 // (P, +-P) entries are zero; that is reproduced here.
 //
-// Layout: one CTA per target cell; warp g owns the two degrees (g, P-g) of 32 (target,
-// source) pairs at a time, one pair per lane, so every per-degree step -- including the
-// constant swap matrices, emitted as straight-line code with immediate coefficients --
-// runs in registers.  The only exchange is the z-translation, which mixes degrees and goes
-// through shared memory (NT x 32 doubles).  Each lane accumulates its pairs' locals in its
-// own column of a shared NT x 32 accumulator; one fixed-order sum over the 32 columns per
-// coefficient gives deterministic results.  Per pair, warp 0 also stores the rotation
-// angles and the translation factors j!/r^(j+1) for the other warps.
+// Layout: one CTA per target cell, 1 or 2 groups of 4 warps; each group takes 32 (target,
+// source) pairs at a time, one pair per lane.  Warp w of a group owns a fixed set of degrees
+// (m2l_schedule.h, balanced by a per-degree cost model) and runs every per-degree step --
+// including the constant swap matrices, emitted as straight-line code with immediate
+// coefficients -- in registers.  The only exchange is the z-translation, which mixes
+// degrees and goes through shared memory (NT x 32 doubles per group).  Each lane
+// accumulates its pairs' locals in its own column of a shared accumulator; one fixed-order
+// sum over the columns per
+// coefficient gives deterministic results.  Instruction footprint limits this kernel (the
+// code of all degrees exceeds the instruction caches), so each pass applies its two swaps
+// through a rolled two-step loop over one copy of the degree's swap code.
 #pragma once
 #include "swap_tables.h"
 #include "tc_harmonics.cuh"
@@ -83,10 +86,14 @@ __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1
     v[0] = 0.0;
     v[2 * D] = 0.0;
   }
-  tc_rot_fwd<D>(v, ez1);
-  TcSwapDeg<D>::apply(v, o);
-  tc_rot_fwd<D>(o, ex1);
-  TcSwapDeg<D>::apply(o, v);
+  // rotate about z, swap, rotate about x, swap: one copy of the swap code, run twice
+#pragma unroll 1
+  for (int rep = 0; rep < 2; rep++) {
+    tc_rot_fwd<D>(v, rep ? ex1 : ez1);
+    TcSwapDeg<D>::apply(v, o);
+#pragma unroll
+    for (int k = 0; k < 2 * D + 1; k++) v[k] = o[k];
+  }
 #pragma unroll
   for (int k = 0; k < 2 * D + 1; k++) buf[(D * D + k) * 32 + lane] = v[k] * c_fcinv[D * D + k];
 }
@@ -136,10 +143,14 @@ __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int 
     l[N + m] = sg * sp;
     pm *= rinv;
   }
-  TcSwapDeg<N>::apply(l, o);
-  tc_rot_inv<N>(o, ex1);
-  TcSwapDeg<N>::apply(o, l);
-  tc_rot_inv<N>(l, ez1);
+  // swap, rotate back about x, swap, rotate back about z: one copy of the swap code, run twice
+#pragma unroll 1
+  for (int rep = 0; rep < 2; rep++) {
+    TcSwapDeg<N>::apply(l, o);
+    tc_rot_inv<N>(o, rep ? ez1 : ex1);
+#pragma unroll
+    for (int k = 0; k < 2 * N + 1; k++) l[k] = o[k];
+  }
   if (valid) {
 #pragma unroll
     for (int k = 0; k < 2 * N + 1; k++) acc[(N * N + k) * (32 * TcM2LGroups<P>::G) + acol] += l[k];

@@ -774,12 +774,16 @@ static tc_status judge(tc_ctx* ctx, int n, int nt, bool jerk, double* rms) {
   std::uniform_int_distribution<int> U(0, n - 1);
   for (int k = 0; k < nt; k++) idx[k] = U(rng);
   TC_CK(ctx->judge_idx.ensure(nt));
-  TC_CK(ctx->judge_out.ensure(7 * (size_t)nt));
+  const int nchunk = std::max(1, std::min(4 * ctx->nsm, n / 1024));
+  TC_CK(ctx->judge_out.ensure(7 * (size_t)nt + 4 * (size_t)nt * nchunk));
   TC_CK(cudaMemcpyAsync(ctx->judge_idx.p, idx.data(), nt * sizeof(int), cudaMemcpyHostToDevice, st));
   TcBodies b = bodies_view(ctx, n, jerk);
   TcOut o = out_view(ctx, n, jerk);
-  k_direct_targets<<<nt, 256, 0, st>>>(n, nt, ctx->judge_idx.p, b, o, ctx->judge_out.p);
-  ctx->launches++;
+  double* part = ctx->judge_out.p + 7 * (size_t)nt;
+  k_direct_targets<<<dim3(nchunk, (nt + kJudgeTile - 1) / kJudgeTile), kJudgeTile, 0, st>>>(n, nt, nchunk,
+                                                                                         ctx->judge_idx.p, b, part);
+  k_direct_targets_sum<<<nblocks(nt, 128), 128, 0, st>>>(nt, nchunk, ctx->judge_idx.p, part, o, ctx->judge_out.p);
+  ctx->launches += 2;
   std::vector<double> ref(7 * (size_t)nt);
   TC_CK(cudaMemcpyAsync(ref.data(), ctx->judge_out.p, ref.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
   TC_CK(cudaStreamSynchronize(st));

@@ -130,32 +130,63 @@ __global__ void k_direct(int n, const TcBodies b, TcOut out) {
   }
 }
 
-// FP64 direct sums at selected bodies (Morton positions), one 256-thread block per target;
-// also copies the evaluation's own result for that body: out[k] = {direct pot, ax, ay, az,
-// evaluated ax, ay, az}.  The judge of the selector and an accuracy probe.
-__global__ void __launch_bounds__(256) k_direct_targets(int n, int nt, const int* __restrict__ tgt, const TcBodies b,
-                                                        TcOut ev, double* __restrict__ out /* nt x 7 */) {
-  __shared__ double red[4][8];
-  int k = blockIdx.x;
-  if (k >= nt) return;
-  int i = tgt[k];
-  double xi = b.x[i], yi = b.y[i], zi = b.z[i];
-  TcAcc<false> a;
-  a.zero();
-  for (int j = threadIdx.x; j < n; j += blockDim.x) tc_p2p_one<false>(xi, yi, zi, 0, 0, 0, b, j, a);
-  for (int o = 16; o > 0; o >>= 1) a.add_xor(o);
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) { red[0][w] = a.pot; red[1][w] = a.ax; red[2][w] = a.ay; red[3][w] = a.az; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double* o = out + 7 * (size_t)k;
-    for (int q = 0; q < 4; q++) {
-      double v = 0;
-      for (int ww = 0; ww < 8; ww++) v += red[q][ww];
-      o[q] = v;
+// FP64 direct sums at selected bodies (Morton positions): the judge of the selector and an
+// accuracy probe.  Block (c, g) takes the source chunk c and up to 256 targets (one per
+// thread, group g); sources pass through shared memory in tiles, so every body is read
+// once per block.  part[(k * nchunk + c) * 4 + q] = chunk c's (pot, ax, ay, az) of target k.
+constexpr int kJudgeTile = 256;
+__global__ void __launch_bounds__(kJudgeTile) k_direct_targets(int n, int nt, int nchunk, const int* __restrict__ tgt,
+                                                               const TcBodies b, double* __restrict__ part) {
+  __shared__ double sx[kJudgeTile], sy[kJudgeTile], sz[kJudgeTile], sm[kJudgeTile];
+  const int c = blockIdx.x, k = blockIdx.y * kJudgeTile + threadIdx.x;
+  const int chunk = (n + nchunk - 1) / nchunk;
+  const int j0 = c * chunk, j1 = min(n, j0 + chunk);
+  const int i = k < nt ? tgt[k] : 0;
+  const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+  double pot = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  for (int t0 = j0; t0 < j1; t0 += kJudgeTile) {
+    const int j = t0 + threadIdx.x;
+    __syncthreads();
+    if (j < j1) {
+      sx[threadIdx.x] = b.x[j];
+      sy[threadIdx.x] = b.y[j];
+      sz[threadIdx.x] = b.z[j];
+      sm[threadIdx.x] = (b.flags[j] & 2) ? b.m[j] : 0.0;
     }
-    o[4] = ev.ax[i]; o[5] = ev.ay[i]; o[6] = ev.az[i];
+    __syncthreads();
+    const int cnt = min(kJudgeTile, j1 - t0);
+    for (int q = 0; q < cnt; q++) {
+      const double dx = sx[q] - xi, dy = sy[q] - yi, dz = sz[q] - zi;
+      const double r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 > 0.0) {
+        const double invr = rsqrt(r2);
+        const double f = sm[q] * invr;
+        pot += f;
+        const double f3 = f * invr * invr;
+        ax += dx * f3;
+        ay += dy * f3;
+        az += dz * f3;
+      }
+    }
   }
+  if (k < nt) {
+    double* o = part + ((size_t)k * nchunk + c) * 4;
+    o[0] = pot; o[1] = ax; o[2] = ay; o[3] = az;
+  }
+}
+
+// out[k] = {direct pot, ax, ay, az (chunks summed in order), evaluated ax, ay, az}
+__global__ void k_direct_targets_sum(int nt, int nchunk, const int* __restrict__ tgt, const double* __restrict__ part,
+                                     TcOut ev, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int c = 0; c < nchunk; c++)
+    for (int q = 0; q < 4; q++) v[q] += part[((size_t)k * nchunk + c) * 4 + q];
+  const int i = tgt[k];
+  double* o = out + 7 * (size_t)k;
+  o[0] = v[0]; o[1] = v[1]; o[2] = v[2]; o[3] = v[3];
+  o[4] = ev.ax[i]; o[5] = ev.ay[i]; o[6] = ev.az[i];
 }
 
 // Morton order -> caller order

@@ -198,6 +198,16 @@ const char* tc_last_error_string(tc_ctx* ctx);
 int tc_pmax(void);
 /* 1 if expansion order p has compiled kernels in this build. */
 int tc_order_supported(int p);
+/* FP64 direct sums at nt target bodies (caller indices targets[k] in [0, n)) over all n bodies
+ * (no softening; r = 0 skipped; sources are the bodies with flag bit 1, all if flags is NULL):
+ * out[7k..7k+6] = pot, ax, ay, az, jx, jy, jz (jerk zero unless vx, vy, vz are given).
+ * Inputs as in tc_evaluate (mem says where x..m and flags live; targets and out are host
+ * arrays).  Uses the context's device and stream but none of its evaluation state.  A
+ * validation helper for accuracy statements: the sums of the reference's direct()
+ * (traverse_eager.h:349-360 over P2P, kernel_fast_lean.h:462), restricted to chosen targets. */
+tc_status tc_direct_sums(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
+                         const double* vy, const double* vz, const double* m, const unsigned char* flags, int nt,
+                         const int* targets, double* out, int mem);
 /* Constant matrices of the tensor-core far field (TC_PREC_MIXED_M2L, order q <= 12): the
  * swap and translation bins, TF32 hi parts then lo parts, 256 floats per 16 x 16 bin in the
  * kernel's shared-memory layout.  Writes at most cap floats into out (may be NULL) and

@@ -59,7 +59,7 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
-           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins"]
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -127,6 +127,8 @@ def load_library(path=LIB_PATH):
     L.tc_set_selector.restype = C.c_int
     L.tc_tc_bins.argtypes = [C.c_int, _fp, C.c_int]
     L.tc_tc_bins.restype = C.c_int
+    L.tc_direct_sums.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8 + [C.c_int, _ip, _dp, C.c_int]
+    L.tc_direct_sums.restype = C.c_int
     _lib = L
     return L
 
@@ -221,6 +223,26 @@ class Gravity:
                                  MEM_DEVICE if dev else MEM_HOST)
         self._check(rc, "tc_evaluate")
         return out
+
+    def direct_sums(self, x, y, z, m, targets, vx=None, vy=None, vz=None, flags=None):
+        """FP64 direct sums at the bodies `targets` (caller indices) over all bodies: a dict of
+        pot, ax, ay, az, jx, jy, jz arrays (numpy), one entry per target.  Inputs are numpy
+        (host) or CUDA torch tensors (device); used for accuracy statements."""
+        n = len(x)
+        dev = hasattr(x, "data_ptr")
+        if not dev:
+            x, y, z, m = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, m))
+            if vx is not None:
+                vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64) for a in (vx, vy, vz))
+            if flags is not None:
+                flags = np.ascontiguousarray(flags, dtype=np.uint8)
+        t = np.ascontiguousarray(targets, dtype=np.int32)
+        out = np.zeros((len(t), 7))
+        rc = self._L.tc_direct_sums(self._h, n, _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(m),
+                                    _ptr(flags), len(t), t.ctypes.data_as(_ip), out.ctypes.data_as(_dp),
+                                    MEM_DEVICE if dev else MEM_HOST)
+        self._check(rc, "tc_direct_sums")
+        return {k: out[:, i].copy() for i, k in enumerate(("pot", "ax", "ay", "az", "jx", "jy", "jz"))}
 
     def kick_drift(self, x, y, z, vx, vy, vz, ax, ay, az, dt_kick, dt_drift):
         """FP64 leapfrog update on CUDA tensors: v += a dt_kick; x += v dt_drift."""

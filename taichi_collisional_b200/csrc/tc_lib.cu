@@ -109,6 +109,10 @@ struct tc_ctx {
   int judge_redo = 0;
   DBuf<int> judge_idx;
   DBuf<double> judge_out;
+  // tc_direct_sums: bodies in caller order, targets, partial and final sums
+  DBuf<double> ds_bod, ds_out;
+  DBuf<uint8_t> ds_flags;
+  DBuf<int> ds_idx, ds_tgt;
   size_t fcap = 0, mcap = 0, pcap = 0;
   // small device structs
   TcRootInfo* d_root = nullptr;
@@ -775,13 +779,13 @@ static tc_status judge(tc_ctx* ctx, int n, int nt, bool jerk, double* rms) {
   for (int k = 0; k < nt; k++) idx[k] = U(rng);
   TC_CK(ctx->judge_idx.ensure(nt));
   const int nchunk = std::max(1, std::min(4 * ctx->nsm, n / 1024));
-  TC_CK(ctx->judge_out.ensure(7 * (size_t)nt + 4 * (size_t)nt * nchunk));
+  TC_CK(ctx->judge_out.ensure(7 * (size_t)nt + 8 * (size_t)nt * nchunk));
   TC_CK(cudaMemcpyAsync(ctx->judge_idx.p, idx.data(), nt * sizeof(int), cudaMemcpyHostToDevice, st));
   TcBodies b = bodies_view(ctx, n, jerk);
   TcOut o = out_view(ctx, n, jerk);
   double* part = ctx->judge_out.p + 7 * (size_t)nt;
-  k_direct_targets<<<dim3(nchunk, (nt + kJudgeTile - 1) / kJudgeTile), kJudgeTile, 0, st>>>(n, nt, nchunk,
-                                                                                         ctx->judge_idx.p, b, part);
+  k_direct_targets<false><<<dim3(nchunk, (nt + kJudgeTile - 1) / kJudgeTile), kJudgeTile, 0, st>>>(
+      n, nt, nchunk, ctx->judge_idx.p, b, part);
   k_direct_targets_sum<<<nblocks(nt, 128), 128, 0, st>>>(nt, nchunk, ctx->judge_idx.p, part, o, ctx->judge_out.p);
   ctx->launches += 2;
   std::vector<double> ref(7 * (size_t)nt);
@@ -982,6 +986,7 @@ tc_status tc_destroy(tc_ctx* ctx) {
   ctx->m2l_tl.release(); ctx->p2p_tl.release(); ctx->leaves.release(); ctx->bpart.release();
   ctx->cell_pn.release(); ctx->cls_start.release(); ctx->cls_tl.release(); ctx->mlp_w.release();
   ctx->judge_idx.release(); ctx->judge_out.release();
+  ctx->ds_bod.release(); ctx->ds_out.release(); ctx->ds_flags.release(); ctx->ds_idx.release(); ctx->ds_tgt.release();
   if (ctx->d_root) cudaFree(ctx->d_root);
   if (ctx->d_lv) cudaFree(ctx->d_lv);
   if (ctx->d_cnt) cudaFree(ctx->d_cnt);
@@ -1164,6 +1169,64 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   }
   if ((herr | ctx->tree_flags) & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
   if ((herr | ctx->tree_flags) & TC_EBIT_DEPTH) return TC_ERR_DEPTH;
+  return TC_OK;
+}
+
+tc_status tc_direct_sums(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
+                         const double* vy, const double* vz, const double* m, const unsigned char* flags, int nt,
+                         const int* targets, double* out, int mem) {
+  if (!ctx || n <= 0 || nt <= 0 || !x || !y || !z || !m || !targets || !out) return TC_ERR_ARG;
+  if (mem != TC_MEM_HOST && mem != TC_MEM_DEVICE) return TC_ERR_ARG;
+  const bool jerk = vx && vy && vz;
+  for (int k = 0; k < nt; k++)
+    if (targets[k] < 0 || targets[k] >= n) return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  cudaStream_t st = ctx->stream;
+  const size_t N = (size_t)n;
+  const double *dx = x, *dy = y, *dz = z, *dm = m, *dvx = vx, *dvy = vy, *dvz = vz;
+  const uint8_t* df = flags;
+  if (mem == TC_MEM_HOST) {
+    TC_CK(ctx->in_d.ensure(7 * N));
+    double* s = ctx->in_d.p;
+    const double* src[7] = {x, y, z, m, vx, vy, vz};
+    for (int a = 0; a < 7; a++) {
+      if (!src[a]) continue;
+      TC_CK(cudaMemcpyAsync(s + a * N, src[a], N * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    dx = s; dy = s + N; dz = s + 2 * N; dm = s + 3 * N;
+    dvx = vx ? s + 4 * N : nullptr; dvy = vy ? s + 5 * N : nullptr; dvz = vz ? s + 6 * N : nullptr;
+    if (flags) {
+      TC_CK(ctx->in_f.ensure(N));
+      TC_CK(cudaMemcpyAsync(ctx->in_f.p, flags, N, cudaMemcpyHostToDevice, st));
+      df = ctx->in_f.p;
+    }
+  }
+  // bodies in caller order, in buffers of their own (the last evaluation's state is kept)
+  TC_CK(ctx->ds_bod.ensure(7 * N));
+  TC_CK(ctx->ds_flags.ensure(N));
+  TC_CK(ctx->ds_idx.ensure(N));
+  TcBodies b;
+  double* bb = ctx->ds_bod.p;
+  b.x = bb; b.y = bb + N; b.z = bb + 2 * N; b.m = bb + 3 * N;
+  b.vx = bb + 4 * N; b.vy = bb + 5 * N; b.vz = bb + 6 * N;
+  b.flags = ctx->ds_flags.p;
+  b.perm = ctx->ds_idx.p;
+  k_identity<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->ds_idx.p);
+  k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->ds_idx.p, dx, dy, dz, dm, dvx, dvy, dvz, df, b);
+  const int nchunk = std::max(1, std::min(4 * ctx->nsm, n / 1024));
+  TC_CK(ctx->ds_tgt.ensure(nt));
+  TC_CK(ctx->ds_out.ensure(7 * (size_t)nt + 8 * (size_t)nt * nchunk));
+  TC_CK(cudaMemcpyAsync(ctx->ds_tgt.p, targets, nt * sizeof(int), cudaMemcpyHostToDevice, st));
+  double* part = ctx->ds_out.p + 7 * (size_t)nt;
+  const dim3 grid(nchunk, (nt + kJudgeTile - 1) / kJudgeTile);
+  if (jerk)
+    k_direct_targets<true><<<grid, kJudgeTile, 0, st>>>(n, nt, nchunk, ctx->ds_tgt.p, b, part);
+  else
+    k_direct_targets<false><<<grid, kJudgeTile, 0, st>>>(n, nt, nchunk, ctx->ds_tgt.p, b, part);
+  k_direct_targets_out<<<nblocks(nt, 128), 128, 0, st>>>(nt, nchunk, part, ctx->ds_out.p);
+  TC_CK(cudaMemcpyAsync(out, ctx->ds_out.p, 7 * (size_t)nt * sizeof(double), cudaMemcpyDeviceToHost, st));
+  TC_CK(cudaStreamSynchronize(st));
+  TC_CK(cudaGetLastError());
   return TC_OK;
 }
 

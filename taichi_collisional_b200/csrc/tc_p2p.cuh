@@ -130,20 +130,23 @@ __global__ void k_direct(int n, const TcBodies b, TcOut out) {
   }
 }
 
-// FP64 direct sums at selected bodies (Morton positions): the judge of the selector and an
-// accuracy probe.  Block (c, g) takes the source chunk c and up to 256 targets (one per
-// thread, group g); sources pass through shared memory in tiles, so every body is read
-// once per block.  part[(k * nchunk + c) * 4 + q] = chunk c's (pot, ax, ay, az) of target k.
+// FP64 direct sums at selected bodies: the judge of the selector, and tc_direct_sums.  Block
+// (c, g) takes the source chunk c and up to 256 targets (one per thread, group g); sources pass
+// through shared memory in tiles, so every body is read once per block.
+// part[(k * nchunk + c) * 8 + q] = chunk c's (pot, ax, ay, az, jx, jy, jz) of target k.
 constexpr int kJudgeTile = 256;
+template <bool JERK>
 __global__ void __launch_bounds__(kJudgeTile) k_direct_targets(int n, int nt, int nchunk, const int* __restrict__ tgt,
                                                                const TcBodies b, double* __restrict__ part) {
   __shared__ double sx[kJudgeTile], sy[kJudgeTile], sz[kJudgeTile], sm[kJudgeTile];
+  __shared__ double su[JERK ? kJudgeTile : 1], sv[JERK ? kJudgeTile : 1], sw[JERK ? kJudgeTile : 1];
   const int c = blockIdx.x, k = blockIdx.y * kJudgeTile + threadIdx.x;
   const int chunk = (n + nchunk - 1) / nchunk;
   const int j0 = c * chunk, j1 = min(n, j0 + chunk);
   const int i = k < nt ? tgt[k] : 0;
   const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
-  double pot = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
+  const double ui = JERK ? b.vx[i] : 0.0, vi = JERK ? b.vy[i] : 0.0, wi = JERK ? b.vz[i] : 0.0;
+  double pot = 0.0, ax = 0.0, ay = 0.0, az = 0.0, jx = 0.0, jy = 0.0, jz = 0.0;
   for (int t0 = j0; t0 < j1; t0 += kJudgeTile) {
     const int j = t0 + threadIdx.x;
     __syncthreads();
@@ -152,6 +155,11 @@ __global__ void __launch_bounds__(kJudgeTile) k_direct_targets(int n, int nt, in
       sy[threadIdx.x] = b.y[j];
       sz[threadIdx.x] = b.z[j];
       sm[threadIdx.x] = (b.flags[j] & 2) ? b.m[j] : 0.0;
+      if (JERK) {
+        su[threadIdx.x] = b.vx[j];
+        sv[threadIdx.x] = b.vy[j];
+        sw[threadIdx.x] = b.vz[j];
+      }
     }
     __syncthreads();
     const int cnt = min(kJudgeTile, j1 - t0);
@@ -159,34 +167,51 @@ __global__ void __launch_bounds__(kJudgeTile) k_direct_targets(int n, int nt, in
       const double dx = sx[q] - xi, dy = sy[q] - yi, dz = sz[q] - zi;
       const double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 > 0.0) {
-        const double invr = rsqrt(r2);
+        const double invr = rsqrt(r2), invr2 = invr * invr;
         const double f = sm[q] * invr;
         pot += f;
-        const double f3 = f * invr * invr;
+        const double f3 = f * invr2;
         ax += dx * f3;
         ay += dy * f3;
         az += dz * f3;
+        if (JERK) {
+          const double du = su[q] - ui, dv = sv[q] - vi, dw = sw[q] - wi;
+          const double g = -3.0 * f3 * invr2 * (dx * du + dy * dv + dz * dw);
+          jx += du * f3 + dx * g;
+          jy += dv * f3 + dy * g;
+          jz += dw * f3 + dz * g;
+        }
       }
     }
   }
   if (k < nt) {
-    double* o = part + ((size_t)k * nchunk + c) * 4;
-    o[0] = pot; o[1] = ax; o[2] = ay; o[3] = az;
+    double* o = part + ((size_t)k * nchunk + c) * 8;
+    o[0] = pot; o[1] = ax; o[2] = ay; o[3] = az; o[4] = jx; o[5] = jy; o[6] = jz;
   }
 }
 
-// out[k] = {direct pot, ax, ay, az (chunks summed in order), evaluated ax, ay, az}
+// judge: out[k] = {direct pot, ax, ay, az (chunks summed in order), evaluated ax, ay, az}
 __global__ void k_direct_targets_sum(int nt, int nchunk, const int* __restrict__ tgt, const double* __restrict__ part,
                                      TcOut ev, double* __restrict__ out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nt) return;
   double v[4] = {0.0, 0.0, 0.0, 0.0};
   for (int c = 0; c < nchunk; c++)
-    for (int q = 0; q < 4; q++) v[q] += part[((size_t)k * nchunk + c) * 4 + q];
+    for (int q = 0; q < 4; q++) v[q] += part[((size_t)k * nchunk + c) * 8 + q];
   const int i = tgt[k];
   double* o = out + 7 * (size_t)k;
   o[0] = v[0]; o[1] = v[1]; o[2] = v[2]; o[3] = v[3];
   o[4] = ev.ax[i]; o[5] = ev.ay[i]; o[6] = ev.az[i];
+}
+
+// tc_direct_sums: out[k] = direct (pot, ax, ay, az, jx, jy, jz), chunks summed in order
+__global__ void k_direct_targets_out(int nt, int nchunk, const double* __restrict__ part, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int c = 0; c < nchunk; c++)
+    for (int q = 0; q < 7; q++) v[q] += part[((size_t)k * nchunk + c) * 8 + q];
+  for (int q = 0; q < 7; q++) out[7 * (size_t)k + q] = v[q];
 }
 
 // Morton order -> caller order

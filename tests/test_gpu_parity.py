@@ -185,3 +185,25 @@ def test_large_n_against_direct_sum():
     st = g.stats()
     assert 30e6 < st["n_m2l"] < 40e6  # ~34.4 M at N = 2^20, theta = 0.4, ncrit = 64
     g.close()
+
+
+@pytest.mark.parametrize("device", [False, True])
+def test_direct_sums_match_oracle(device):
+    # tc_direct_sums (the accuracy probe of bench.py) against the oracle's FP64 direct sum,
+    # with jerks, from host arrays and from device tensors
+    n = 20000
+    x, y, z, vx, vy, vz, m = ics.plummer_kroupa(n, 5)
+    idx = np.random.default_rng(5).choice(n, 300, replace=False)
+    ref = oracle.direct(x, y, z, m, vx, vy, vz, targets=idx)
+    g = tcb.Gravity(p=8, ncrit=64, theta=0.5, variant=tcb.VARIANT_JERKS)
+    args = (x, y, z, m)
+    vel = (vx, vy, vz)
+    if device:
+        import torch
+        args = tuple(torch.tensor(a, device="cuda") for a in args)
+        vel = tuple(torch.tensor(a, device="cuda") for a in vel)
+    got = g.direct_sums(*args, idx, *vel)
+    g.close()
+    assert rel_err(got["pot"], ref["pot"]).max() < 1e-12
+    assert rel_vec_err(vec(got, "a"), vec(ref, "a")).max() < 1e-12
+    assert rel_vec_err(vec(got, "j"), vec(ref, "j")).max() < 1e-11

@@ -198,6 +198,19 @@ const char* tc_last_error_string(tc_ctx* ctx);
 int tc_pmax(void);
 /* 1 if expansion order p has compiled kernels in this build. */
 int tc_order_supported(int p);
+/* get_force_and_potential(bodies, true) of the top-level tree (integrator.h:459-562 with
+ * get_steps; traverse_eager.h:151-203): the time-step pass.  As in the reference, no M2L is
+ * done -- pot and acc are the near-field (P2P) parts only -- and every P2P pair adds the
+ * pairwise criterion of kernel_fast_lean.h:462-548: timestep[i] = sum over the body's P2P
+ * source cells of 1 / tau_min^4 (the reference's Body::timestep after the call; its
+ * integrator takes 1 / sqrt(sqrt(timestep))).  dt_param is the reference's dt_param
+ * (exafmm.h:109).  Velocities are required.  Always builds the tree.  Returns
+ * TC_ERR_UNSUPPORTED for the jerks tree, whose theta path has no time-step pass
+ * (taichi_with_jerks/traverse_eager.h:125-155 ignores get_steps); use tc_evaluate there. */
+tc_status tc_evaluate_steps(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
+                            const double* vy, const double* vz, const double* m, const unsigned char* flags,
+                            double dt_param, double* ax, double* ay, double* az, double* pot, double* timestep,
+                            int mem);
 /* FP64 direct sums at nt target bodies (caller indices targets[k] in [0, n)) over all n bodies
  * (no softening; r = 0 skipped; sources are the bodies with flag bit 1, all if flags is NULL):
  * out[7k..7k+6] = pot, ax, ay, az, jx, jy, jz (jerk zero unless vx, vy, vz are given).

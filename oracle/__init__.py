@@ -66,6 +66,9 @@ def lib():
         L = C.CDLL(path)
         L.tco_evaluate.argtypes = [C.POINTER(Params), C.c_int] + [_dp] * 7 + [_u8p] + [_dp] * 7 + [C.POINTER(Stats)]
         L.tco_evaluate.restype = C.c_int
+        L.tco_evaluate_steps.argtypes = [C.POINTER(Params), C.c_double, C.c_int] + [_dp] * 7 + [_u8p] + [_dp] * 5 + \
+            [C.POINTER(Stats)]
+        L.tco_evaluate_steps.restype = C.c_int
         L.tco_last_ncell.restype = C.c_int
         L.tco_last_cells.argtypes = [_ip] * 5 + [_dp, _dp, _ip]
         L.tco_last_expansions.argtypes = [_dp] * 4
@@ -107,6 +110,26 @@ def evaluate(x, y, z, m, vx=None, vy=None, vz=None, *, p, theta, ncrit, variant=
                         *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")], C.byref(st))
     if rc != 0:
         raise RuntimeError("oracle evaluate failed (%d)" % rc)
+    out["stats"] = {f: getattr(st, f) for f, _ in Stats._fields_}
+    return out
+
+
+def evaluate_steps(x, y, z, m, vx, vy, vz, *, p, theta, ncrit, dt_param, flags=None):
+    """Oracle time-step pass of the top-level tree (get_steps = true); returns dict(ax, ay,
+    az, pot, timestep, stats), timestep = each body's sum of 1 / tau^4."""
+    L = lib()
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    vx, vy, vz = map(_f64, (vx, vy, vz))
+    prm = Params(p=p, ncrit=ncrit, variant=VARIANT_TOP, use_shift=0, theta=theta, direct_below=0)
+    out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot", "timestep")}
+    st = Stats()
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    rc = L.tco_evaluate_steps(C.byref(prm), dt_param, n, _d(x), _d(y), _d(z), _d(vx), _d(vy), _d(vz), _d(m),
+                              None if fl is None else fl.ctypes.data_as(_u8p),
+                              *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "timestep")], C.byref(st))
+    if rc != 0:
+        raise RuntimeError("oracle evaluate_steps failed (%d)" % rc)
     out["stats"] = {f: getattr(st, f) for f, _ in Stats._fields_}
     return out
 
@@ -186,6 +209,10 @@ def ref_lib(variant, p):
         L.tcr_list.argtypes = [C.c_int, _ip, _ip]
         L.tcr_list.restype = C.c_longlong
         L.tcr_shift_uniforms.argtypes = [C.c_long, _dp]
+        if hasattr(L, "tcr_evaluate_steps"):
+            L.tcr_evaluate_steps.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_double,
+                                                                     C.c_int] + [_dp] * 5
+            L.tcr_evaluate_steps.restype = C.c_int
         _ref_libs[key] = L
     return _ref_libs[key]
 
@@ -211,6 +238,21 @@ def ref_evaluate(x, y, z, m, vx=None, vy=None, vz=None, *, p, theta, ncrit, vari
                         *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")], _d(times))
     out["ncell"] = nc
     out["times"] = times
+    return out
+
+
+def ref_evaluate_steps(x, y, z, m, vx, vy, vz, *, p, theta, ncrit, dt_param, nthreads=1, flags=None):
+    """The reference's own time-step pass (top-level tree, horizontalPass with get_steps)."""
+    L = ref_lib(VARIANT_TOP, p)
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    vx, vy, vz = map(_f64, (vx, vy, vz))
+    out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot", "timestep")}
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    nc = L.tcr_evaluate_steps(n, _d(x), _d(y), _d(z), _d(vx), _d(vy), _d(vz), _d(m),
+                              None if fl is None else fl.ctypes.data_as(_u8p), theta, ncrit, dt_param, nthreads,
+                              *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "timestep")])
+    out["ncell"] = nc
     return out
 
 

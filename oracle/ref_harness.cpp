@@ -62,6 +62,11 @@ static void record(Cell* Ci, Cell* Cj) {
   }
 }
 
+static int run(int n, const double* x, const double* y, const double* z, const double* vx, const double* vy,
+               const double* vz, const double* m, const unsigned char* flags, double th, int nc, long seed,
+               int nthreads, double* ax, double* ay, double* az, double* pot, double* jx, double* jy,
+               double* jz, double* times, bool get_steps, double* timestep);
+
 extern "C" {
 
 int tcr_expansion(void) { return EXPANSION; }
@@ -80,6 +85,28 @@ int tcr_evaluate(int n, const double* x, const double* y, const double* z, const
                  const double* vy, const double* vz, const double* m, const unsigned char* flags,
                  double th, int nc, long seed, int nthreads, double* ax, double* ay, double* az,
                  double* pot, double* jx, double* jy, double* jz, double* times) {
+  return run(n, x, y, z, vx, vy, vz, m, flags, th, nc, seed, nthreads, ax, ay, az, pot, jx, jy, jz, times,
+             false, NULL);
+}
+
+// The same evaluation with get_steps = true (horizontalPass(cells, cells, 0, true)): the
+// time-step pass of the top-level tree (no M2L; P2P with the pairwise criterion,
+// kernel_fast_lean.h:462-548).  timestep[i] = the body's accumulated sum of 1/tau^4.
+int tcr_evaluate_steps(int n, const double* x, const double* y, const double* z, const double* vx,
+                       const double* vy, const double* vz, const double* m, const unsigned char* flags,
+                       double th, int nc, double dtp, int nthreads, double* ax, double* ay, double* az,
+                       double* pot, double* timestep) {
+  dt_param = dtp;
+  return run(n, x, y, z, vx, vy, vz, m, flags, th, nc, 1, nthreads, ax, ay, az, pot, NULL, NULL, NULL, NULL,
+             true, timestep);
+}
+
+}  // extern "C"
+
+static int run(int n, const double* x, const double* y, const double* z, const double* vx, const double* vy,
+               const double* vz, const double* m, const unsigned char* flags, double th, int nc, long seed,
+               int nthreads, double* ax, double* ay, double* az, double* pot, double* jx, double* jy,
+               double* jz, double* times, bool get_steps, double* timestep) {
   if (!g_init) {
     P = EXPANSION;
     initKernel();
@@ -113,7 +140,7 @@ int tcr_evaluate(int n, const double* x, const double* y, const double* z, const
   for (size_t c = 0; c < g_cells.size(); c++) g_cells[c].has_sink = false;
   upwardPass(g_cells);
   double t2 = now_s();
-  horizontalPass(g_cells, g_cells, 0, false);
+  horizontalPass(g_cells, g_cells, 0, get_steps);
   double t3 = now_s();
   downwardPass(g_cells);
   double t4 = now_s();
@@ -124,6 +151,7 @@ int tcr_evaluate(int n, const double* x, const double* y, const double* z, const
     const Body& B = bodies[b];
     int i = B.index;
     ax[i] = B.F[0]; ay[i] = B.F[1]; az[i] = B.F[2]; pot[i] = B.p;
+    if (timestep) timestep[i] = B.timestep;
 #ifdef TCR_JERKS
     if (jx) { jx[i] = B.J[0]; jy[i] = B.J[1]; jz[i] = B.J[2]; }
 #else
@@ -133,6 +161,8 @@ int tcr_evaluate(int n, const double* x, const double* y, const double* z, const
   for (int k = 0; k < 2; k++) { g_list_t[k].clear(); g_list_s[k].clear(); }
   return (int)g_cells.size();
 }
+
+extern "C" {
 
 // Cells of the last evaluation in the reference's own order.
 void tcr_cells(int* begin, int* nbody, int* nchild, int* child, double* X, double* R, int* index) {

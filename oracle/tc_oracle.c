@@ -756,6 +756,53 @@ static void p2p(int ci, int cj, double* out) {
   }
 }
 
+/* P2P in the time-step pass (get_steps, top-level tree): kernel_fast_lean.h:462-548 (the
+ * SIMD / DOUBLE_P2P branch the reference builds with).  Per target i and this source cell:
+ * acc and pot as in P2P_simple (sources only), and the pairwise step
+ *   tau1 = dt/sqrt2 r sqrt(r/mi) / (1 - dtau1/2),  dtau1 = min(1, 3/2 tau1 (d.dv)/r^2)
+ *   tau2 = dt r/|dv|       / (1 - dtau2/2),  dtau2 = min(1, tau2 (d.dv)/r^2 (1 + mi/(v^2 r)))
+ * minimised over the cell's bodies; the target's timestep gains 1/min^4.  As in the
+ * reference, mi starts at the target's mass and accumulates every body of the cell met so
+ * far (sources or not, self excluded), in the cell's body order. */
+static void p2p_steps(int ci, int cj, double dtp, double* out, double* ts) {
+  for (int i = T.begin[ci]; i < T.begin[ci] + T.nbody[ci]; i++) {
+    double ax = 0, ay = 0, az = 0, pot = 0, tmin = 1e38, mi = T.m[i];
+    for (int j = T.begin[cj]; j < T.begin[cj] + T.nbody[cj]; j++) {
+      double mj = T.m[j];
+      double dx = T.x[j] - T.x[i], dy = T.y[j] - T.y[i], dz = T.z[j] - T.z[i];
+      double dvx = T.vx[j] - T.vx[i], dvy = T.vy[j] - T.vy[i], dvz = T.vz[j] - T.vz[i];
+      double r2 = dx * dx + dy * dy + dz * dz;
+      double v2 = dvx * dvx + dvy * dvy + dvz * dvz + 1e-20;
+      if (!(r2 > 0)) { mj = 0; r2 = 1e38; }
+      mi += mj;
+      double vdotdr2 = (dx * dvx + dy * dvy + dz * dvz) / r2;
+      double r = sqrt(r2), invr = 1 / r;
+      double tau = dtp / M_SQRT2 * r * sqrt(r / mi);
+      double dtau = 3 * tau * vdotdr2 / 2;
+      if (!(dtau < 1)) dtau = 1;
+      tau /= (1 - dtau / 2);
+      if (tau < tmin) tmin = tau;
+      tau = dtp * r / sqrt(v2);
+      dtau = tau * vdotdr2 * (1 + mi / (v2 * r));
+      if (!(dtau < 1)) dtau = 1;
+      tau /= (1 - dtau / 2);
+      if (tau < tmin) tmin = tau;
+      mj *= invr;
+      if (T.source[j]) {
+        pot += mj;
+        double f = mj * (invr * invr);
+        ax += dx * f; ay += dy * f; az += dz * f;
+      }
+    }
+    tmin *= tmin;
+    tmin *= tmin;
+    if (!T.sink[i]) continue;
+    double* o = out + 7 * (size_t)i;
+    o[0] += pot; o[1] += ax; o[2] += ay; o[3] += az;
+    ts[i] += 1 / tmin;
+  }
+}
+
 static void free_tree(void) {
   free(T.perm); free(T.x); free(T.y); free(T.z); free(T.vx); free(T.vy); free(T.vz); free(T.m);
   free(T.sink); free(T.source); free(T.X); free(T.R); free(T.has_sink);
@@ -793,10 +840,33 @@ void tco_direct(int n, const double* x, const double* y, const double* z, const 
   }
 }
 
+static int evaluate(const tco_params* prm, int n, const double* x, const double* y, const double* z,
+                    const double* vx, const double* vy, const double* vz, const double* m,
+                    const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                    double* jx, double* jy, double* jz, tco_stats* st, int steps, double dtp,
+                    double* timestep);
+
 int tco_evaluate(const tco_params* prm, int n, const double* x, const double* y, const double* z,
                  const double* vx, const double* vy, const double* vz, const double* m,
                  const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
                  double* jx, double* jy, double* jz, tco_stats* st) {
+  return evaluate(prm, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, st, 0, 0.0, NULL);
+}
+
+int tco_evaluate_steps(const tco_params* prm, double dt_param, int n, const double* x, const double* y,
+                       const double* z, const double* vx, const double* vy, const double* vz, const double* m,
+                       const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                       double* timestep, tco_stats* st) {
+  if (prm->variant != TCO_VARIANT_TOP || !timestep) return -1;
+  return evaluate(prm, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, NULL, NULL, NULL, st, 1, dt_param,
+                  timestep);
+}
+
+static int evaluate(const tco_params* prm, int n, const double* x, const double* y, const double* z,
+                    const double* vx, const double* vy, const double* vz, const double* m,
+                    const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                    double* jx, double* jy, double* jz, tco_stats* st, int steps, double dtp,
+                    double* timestep) {
   if (n <= 0 || prm->p < 1 || prm->p > PMAX_O) return -1;
   int jerk = prm->variant == TCO_VARIANT_JERKS;
   free_tree();
@@ -817,7 +887,8 @@ int tco_evaluate(const tco_params* prm, int n, const double* x, const double* y,
     T.source[i] = flags ? ((flags[i] >> 1) & 1) : 1;
   }
   double* out = calloc((size_t)7 * n, sizeof(double));
-  if (n < prm->direct_below) {
+  double* ts = steps ? calloc((size_t)n, sizeof(double)) : NULL;
+  if (n < prm->direct_below && !steps) {
     /* direct(), traverse_eager.h:349-370: every target against every source */
     for (int i = 0; i < n; i++) T.perm[i] = i;
     T.ncell = 0;
@@ -856,6 +927,13 @@ int tco_evaluate(const tco_params* prm, int n, const double* x, const double* y,
     }
     upward();
     horizontal(0, 0);
+    if (steps) {
+      /* time-step pass (traverse_eager.h:151-203 with get_steps): no M2L, no local
+       * expansions; every recorded P2P pair with the criterion */
+      for (long long k = 0; k < T.np2p; k++)
+        if (T.has_sink[T.p2p_t[k]]) p2p_steps(T.p2p_t[k], T.p2p_s[k], dtp, out, ts);
+      goto done;
+    }
     /* M2L over the visited pairs (top: mutual form, kernel_fast_lean.h:1036 -> one call
      * per direction, skipped when neither cell has a sink; jerks: one-sided). */
     for (long long k = 0; k < T.nm2l; k++) {
@@ -892,11 +970,13 @@ int tco_evaluate(const tco_params* prm, int n, const double* x, const double* y,
       }
     }
   }
+done:
   for (int s = 0; s < n; s++) {
     int i = T.perm[s];
     const double* o = out + 7 * (size_t)s;
     pot[i] = o[0]; ax[i] = o[1]; ay[i] = o[2]; az[i] = o[3];
     if (jx) { jx[i] = o[4]; jy[i] = o[5]; jz[i] = o[6]; }
+    if (ts) timestep[i] = ts[s];
   }
   if (st) {
     st->n_cells = T.ncell;
@@ -911,6 +991,7 @@ int tco_evaluate(const tco_params* prm, int n, const double* x, const double* y,
     st->max_level = T.max_level;
   }
   free(out);
+  free(ts);
   return 0;
 }
 

@@ -42,6 +42,16 @@ int tco_evaluate(const tco_params* prm, int n, const double* x, const double* y,
                  const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
                  double* jx, double* jy, double* jz, tco_stats* st);
 
+/* The time-step pass of the top-level tree (get_force_and_potential(bodies, true) on the
+ * theta path: traverse_eager.h:151-203 with get_steps, P2P of kernel_fast_lean.h:462-548):
+ * no M2L; near-field pot/acc only; timestep[i] = sum over the body's P2P source cells of
+ * 1/tau_min^4 (dt_param scales tau).  Always builds the tree (n < ncrit gives one leaf).
+ * Returns -1 for the jerks tree, whose theta path has no time-step pass. */
+int tco_evaluate_steps(const tco_params* prm, double dt_param, int n, const double* x, const double* y,
+                       const double* z, const double* vx, const double* vy, const double* vz, const double* m,
+                       const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                       double* timestep, tco_stats* st);
+
 /* Tree of the last tco_evaluate call (reference cell order: depth-first, child blocks
  * allocated when the parent is split).  Arrays sized by tco_last_ncell()/n. */
 int tco_last_ncell(void);

@@ -59,7 +59,7 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
-           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums"]
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -129,6 +129,9 @@ def load_library(path=LIB_PATH):
     L.tc_tc_bins.restype = C.c_int
     L.tc_direct_sums.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8 + [C.c_int, _ip, _dp, C.c_int]
     L.tc_direct_sums.restype = C.c_int
+    L.tc_evaluate_steps.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8 + [C.c_double] + [C.c_void_p] * 5 + \
+        [C.c_int]
+    L.tc_evaluate_steps.restype = C.c_int
     _lib = L
     return L
 
@@ -222,6 +225,27 @@ class Gravity:
                                  _ptr(out.get("jx")), _ptr(out.get("jy")), _ptr(out.get("jz")),
                                  MEM_DEVICE if dev else MEM_HOST)
         self._check(rc, "tc_evaluate")
+        return out
+
+    def evaluate_steps(self, x, y, z, m, vx, vy, vz, dt_param, flags=None):
+        """The time-step pass of the top-level tree (get_force_and_potential(bodies, true)):
+        dict ax, ay, az, pot (near field only, as in the reference) and timestep (each body's
+        sum of 1 / tau^4), numpy or CUDA tensors like the inputs."""
+        n = len(x)
+        dev = hasattr(x, "data_ptr")
+        if dev:
+            import torch
+            out = {k: torch.empty(n, dtype=torch.float64, device=x.device) for k in ("ax", "ay", "az", "pot", "timestep")}
+        else:
+            out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot", "timestep")}
+            x, y, z, m, vx, vy, vz = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, m, vx, vy, vz))
+            if flags is not None:
+                flags = np.ascontiguousarray(flags, dtype=np.uint8)
+        rc = self._L.tc_evaluate_steps(self._h, n, _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(m),
+                                       _ptr(flags), float(dt_param), _ptr(out["ax"]), _ptr(out["ay"]),
+                                       _ptr(out["az"]), _ptr(out["pot"]), _ptr(out["timestep"]),
+                                       MEM_DEVICE if dev else MEM_HOST)
+        self._check(rc, "tc_evaluate_steps")
         return out
 
     def direct_sums(self, x, y, z, m, targets, vx=None, vy=None, vz=None, flags=None):

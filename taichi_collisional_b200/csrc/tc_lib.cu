@@ -109,6 +109,10 @@ struct tc_ctx {
   int judge_redo = 0;
   DBuf<int> judge_idx;
   DBuf<double> judge_out;
+  // time-step pass (tc_evaluate_steps): per-body sum of 1/tau^4 in Morton order
+  bool steps = false;
+  double dt_param = 0.025;
+  DBuf<double> tsum;
   // tc_direct_sums: bodies in caller order, targets, partial and final sums
   DBuf<double> ds_bod, ds_out;
   DBuf<uint8_t> ds_flags;
@@ -292,7 +296,8 @@ static TcBodies bodies_view(tc_ctx* c, int n, bool jerk) {
   double* d = c->bod.p;
   size_t N = (size_t)n;
   b.x = d; b.y = d + N; b.z = d + 2 * N; b.m = d + 3 * N;
-  b.vx = jerk ? d + 4 * N : nullptr; b.vy = jerk ? d + 5 * N : nullptr; b.vz = jerk ? d + 6 * N : nullptr;
+  const bool vel = jerk || c->steps;  // the time-step pass needs velocities in the top tree too
+  b.vx = vel ? d + 4 * N : nullptr; b.vy = vel ? d + 5 * N : nullptr; b.vz = vel ? d + 6 * N : nullptr;
   b.flags = c->bflags.p;
   b.perm = c->perm.p;
   return b;
@@ -715,7 +720,9 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   ctx->class_order[0] = P;
   ctx->class_pairs[0] = (long long)ctx->n_m2l;
   ctx->flop_frac = 1.0;
-  if (hs[0] > 0 && prm.selector > 0 && !mixed && TcOrderClasses<P>::n > 1) {
+  if (ctx->steps) {
+    // time-step pass: no far field (the reference skips M2L when get_steps is set)
+  } else if (hs[0] > 0 && prm.selector > 0 && !mixed && TcOrderClasses<P>::n > 1) {
     cudaError_t ce = run_m2l_classes<P, JERK>(ctx, cv);
     if (ce != cudaSuccess) return cuda_fail(ctx, ce, "far field by order class");
   } else if (hs[0] > 0) {
@@ -740,7 +747,18 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[4], st);
-  if (hs[1] > 0) {
+  if (ctx->steps) {
+    TC_CK(ctx->tsum.ensure((size_t)n));
+    TC_CK(cudaMemsetAsync(ctx->tsum.p, 0, sizeof(double) * (size_t)n, st));
+  }
+  if (hs[1] > 0 && ctx->steps) {
+    if constexpr (!JERK) {
+      k_p2p_steps<<<nblocks(hs[1], kP2PWarps), kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p,
+                                                                        ctx->p2p_src.p, b, cv, o, ctx->dt_param,
+                                                                        ctx->tsum.p);
+      ctx->launches++;
+    }
+  } else if (hs[1] > 0) {
     int g = nblocks(hs[1], kP2PWarps);
     if (mixed_p2p)
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b,
@@ -750,7 +768,11 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[5], st);
-  // ---- downward
+  // ---- downward (nothing to add in the time-step pass: every local expansion is zero)
+  if (ctx->steps) {
+    if (ctx->events) cudaEventRecord(ctx->ev[6], st);
+    return TC_OK;
+  }
   ctx->launches += maxl + (ctx->nleaf > 0);
   for (int l = 1; l <= maxl; l++) {
     int cnt = ctx->lv.count[l];
@@ -987,6 +1009,7 @@ tc_status tc_destroy(tc_ctx* ctx) {
   ctx->cell_pn.release(); ctx->cls_start.release(); ctx->cls_tl.release(); ctx->mlp_w.release();
   ctx->judge_idx.release(); ctx->judge_out.release();
   ctx->ds_bod.release(); ctx->ds_out.release(); ctx->ds_flags.release(); ctx->ds_idx.release(); ctx->ds_tgt.release();
+  ctx->tsum.release();
   if (ctx->d_root) cudaFree(ctx->d_root);
   if (ctx->d_lv) cudaFree(ctx->d_lv);
   if (ctx->d_cnt) cudaFree(ctx->d_cnt);
@@ -1004,9 +1027,37 @@ tc_status tc_set_stream(tc_ctx* ctx, void* stream) {
   return TC_OK;
 }
 
+static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+                               const double* vx, const double* vy, const double* vz, const double* m,
+                               const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                               double* jx, double* jy, double* jz, int mem, double* timestep);
+
 tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
                       const double* vy, const double* vz, const double* m, const unsigned char* flags, double* ax,
                       double* ay, double* az, double* pot, double* jx, double* jy, double* jz, int mem) {
+  if (!ctx) return TC_ERR_ARG;
+  ctx->steps = false;
+  return evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, mem, nullptr);
+}
+
+tc_status tc_evaluate_steps(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
+                            const double* vy, const double* vz, const double* m, const unsigned char* flags,
+                            double dt_param, double* ax, double* ay, double* az, double* pot, double* timestep,
+                            int mem) {
+  if (!ctx || !vx || !vy || !vz || !timestep) return TC_ERR_ARG;
+  if (ctx->prm.variant != TC_VARIANT_TOP) return TC_ERR_UNSUPPORTED;
+  ctx->steps = true;
+  ctx->dt_param = dt_param;
+  tc_status r = evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, nullptr, nullptr, nullptr, mem,
+                              timestep);
+  ctx->steps = false;
+  return r;
+}
+
+static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+                               const double* vx, const double* vy, const double* vz, const double* m,
+                               const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                               double* jx, double* jy, double* jz, int mem, double* timestep) {
   if (!ctx || n <= 0 || !x || !y || !z || !m || !ax || !ay || !az || !pot) return TC_ERR_ARG;
   const bool jerk = ctx->prm.variant == TC_VARIANT_JERKS;
   if (jerk && (!vx || !vy || !vz)) return TC_ERR_ARG;
@@ -1046,7 +1097,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   TC_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));
   int direct_below = ctx->prm.direct_below;
   if (direct_below < 0) direct_below = jerk ? 8000 : ctx->prm.ncrit;
-  ctx->direct = n < direct_below;
+  ctx->direct = n < direct_below && !ctx->steps;  // the time-step pass always builds the tree
   TcBodies b = bodies_view(ctx, n, jerk);
   TcOut o = out_view(ctx, n, jerk);
   tc_status rs = TC_OK;
@@ -1095,7 +1146,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   // ---- judge: FP64 direct sums at seeded bodies; a rejected selector step is redone at fixed p
   ctx->judge_rms = 0.0;
   ctx->judge_redo = 0;
-  if (ctx->prm.judge_n > 0) {
+  if (ctx->prm.judge_n > 0 && !ctx->steps) {
     int nt = std::min(ctx->prm.judge_n, n);
     double rms = 0.0;
     tc_status js = judge(ctx, n, nt, jerk, &rms);
@@ -1116,14 +1167,20 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
   }
   // ---- outputs to the caller's order
   double *opot = pot, *oax = ax, *oay = ay, *oaz = az, *ojx = jx, *ojy = jy, *ojz = jz;
+  double* ots = timestep;
   if (mem == TC_MEM_HOST) {
-    TC_CK(ctx->out_d.ensure(7 * N));
+    TC_CK(ctx->out_d.ensure(8 * N));
     double* s = ctx->out_d.p;
     opot = s; oax = s + N; oay = s + 2 * N; oaz = s + 3 * N;
     ojx = jx ? s + 4 * N : nullptr; ojy = jx ? s + 5 * N : nullptr; ojz = jx ? s + 6 * N : nullptr;
+    ots = s + 7 * N;
   }
   k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, o, opot, oax, oay, oaz, ojx, ojy, ojz);
   ctx->launches++;
+  if (timestep) {
+    k_scatter_one<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, ctx->tsum.p, ots);
+    ctx->launches++;
+  }
   if (ctx->events) cudaEventRecord(ctx->ev[7], st);
   unsigned herr = 0;
   TC_CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -1134,6 +1191,7 @@ tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, cons
       if (!dst[a] || (a >= 4 && !jx)) continue;
       TC_CK(cudaMemcpyAsync(dst[a], s + a * N, N * sizeof(double), cudaMemcpyDeviceToHost, st));
     }
+    if (timestep) TC_CK(cudaMemcpyAsync(timestep, s + 7 * N, N * sizeof(double), cudaMemcpyDeviceToHost, st));
   }
   TC_CK(cudaStreamSynchronize(st));
   TC_CK(cudaGetLastError());

@@ -214,6 +214,92 @@ __global__ void k_direct_targets_out(int nt, int nchunk, const double* __restric
   for (int q = 0; q < 7; q++) out[7 * (size_t)k + q] = v[q];
 }
 
+// Time-step pass of the top-level tree (get_force_and_potential(bodies, true) on the theta
+// path): P2P of kernel_fast_lean.h:462-548 (the SIMD / DOUBLE_P2P branch), in FP64.  For a
+// target body and one source cell: pot and acc from the cell's sources as in P2P_simple, and
+// the pairwise step
+//   tau1 = dt/sqrt2 r sqrt(r/mi) / (1 - dtau1/2),  dtau1 = min(1, 3/2 tau1 (d.dv)/r^2)
+//   tau2 = dt r/|dv|       / (1 - dtau2/2),  dtau2 = min(1, tau2 (d.dv)/r^2 (1 + mi/(v^2 r)))
+// minimised over the cell's bodies; the target's step sum gains 1/min^4.  As in the
+// reference, mi starts at the target's mass and accumulates every body of the cell met so far
+// (sources or not, self excluded) in the cell's body order, so each lane (one target) walks
+// each source cell's bodies in order.  One warp per target cell.
+__global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_steps(const int* __restrict__ tlist, int ntl,
+                                                              const int* __restrict__ tstart,
+                                                              const int* __restrict__ src, const TcBodies b,
+                                                              const TcCells c, TcOut out, double dtp,
+                                                              double* __restrict__ tsum) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double dts = dtp / 1.41421356237309504880;  // dt_param / M_SQRT2
+  for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
+    const int t = tlist[k];
+    if (!c.has_sink[t]) continue;
+    const int tb = c.begin[t], nt = c.nbody[t];
+    const int sb = tstart[t], se = tstart[t + 1];
+    for (int t0 = 0; t0 < nt; t0 += 32) {
+      const bool vi = t0 + lane < nt;
+      const int i = tb + (vi ? t0 + lane : 0);
+      const double xi = b.x[i], yi = b.y[i], zi = b.z[i], ui = b.vx[i], vvi = b.vy[i], wi = b.vz[i];
+      const double m0 = b.m[i];
+      double pot = 0.0, ax = 0.0, ay = 0.0, az = 0.0, ts = 0.0;
+      for (int q = sb; q < se; q++) {
+        const int sc = src[q];
+        const int jb = c.begin[sc], jn = c.nbody[sc];
+        double mi = m0, tmin = 1e38;
+        for (int j = jb; j < jb + jn; j++) {
+          double mj = b.m[j];
+          const double dx = b.x[j] - xi, dy = b.y[j] - yi, dz = b.z[j] - zi;
+          const double du = b.vx[j] - ui, dv = b.vy[j] - vvi, dw = b.vz[j] - wi;
+          double r2 = dx * dx + dy * dy + dz * dz;
+          const double v2 = du * du + dv * dv + dw * dw + 1e-20;
+          if (!(r2 > 0.0)) {
+            mj = 0.0;
+            r2 = 1e38;
+          }
+          mi += mj;
+          const double vdotdr2 = (dx * du + dy * dv + dz * dw) / r2;
+          const double r = sqrt(r2), invr = 1.0 / r;
+          double tau = dts * r * sqrt(r / mi);
+          double dtau = 3.0 * tau * vdotdr2 / 2.0;
+          if (!(dtau < 1.0)) dtau = 1.0;
+          tau /= (1.0 - dtau / 2.0);
+          tmin = tau < tmin ? tau : tmin;
+          tau = dtp * r / sqrt(v2);
+          dtau = tau * vdotdr2 * (1.0 + mi / (v2 * r));
+          if (!(dtau < 1.0)) dtau = 1.0;
+          tau /= (1.0 - dtau / 2.0);
+          tmin = tau < tmin ? tau : tmin;
+          mj *= invr;
+          if (b.flags[j] & 2) {
+            pot += mj;
+            const double f = mj * (invr * invr);
+            ax += dx * f;
+            ay += dy * f;
+            az += dz * f;
+          }
+        }
+        tmin *= tmin;
+        tmin *= tmin;
+        ts += 1.0 / tmin;
+      }
+      if (vi && (b.flags[i] & 1)) {
+        out.pot[i] += pot;
+        out.ax[i] += ax;
+        out.ay[i] += ay;
+        out.az[i] += az;
+        tsum[i] += ts;
+      }
+    }
+  }
+}
+
+// one array, Morton order -> caller order
+__global__ void k_scatter_one(int n, const int* __restrict__ perm, const double* __restrict__ s,
+                              double* __restrict__ d) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[perm[i]] = s[i];
+}
+
 // Morton order -> caller order
 __global__ void k_scatter_out(int n, const int* __restrict__ perm, TcOut s, double* pot, double* ax, double* ay,
                               double* az, double* jx, double* jy, double* jz) {

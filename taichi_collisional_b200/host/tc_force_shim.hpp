@@ -13,8 +13,15 @@
 // Unlike the reference, `bodies` keeps its order (results are written in place, so the
 // Body::index round trip still works but is no longer needed).
 //
-// get_steps == true (the pairwise time-step criterion of P2P, kernel_fast_lean.h:548-574) is
-// not provided by the library; the shim stops the run with the reference's ENDRUN.
+// get_steps == true: for the top-level tree, the time-step pass of the reference
+// (tc_evaluate_steps: no M2L, near-field F and p, Body::timestep = sum of 1/tau^4 from the
+// pairwise criterion of kernel_fast_lean.h:462-548, with the global dt_param); for the jerks
+// tree the reference's theta path ignores get_steps (taichi_with_jerks/traverse_eager.h:
+// 125-155), and so does the shim.  Body::timestep is otherwise reset as the reference does
+// (0 for the top-level tree, integrator.h:500-507; HUGE for the jerks tree,
+// taichi_with_jerks/integrator.h:352-364).  Body::acc_old is left unchanged: the reference
+// fills it from its low-order pre-pass, which belongs to the error-controlled MAC path, not to
+// the theta path implemented here.
 #pragma once
 #include <vector>
 
@@ -43,10 +50,12 @@ inline tc_ctx* tc_shim_context() {
 }
 
 inline void get_force_and_potential(Bodies& bodies, bool get_steps) {
-  if (get_steps) ENDRUN("get_force_and_potential(get_steps=true) is not provided by taichi_b200\n");
+#ifdef TC_SHIM_JERKS
+  get_steps = false;
+#endif
   const int n = (int)bodies.size();
   std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), m(n), ax(n), ay(n), az(n), pot(n), jx(n), jy(n),
-      jz(n);
+      jz(n), ts(n);
   std::vector<unsigned char> flags(n);
   for (int i = 0; i < n; i++) {
     const Body& b = bodies[i];
@@ -55,10 +64,18 @@ inline void get_force_and_potential(Bodies& bodies, bool get_steps) {
     m[i] = b.q;
     flags[i] = (unsigned char)((b.issink ? 1 : 0) | (b.issource ? 2 : 0));
   }
-  tc_status s = tc_evaluate(tc_shim_context(), n, x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(),
-                            m.data(), flags.data(), ax.data(), ay.data(), az.data(), pot.data(), jx.data(),
-                            jy.data(), jz.data(), TC_MEM_HOST);
-  if (s != TC_OK) ENDRUN("tc_evaluate: %s\n", tc_status_string(s));
+  tc_status s;
+#ifndef TC_SHIM_JERKS
+  if (get_steps)
+    s = tc_evaluate_steps(tc_shim_context(), n, x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(),
+                          m.data(), flags.data(), dt_param, ax.data(), ay.data(), az.data(), pot.data(), ts.data(),
+                          TC_MEM_HOST);
+  else
+#endif
+    s = tc_evaluate(tc_shim_context(), n, x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(), m.data(),
+                    flags.data(), ax.data(), ay.data(), az.data(), pot.data(), jx.data(), jy.data(), jz.data(),
+                    TC_MEM_HOST);
+  if (s != TC_OK) ENDRUN("taichi_b200 force evaluation: %s\n", tc_status_string(s));
   for (int i = 0; i < n; i++) {
     Body& b = bodies[i];
     // the reference's FMM branch resets F, p (and J) before accumulating
@@ -67,6 +84,9 @@ inline void get_force_and_potential(Bodies& bodies, bool get_steps) {
     b.p = pot[i];
 #ifdef TC_SHIM_JERKS
     b.J[0] = jx[i]; b.J[1] = jy[i]; b.J[2] = jz[i];
+    b.timestep = HUGE;
+#else
+    b.timestep = get_steps ? ts[i] : 0;
 #endif
   }
 }

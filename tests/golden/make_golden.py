@@ -8,7 +8,11 @@ Run from the repository root, where the reference tree is available and
 
 Each case stores its inputs, the reference's per-body outputs (single-threaded, so the
 sums are reproducible), the reference's cells (begin, nbody, nchild, child, centre,
-radius) and its M2L / P2P lists as visited by the reference recursion.
+radius) and its M2L / P2P lists as visited by the reference recursion.  The steps_* cases
+store the time-step pass of the top-level tree (get_steps = true): near-field pot / acc and
+each body's accumulated 1 / tau^4, with a sink / source subset.
+
+    python tests/golden/make_golden.py [--steps-only]
 """
 import os
 import sys
@@ -30,8 +34,39 @@ CASES = [
 ]
 
 
+STEPS_CASES = [
+    # name, generator, n, seed, p, theta, ncrit, dt_param, flags pattern
+    ("steps_top_kroupa2k_p8", "plummer_kroupa", 2000, 21, 8, 0.5, 32, 0.025, True),
+    ("steps_top_plummer40_p8", "plummer", 40, 22, 8, 0.5, 64, 0.01, False),
+]
+
+
+def steps_flags(n):
+    """every third body a sink only, every fifth (from 1) a source only, the rest both"""
+    fl = np.full(n, 3, np.uint8)
+    fl[::3] = 1
+    fl[1::5] = 2
+    return fl
+
+
+def make_steps(out_dir):
+    for name, gen, n, seed, p, theta, ncrit, dtp, use_flags in STEPS_CASES:
+        x, y, z, vx, vy, vz, m = getattr(ics, gen)(n, seed)
+        fl = steps_flags(n) if use_flags else np.full(n, 3, np.uint8)
+        r = oracle.ref_evaluate_steps(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, dt_param=dtp,
+                                      flags=fl)
+        np.savez_compressed(
+            os.path.join(out_dir, name + ".npz"), p=p, theta=theta, ncrit=ncrit, dt_param=dtp,
+            x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m, flags=fl,
+            ax=r["ax"], ay=r["ay"], az=r["az"], pot=r["pot"], timestep=r["timestep"])
+        print(name, "cells", r["ncell"])
+
+
 def main():
     out_dir = os.path.dirname(os.path.abspath(__file__))
+    make_steps(out_dir)
+    if "--steps-only" in sys.argv:
+        return
     for name, variant, gen, n, seed, p, theta, ncrit, sseed in CASES:
         x, y, z, vx, vy, vz, m = getattr(ics, gen)(n, seed)
         r = oracle.ref_evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, variant=variant,

@@ -3,6 +3,8 @@
 Tolerance: plain FP64 must reproduce the reference FMM within 1e-12 relative per particle
 (acceleration, potential, jerk; bodies whose value is below 1e-3 of the rms are measured
 against the rms).  Cells and interaction lists must be identical as sets."""
+import os
+
 import numpy as np
 import pytest
 
@@ -207,3 +209,38 @@ def test_direct_sums_match_oracle(device):
     assert rel_err(got["pot"], ref["pot"]).max() < 1e-12
     assert rel_vec_err(vec(got, "a"), vec(ref, "a")).max() < 1e-12
     assert rel_vec_err(vec(got, "j"), vec(ref, "j")).max() < 1e-11
+
+
+@pytest.mark.parametrize("name", ["steps_top_kroupa2k_p8", "steps_top_plummer40_p8"])
+@pytest.mark.parametrize("device", [False, True])
+def test_time_step_pass_matches_reference(name, device):
+    # get_force_and_potential(bodies, true) of the top-level tree: near-field pot / acc and
+    # each body's sum of 1 / tau^4, against the reference's own output (tests/golden)
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    g = tcb.Gravity(p=int(d["p"]), ncrit=int(d["ncrit"]), theta=float(d["theta"]), variant=tcb.VARIANT_TOP)
+    args = [d[k] for k in ("x", "y", "z", "m", "vx", "vy", "vz")]
+    fl = d["flags"]
+    if device:
+        import torch
+        args = [torch.tensor(a, device="cuda") for a in args]
+        fl = torch.tensor(fl, device="cuda")
+    out = g.evaluate_steps(*args, float(d["dt_param"]), flags=fl)
+    if device:
+        out = {k: v.cpu().numpy() for k, v in out.items()}
+    st = g.stats()
+    g.close()
+    assert st["n_m2l"] > 0 or st["n_cells"] == 1
+    ts = d["timestep"]
+    sink = (d["flags"] & 1) > 0
+    assert np.all(out["timestep"][~sink] == 0)
+    assert np.all(np.abs(out["timestep"][sink] - ts[sink]) <= 1e-12 * ts[sink])
+    for k in ("ax", "ay", "az", "pot"):
+        assert np.abs(out[k] - d[k]).max() <= 1e-12 * np.abs(d[k]).max()
+
+
+def test_time_step_pass_is_top_tree_only():
+    x, y, z, vx, vy, vz, m = ics.plummer(256, 3)
+    g = tcb.Gravity(p=8, ncrit=32, theta=0.5, variant=tcb.VARIANT_JERKS)
+    with pytest.raises(tcb.TaichiError):
+        g.evaluate_steps(x, y, z, m, vx, vy, vz, 0.025)
+    g.close()

@@ -3,6 +3,7 @@ the golden fixtures (tests/golden/make_golden.py, generated by the reference's h
 compiled behind oracle/ref_harness.cpp) and, when oracle/_ref is built, fresh runs of the
 reference on new inputs."""
 import math
+import os
 
 import numpy as np
 import pytest
@@ -179,3 +180,20 @@ def test_oracle_against_reference_build(variant, p, n, seed, ncrit, theta):
     if variant == oracle.VARIANT_JERKS:
         assert rel_vec_err(vec(o, "j"), vec(r, "j")).max() < TOL
     assert o["stats"]["n_cells"] == r["ncell"]
+
+
+@pytest.mark.parametrize("name", ["steps_top_kroupa2k_p8", "steps_top_plummer40_p8"])
+def test_oracle_time_step_pass_matches_reference(name):
+    # get_steps = true on the top-level tree: near-field pot / acc and the accumulated
+    # 1 / tau^4 of kernel_fast_lean.h:462-548, against the reference's own output
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", name + ".npz"))
+    o = oracle.evaluate_steps(d["x"], d["y"], d["z"], d["m"], d["vx"], d["vy"], d["vz"], p=int(d["p"]),
+                              theta=float(d["theta"]), ncrit=int(d["ncrit"]), dt_param=float(d["dt_param"]),
+                              flags=d["flags"])
+    sink = (d["flags"] & 1) > 0
+    ts = d["timestep"]
+    assert np.all(ts[sink] > 0) and np.all(ts[~sink] == 0)
+    assert np.abs(o["timestep"] - ts).max() <= 1e-13 * np.abs(ts).max()
+    assert np.all(np.abs(o["timestep"][sink] - ts[sink]) <= 1e-13 * ts[sink])
+    for k in ("ax", "ay", "az", "pot"):
+        assert np.abs(o[k] - d[k]).max() <= 1e-13 * np.abs(d[k]).max()

@@ -18,6 +18,7 @@ int main(int argc, char**) {
   exafmm::P = EXPANSION;
   exafmm::bodies.resize(3);
   if (argc > 5) exafmm::get_force_and_potential(exafmm::bodies, false);
+  if (argc > 6) exafmm::get_force_and_potential(exafmm::bodies, true);
   return 0;
 }
 """
@@ -29,7 +30,7 @@ def test_shim_compiles_and_links_against_reference_types(tmp_path, tree, defs):
     src = tmp_path / "shim_main.cpp"
     src.write_text(PROGRAM)
     inc = os.path.join(REF, tree) if tree else REF
-    cmd = ["g++", "-std=gnu++14", "-DEXPANSION=8", *defs, "-I", inc, "-I", ROOT, str(src), "-o",
+    cmd = ["g++", "-std=gnu++14", "-DEXPANSION=8", "-DHUGE=HUGE_VAL", *defs, "-I", inc, "-I", ROOT, str(src), "-o",
            str(tmp_path / "shim"), "-L", os.path.join(ROOT, "taichi_collisional_b200"), "-ltaichi_b200",
            "-Wl,-rpath," + os.path.join(ROOT, "taichi_collisional_b200")]
     r = subprocess.run(cmd, capture_output=True, text=True)

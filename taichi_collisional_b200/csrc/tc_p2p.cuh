@@ -390,10 +390,11 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
                                                               const int* __restrict__ tstart,
                                                               const int* __restrict__ src, const TcBodies b,
                                                               const TcCells c, TcOut out) {
-  // per warp source tile: xh yh zh xl yl zl mh ml vx vy vz
-  __shared__ float tile[kP2PWarps][11][32];
+  // per warp source tile, three 16-byte vectors per source (one broadcast load each):
+  // (xh, yh, zh, xl) (yl, zl, mh, ml) (vx, vy, vz, -)
+  __shared__ float4 tile[kP2PWarps][32][3];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float(*T)[32] = tile[w];
+  float4(*T)[3] = tile[w];
   for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
     int t = tlist[k];
     if (!c.has_sink[t]) continue;
@@ -428,19 +429,23 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
           __syncwarp();
           if (lane < cnt) {
             int j = jb + j0 + lane;
-            tc_split(b.x[j], Xc, T[0][lane], T[3][lane]);
-            tc_split(b.y[j], Yc, T[1][lane], T[4][lane]);
-            tc_split(b.z[j], Zc, T[2][lane], T[5][lane]);
-            tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, T[6][lane], T[7][lane]);
-            if (JERK) { T[8][lane] = (float)b.vx[j]; T[9][lane] = (float)b.vy[j]; T[10][lane] = (float)b.vz[j]; }
+            float4 s0, s1;
+            tc_split(b.x[j], Xc, s0.x, s0.w);
+            tc_split(b.y[j], Yc, s0.y, s1.x);
+            tc_split(b.z[j], Zc, s0.z, s1.y);
+            tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, s1.z, s1.w);
+            T[lane][0] = s0;
+            T[lane][1] = s1;
+            if (JERK) T[lane][2] = make_float4((float)b.vx[j], (float)b.vy[j], (float)b.vz[j], 0.f);
           }
           __syncwarp();
           float sp = 0, sx = 0, sy = 0, sz = 0, qx = 0, qy = 0, qz = 0;
           if (vi) {
             for (int jj = grp; jj < cnt; jj += ng) {
-              TcPair32 v = tc_pair32<JERK>(T[0][jj], T[1][jj], T[2][jj], T[3][jj], T[4][jj], T[5][jj], T[6][jj],
-                                           T[7][jj], JERK ? T[8][jj] : 0.f, JERK ? T[9][jj] : 0.f,
-                                           JERK ? T[10][jj] : 0.f, xh, yh, zh, xl, yl, zl, vxi, vyi, vzi);
+              const float4 s0 = T[jj][0], s1 = T[jj][1];
+              const float4 s2 = JERK ? T[jj][2] : make_float4(0.f, 0.f, 0.f, 0.f);
+              TcPair32 v = tc_pair32<JERK>(s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w, s2.x, s2.y, s2.z, xh, yh,
+                                           zh, xl, yl, zl, vxi, vyi, vzi);
               sp = __fadd_rn(sp, v.f0);
               sx = __fmaf_rn(v.dx, v.f, sx);
               sy = __fmaf_rn(v.dy, v.f, sy);

@@ -626,7 +626,15 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   // ---- upward, deepest level first
   int* d_start = &((TcLevels*)ctx->d_lv)->start[0];
   int* d_count = &((TcLevels*)ctx->d_lv)->count[0];
-  ctx->launches += maxl + 1;
+  ctx->launches += maxl + 3;
+  {
+    int g = nblocks(ctx->ncell, kUpWarps);
+    if (g > 148 * 16) g = 148 * 16;
+    k_leaf_balls<<<g, kUpWarps * 32, 0, st>>>(ctx->ncell, b, cv, ctx->d_err);
+    g = nblocks(ctx->ncell, kP2MWarps);
+    if (g > 148 * 16) g = 148 * 16;
+    k_p2m_leaves<P, JERK><<<g, kP2MWarps * 32, 0, st>>>(ctx->ncell, b, cv);
+  }
   for (int l = maxl; l >= 0; l--) {
     int cnt = ctx->lv.count[l];
     int g = nblocks(cnt, kUpWarps);

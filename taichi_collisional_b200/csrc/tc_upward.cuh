@@ -1,5 +1,6 @@
-// Upward pass on the device, one warp per cell, one launch per tree level (deepest first).
-// Restates upwardPass (traverse_eager.h:9-34) with MINIBALL: each cell's expansion centre
+// Upward pass on the device: the balls of every leaf (one launch), P2M of every leaf (one
+// launch), then one launch per tree level (deepest first) for the inner cells, one warp per
+// cell.  Restates upwardPass (traverse_eager.h:9-34) with MINIBALL: each cell's expansion centre
 // and radius are the smallest ball enclosing its bodies (leaf, kernel_fast_lean.h:707-737)
 // or, for an inner cell, the bodies of its leaf children plus 64 t-design points around
 // every grandchild (:833-892); R = r_ball + 1e-6.  Then P2M (:745-781) for leaves and M2M
@@ -208,66 +209,142 @@ __device__ void tc_warp_miniball(const TcPointSet& ps, const TcBodies& b, const 
 }
 
 // ---------------------------------------------------------------------------------------
-// P2M: lane m accumulates column m of sum_b q_b G(x_b - X) (and of Gdot(v_b) with jerks)
+// P2M of every leaf (kernel_fast_lean.h:745-781; with jerks the Mdot of
+// taichi_with_jerks/kernel_fast_lean.h:769-817): M[n][m] = sum_b q_b G[n][m](x_b - X) and
+// Mdot[n][m] = sum_b q_b Gdot[n][m](x_b - X, v_b).
+//
+// One warp per leaf, LW lanes per body (lane a = order m), 32 / LW bodies per pass.  The
+// column recurrence in n uses tabulated coefficients (no divisions):
+//   G[n][c] = (A[n][c] dz) G[n-1][c] - (B[n][c] r^2) G[n-2][c],
+//   A = (2n-1) / (n^2 - c^2), B = 1 / (n^2 - c^2) for n > c, A = B = 0 for n <= c,
+// so a column is zero below its diagonal, and G[c][c] is picked from the running diagonal
+// d_n = d_{n-1} (x + i y) / (2n), shared by every column of the body.  At n = c + 1 the
+// recurrence is exactly dz G[c][c] (A = 1, G[c-1][c] = 0).
 // ---------------------------------------------------------------------------------------
-template <int P, bool JERK>
-__device__ void tc_p2m_warp(int ci, const TcBodies& b, const TcCells& c) {
-  constexpr int NT = (P + 1) * (P + 1);
-  int lane = threadIdx.x & 31;
-  int beg = c.begin[ci], nb = c.nbody[ci];
-  double X = c.X[ci], Y = c.Y[ci], Z = c.Z[ci];
-  double* M = c.M + (size_t)ci * NT;
-  double* Md = JERK ? c.Md + (size_t)ci * NT : nullptr;
-  if (lane > P) return;
-  const int m = lane;
-  cd acc[P + 1], accd[P + 1];
-#pragma unroll
-  for (int n = 0; n <= P; n++) { acc[n] = mk(0, 0); accd[n] = mk(0, 0); }
-  for (int i = beg; i < beg + nb; i++) {
-    double q = (b.flags[i] & 2) ? b.m[i] : 0.0;
-    double dx = b.x[i] - X, dy = b.y[i] - Y, dz = b.z[i] - Z;
-    double r2 = dx * dx + dy * dy + dz * dz;
-    if (!JERK) {
-      cd d0 = mk(1, 0);
-      for (int j = 1; j <= m; j++) d0 = d0 * mk(dx / (2 * j), dy / (2 * j));
-      TcCol col;
-      col.init(m, d0);
-#pragma unroll
-      for (int n = 0; n <= P; n++) {
-        cd g = col.step(n, dz, r2);
-        acc[n] += q * g;
-      }
-    } else {
-      double vx = b.vx[i], vy = b.vy[i], vz = b.vz[i];
-      cd etad = mk(-vx * 0.5, vy * 0.5), zd = mk(vz, 0), ksid = mk(vx * 0.5, vy * 0.5);
-      TcCols3 cols;
-      cols.init(m, dx, dy);
-      cd pa = mk(0, 0), pb = mk(0, 0), pc = mk(0, 0);
-#pragma unroll
-      for (int n = 0; n <= P; n++) {
-        cd ga, gb, gc;
-        cols.step(n, dz, r2, ga, gb, gc);
-        acc[n] += q * gb;
-        if (n >= 1) {
-          cd gd = mk(0, 0);
-          if (m <= n - 2) gd += pc * etad;
-          if (m <= n - 1) gd += pb * zd;
-          if (n - 1 >= 1 || m >= 1) gd += pa * ksid;  // G[0][-1] reads as zero
-          accd[n] += q * gd;
-        }
-        pa = ga; pb = gb; pc = gc;
-      }
+template <int P>
+struct TcColTab {
+  double A[P + 1][P + 2], B[P + 1][P + 2];
+  __device__ void fill() {
+    for (int i = threadIdx.x; i < (P + 1) * (P + 2); i += blockDim.x) {
+      int n = i / (P + 2), c = i % (P + 2);
+      double m2 = (double)(n * n - c * c);
+      A[n][c] = n > c ? (2 * n - 1.) / m2 : 0.0;
+      B[n][c] = n > c ? 1.0 / m2 : 0.0;
     }
   }
+};
+
+// G[n][c] from G[n-1][c] (g1), G[n-2][c] (g2); on the diagonal it is d; shifts g1, g2
+__device__ __forceinline__ cd tc_col_next(bool on_diag, cd d, cd& g1, cd& g2, double ta, double tb, double dz,
+                                          double r2) {
+  double u = ta * dz, v = tb * r2;
+  cd g = mk(u * g1.x - v * g2.x, u * g1.y - v * g2.y);
+  if (on_diag) g = d;
+  g2 = g1;
+  g1 = g;
+  return g;
+}
+
+constexpr int kP2MWarps = 4;
+#ifndef TC_P2M_JERK_BLOCKS
+#define TC_P2M_JERK_BLOCKS 2  // resident blocks per SM asked of the compiler (2: no spills)
+#endif
+
+template <int P, bool JERK>
+__global__ void __launch_bounds__(kP2MWarps * 32, JERK ? TC_P2M_JERK_BLOCKS : 4) k_p2m_leaves(int ncell, const TcBodies b, TcCells c) {
+  constexpr int NT = (P + 1) * (P + 1);
+  constexpr int LW = (P + 1 <= 16) ? 16 : 32;  // lanes per body
+  constexpr int NH = 32 / LW;                  // bodies per pass
+  __shared__ TcColTab<P> tab;
+  __shared__ double sbod[kP2MWarps][32][9];    // dx dy dz q vx vy vz (row padded to 9)
+  tab.fill();
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int a = lane % LW, h = lane / LW;
+  // columns a-1, a, a+1 (column -1 is -conj(column 1), so a = 0 runs column 1 twice)
+  const int ca = a > 0 ? a - 1 : 1, cb = a <= P ? a : P, cc = a <= P ? a + 1 : P + 1;
+  double(*S)[9] = sbod[w];
+  for (int ci = blockIdx.x * kP2MWarps + w; ci < ncell; ci += gridDim.x * kP2MWarps) {
+    if (c.nchild[ci] != 0) continue;
+    const int beg = c.begin[ci], nb = c.nbody[ci];
+    const double X = c.X[ci], Y = c.Y[ci], Z = c.Z[ci];
+    cd acc[P + 1], accd[P + 1];
 #pragma unroll
-  for (int n = 0; n <= P; n++) {
-    if (n < m) continue;
-    int is = n * n + n;
-    M[is + m] = acc[n].x;
-    if (m > 0) M[is - m] = acc[n].y;
-    if (JERK) {
-      Md[is + m] = accd[n].x;
-      if (m > 0) Md[is - m] = accd[n].y;
+    for (int n = 0; n <= P; n++) { acc[n] = mk(0, 0); accd[n] = mk(0, 0); }
+    for (int j0 = 0; j0 < nb; j0 += 32) {
+      const int cnt = min(32, nb - j0);
+      __syncwarp();
+      if (lane < cnt) {
+        const int i = beg + j0 + lane;
+        S[lane][0] = b.x[i] - X;
+        S[lane][1] = b.y[i] - Y;
+        S[lane][2] = b.z[i] - Z;
+        S[lane][3] = (b.flags[i] & 2) ? b.m[i] : 0.0;
+        if (JERK) { S[lane][4] = b.vx[i]; S[lane][5] = b.vy[i]; S[lane][6] = b.vz[i]; }
+      }
+      __syncwarp();
+      for (int jj = h; a <= P && jj < cnt; jj += NH) {
+        const double dx = S[jj][0], dy = S[jj][1], dz = S[jj][2], q = S[jj][3];
+        const double r2 = dx * dx + dy * dy + dz * dz;
+        cd etad, zd, ksid;
+        if (JERK) {
+          const double vx = S[jj][4], vy = S[jj][5], vz = S[jj][6];
+          etad = mk(-vx * 0.5, vy * 0.5);
+          zd = mk(vz, 0);
+          ksid = mk(vx * 0.5, vy * 0.5);
+        }
+        // column indices laundered per body: keeps the coefficient loads inside the body loop
+        // (hoisted, the 6 (P + 1) table values would not fit in registers)
+        int ka = ca, kb = cb, kc = cc;
+        asm volatile("" : "+r"(ka), "+r"(kb), "+r"(kc));
+        cd d = mk(1, 0);
+        cd A1 = mk(0, 0), A2 = mk(0, 0), B1 = mk(0, 0), B2 = mk(0, 0), C1 = mk(0, 0), C2 = mk(0, 0);
+#pragma unroll
+        for (int n = 0; n <= P; n++) {
+          if (JERK && n >= 1) {
+            // Gdot[n][a] from G[n-1][a-1], G[n-1][a], G[n-1][a+1]
+            const cd pa = a > 0 ? A1 : mk(-C1.x, C1.y);
+            cd gd = mk(0, 0);
+            if (a <= n - 2) gd += C1 * etad;
+            if (a <= n - 1) gd += B1 * zd;
+            if (n - 1 >= 1 || a >= 1) gd += pa * ksid;
+            accd[n] += q * gd;
+          }
+          if (n >= 1) d = d * mk(dx * (0.5 / n), dy * (0.5 / n));
+          if (JERK) {
+            tc_col_next(n == kc, d, C1, C2, tab.A[n][kc], tab.B[n][kc], dz, r2);
+            tc_col_next(n == ka, d, A1, A2, tab.A[n][ka], tab.B[n][ka], dz, r2);
+          }
+          const cd gb = tc_col_next(n == kb, d, B1, B2, tab.A[n][kb], tab.B[n][kb], dz, r2);
+          acc[n] += q * gb;
+        }
+      }
+    }
+    if (NH == 2) {
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        acc[n].x += __shfl_down_sync(0xffffffffu, acc[n].x, 16);
+        acc[n].y += __shfl_down_sync(0xffffffffu, acc[n].y, 16);
+        if (JERK) {
+          accd[n].x += __shfl_down_sync(0xffffffffu, accd[n].x, 16);
+          accd[n].y += __shfl_down_sync(0xffffffffu, accd[n].y, 16);
+        }
+      }
+    }
+    if (h == 0 && a <= P) {
+      double* M = c.M + (size_t)ci * NT;
+      double* Md = JERK ? c.Md + (size_t)ci * NT : nullptr;
+#pragma unroll
+      for (int n = 0; n <= P; n++) {
+        if (n < a) continue;
+        const int is = n * n + n;
+        M[is + a] = acc[n].x;
+        if (a > 0) M[is - a] = acc[n].y;
+        if (JERK) {
+          Md[is + a] = accd[n].x;
+          if (a > 0) Md[is - a] = accd[n].y;
+        }
+      }
     }
   }
 }
@@ -350,16 +427,11 @@ __device__ void tc_m2m_warp(int ci, const TcCells& c, cd* G) {
 
 constexpr int kUpWarps = 4;
 
-template <int P, bool JERK>
-__global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcBodies b, TcCells c,
-                                                                const int* __restrict__ lv_start,
-                                                                const int* __restrict__ lv_count, unsigned int* err) {
-  __shared__ cd sG[kUpWarps][(P + 1) * (P + 1)];
-  __shared__ double s_td[193];
+// t-design table in shared memory; s_td[192] = the largest |t_k| (rows 36-47 of the
+// reference's table are not unit vectors, |t| = 1.1968, so the pruning bound uses the norm)
+__device__ __forceinline__ void tc_load_tdesign(double* s_td) {
   for (int i = threadIdx.x; i < 192; i += blockDim.x) s_td[i] = c_tdesign[i];
   if (threadIdx.x == 0) {
-    // rows 36-47 of the reference's table are not unit vectors (|t| = 1.1968), so the
-    // pruning bound uses the largest norm
     double mx = 0;
     for (int k = 0; k < 64; k++)
       mx = fmax(mx, sqrt(c_tdesign[3 * k] * c_tdesign[3 * k] + c_tdesign[3 * k + 1] * c_tdesign[3 * k + 1] +
@@ -367,52 +439,76 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcB
     s_td[192] = mx * (1.0 + 1e-12);
   }
   __syncthreads();
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+}
+
+// one warp: expansion centre, radius and has_sink of cell ci
+__device__ void tc_cell_ball(int ci, const TcBodies& b, TcCells& c, const double* s_td, unsigned int* err) {
+  int lane = threadIdx.x & 31;
+  TcPointSet ps;
+  int nch = c.nchild[ci];
+  bool sink = false;
+  if (nch == 0) {
+    ps.leaf = 1;
+    ps.seg_a[0] = c.begin[ci];
+    ps.total = c.nbody[ci];
+    for (int i = c.begin[ci] + lane; i < c.begin[ci] + c.nbody[ci]; i += 32) sink |= (b.flags[i] & 1) != 0;
+  } else {
+    ps.leaf = 0;
+    ps.nseg = nch;
+    int tot = 0;
+    for (int s = 0; s < nch; s++) {
+      int ch = c.child[ci] + s;
+      ps.seg_start[s] = tot;
+      sink |= c.has_sink[ch] != 0;
+      if (c.nchild[ch] == 0) {
+        ps.seg_kind[s] = 0;
+        ps.seg_a[s] = c.begin[ch];
+        tot += c.nbody[ch];
+      } else {
+        ps.seg_kind[s] = 1;
+        ps.seg_a[s] = c.child[ch];
+        tot += 64 * c.nchild[ch];
+      }
+    }
+    ps.seg_start[nch] = tot;
+    ps.total = tot;
+  }
+  sink = __any_sync(0xffffffffu, sink);
+  double cc[3], r2;
+  tc_warp_miniball(ps, b, c, s_td, cc, &r2, err);
+  if (lane == 0) {
+    c.X[ci] = cc[0]; c.Y[ci] = cc[1]; c.Z[ci] = cc[2];
+    c.R[ci] = sqrt(r2) + 1e-6;
+    c.has_sink[ci] = sink;
+  }
+  __syncwarp();
+}
+
+// balls of every leaf (they depend on the leaf's own bodies only)
+__global__ void __launch_bounds__(kUpWarps * 32) k_leaf_balls(int ncell, const TcBodies b, TcCells c,
+                                                              unsigned int* err) {
+  __shared__ double s_td[193];
+  tc_load_tdesign(s_td);
+  int w = threadIdx.x >> 5;
+  for (int ci = blockIdx.x * kUpWarps + w; ci < ncell; ci += gridDim.x * kUpWarps)
+    if (c.nchild[ci] == 0) tc_cell_ball(ci, b, c, s_td, err);
+}
+
+// inner cells of level l: ball over the children's points, then M2M from the children
+template <int P, bool JERK>
+__global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcBodies b, TcCells c,
+                                                                const int* __restrict__ lv_start,
+                                                                const int* __restrict__ lv_count, unsigned int* err) {
+  __shared__ cd sG[kUpWarps][(P + 1) * (P + 1)];
+  __shared__ double s_td[193];
+  tc_load_tdesign(s_td);
+  int w = threadIdx.x >> 5;
   int cnt = lv_count[l], st = lv_start[l];
   for (int k = blockIdx.x * kUpWarps + w; k < cnt; k += gridDim.x * kUpWarps) {
     int ci = st + k;
-    TcPointSet ps;
-    int nch = c.nchild[ci];
-    bool sink = false;
-    if (nch == 0) {
-      ps.leaf = 1;
-      ps.seg_a[0] = c.begin[ci];
-      ps.total = c.nbody[ci];
-      for (int i = c.begin[ci] + lane; i < c.begin[ci] + c.nbody[ci]; i += 32) sink |= (b.flags[i] & 1) != 0;
-    } else {
-      ps.leaf = 0;
-      ps.nseg = nch;
-      int tot = 0;
-      for (int s = 0; s < nch; s++) {
-        int ch = c.child[ci] + s;
-        ps.seg_start[s] = tot;
-        sink |= c.has_sink[ch] != 0;
-        if (c.nchild[ch] == 0) {
-          ps.seg_kind[s] = 0;
-          ps.seg_a[s] = c.begin[ch];
-          tot += c.nbody[ch];
-        } else {
-          ps.seg_kind[s] = 1;
-          ps.seg_a[s] = c.child[ch];
-          tot += 64 * c.nchild[ch];
-        }
-      }
-      ps.seg_start[nch] = tot;
-      ps.total = tot;
-    }
-    sink = __any_sync(0xffffffffu, sink);
-    double cc[3], r2;
-    tc_warp_miniball(ps, b, c, s_td, cc, &r2, err);
-    if (lane == 0) {
-      c.X[ci] = cc[0]; c.Y[ci] = cc[1]; c.Z[ci] = cc[2];
-      c.R[ci] = sqrt(r2) + 1e-6;
-      c.has_sink[ci] = sink;
-    }
-    __syncwarp();
-    if (nch == 0)
-      tc_p2m_warp<P, JERK>(ci, b, c);
-    else
-      tc_m2m_warp<P, JERK>(ci, c, sG[w]);
+    if (c.nchild[ci] == 0) continue;
+    tc_cell_ball(ci, b, c, s_td, err);
+    tc_m2m_warp<P, JERK>(ci, c, sG[w]);
     __syncwarp();
   }
 }

@@ -91,13 +91,17 @@ __device__ __forceinline__ void tc_l2p_acc(const cd* sl, double dx, double dy, d
   a[2] = -p10.x;
 }
 
-// L2P for every leaf; one warp per leaf, one lane per body
+// L2P for every leaf; one warp per leaf, one lane per body.  The solid-harmonic columns use the
+// tabulated recurrence of the P2M (TcColTab, tc_col_next).
 template <int P, bool JERK>
 __global__ void __launch_bounds__(kUpWarps * 32) k_l2p(const int* __restrict__ leaves, int nleaf, const TcBodies b,
                                                        const TcCells c, TcOut out) {
   constexpr int NT = (P + 1) * (P + 1);
   __shared__ cd sL[kUpWarps][NT];
   __shared__ cd sLd[kUpWarps][JERK ? NT : 1];
+  __shared__ TcColTab<P> tab;
+  tab.fill();
+  __syncthreads();
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int k = blockIdx.x * kUpWarps + w; k < nleaf; k += gridDim.x * kUpWarps) {
     int ci = leaves[k];
@@ -129,19 +133,23 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_l2p(const int* __restrict__ l
         zd = mk(vz, 0);
         ksid = mk(vx * 0.5, vy * 0.5);
       }
+      // diagonal G[j][j] at j = m - 1, m, m + 1, advanced with the order m
+      cd Dm1 = mk(0, 0), D0 = mk(1, 0), Dp1 = mk(dx * tab.H[1], dy * tab.H[1]);
       for (int m = 0; m <= P; m++) {
-        double sgn = (m & 1) ? -1.0 : 1.0;
-        TcCols3 cols;
-        cols.init(m, dx, dy);
-        cd pa = mk(0, 0), pb = mk(0, 0), pc = mk(0, 0);
+        const double sgn = (m & 1) ? -1.0 : 1.0;
+        const int ca = m > 0 ? m - 1 : 1, cc = m + 1;  // column -1 is -conj(column 1)
+        cd A1 = mk(0, 0), A2 = mk(0, 0), B1 = mk(0, 0), B2 = mk(0, 0), C1 = mk(0, 0), C2 = mk(0, 0);
 #pragma unroll
         for (int n = 0; n <= P; n++) {
-          cd ga, gb, gc;
+          cd pa, pb, pc;  // G[n-1][m-1], G[n-1][m], G[n-1][m+1]
           if (JERK) {
-            cols.step(n, dz, r2, ga, gb, gc);
-          } else {
-            gb = cols.B.step(n, dz, r2);
+            pa = m > 0 ? A1 : mk(-C1.x, C1.y);
+            pb = B1;
+            pc = C1;
+            tc_col_next(n == cc, Dp1, C1, C2, tab.A[n][cc], tab.B[n][cc], dz, r2);
+            if (m > 0) tc_col_next(n == ca, Dm1, A1, A2, tab.A[n][ca], tab.B[n][ca], dz, r2);
           }
+          const cd gb = tc_col_next(n == m, D0, B1, B2, tab.A[n][m], tab.B[n][m], dz, r2);
           if (n >= m) {
             // l = +m and l = -m terms of sum_k,l L[n'+k, m'+l] conj(G[k,l]) at k = n
             cd cgp = conj(gb), cgn = sgn * gb;
@@ -174,8 +182,10 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_l2p(const int* __restrict__ l
               }
             }
           }
-          if (JERK) { pa = ga; pb = gb; pc = gc; }
         }
+        Dm1 = D0;
+        D0 = Dp1;
+        Dp1 = Dp1 * mk(dx * tab.H[m + 2], dy * tab.H[m + 2]);
       }
       out.pot[i] += p00.x;
       out.ax[i] -= p11.x;

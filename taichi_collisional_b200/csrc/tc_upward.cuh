@@ -224,6 +224,7 @@ __device__ void tc_warp_miniball(const TcPointSet& ps, const TcBodies& b, const 
 template <int P>
 struct TcColTab {
   double A[P + 1][P + 2], B[P + 1][P + 2];
+  double H[P + 3];  // 1 / (2j): the diagonal step G[j][j] = G[j-1][j-1] (x + i y) / (2j)
   __device__ void fill() {
     for (int i = threadIdx.x; i < (P + 1) * (P + 2); i += blockDim.x) {
       int n = i / (P + 2), c = i % (P + 2);
@@ -231,6 +232,7 @@ struct TcColTab {
       A[n][c] = n > c ? (2 * n - 1.) / m2 : 0.0;
       B[n][c] = n > c ? 1.0 / m2 : 0.0;
     }
+    for (int j = threadIdx.x; j < P + 3; j += blockDim.x) H[j] = j > 0 ? 0.5 / j : 0.0;
   }
 };
 

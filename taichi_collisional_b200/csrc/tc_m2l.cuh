@@ -103,12 +103,140 @@ __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1
 // Pair batches processed at once by one CTA (each batch by 4 warps); limited by shared memory.
 template <int P>
 struct TcM2LGroups {
-  static constexpr int G = (P >= 14) ? 1 : 2;
+  static constexpr int G = (P >= 14) ? 2 : (P >= 12) ? 3 : 4;
 };
+
+// ---------------------------------------------------------------------------------------
+// Per-lane accumulators in tensor memory.  Warp w of group g accumulates the locals of the
+// degrees it owns for its lane's pairs in TMEM lane 32 (w % 4) + lane (the lane quarter the
+// warp may access), columns g * CW + offset of the degree; a double takes two 32-bit columns.
+// The allocation base is column-aligned, CW and every degree offset are multiples of 16.
+// Shared memory then only holds the translation exchange buffer, which lets more groups
+// (warps) share an SM.
+// ---------------------------------------------------------------------------------------
+template <int Q>
+struct TcM2LTmem {
+  using S = TcDegSets<Q>;
+  // each degree's block starts on a multiple of 16 columns, so the 16/8/4/2-column chunks of
+  // tc_tm_ld / tc_tm_st each start on a multiple of their own width
+  static constexpr int cols_before(int w, int i) {
+    int c = 0;
+    for (int k = 0; k < i; k++)
+      if (S::d[w][k] >= 0) c += (2 * (2 * S::d[w][k] + 1) + 15) / 16 * 16;
+    return c;
+  }
+  static constexpr int cols_of(int w) { return cols_before(w, S::L); }
+  static constexpr int cw_raw() {
+    int m = 0;
+    for (int w = 0; w < 4; w++) m = cols_of(w) > m ? cols_of(w) : m;
+    return m;
+  }
+  static constexpr int CW = (cw_raw() + 15) / 16 * 16;  // columns per warp, multiple of 16
+  static constexpr int TOTAL = CW * TcM2LGroups<Q>::G;
+  static constexpr int ALLOC = TOTAL <= 32 ? 32 : TOTAL <= 64 ? 64 : TOTAL <= 128 ? 128 : TOTAL <= 256 ? 256 : 512;
+  static_assert(TOTAL <= 512, "M2L accumulators exceed tensor memory");
+};
+
+#define TC_TM_R2(i) "=r"(r[(i)]), "=r"(r[(i) + 1])
+#define TC_TM_W2(i) "r"(r[(i)]), "r"(r[(i) + 1])
+template <int N>
+__device__ __forceinline__ void tc_tm_ld_chunk(uint32_t ta, uint32_t* r);
+template <int N>
+__device__ __forceinline__ void tc_tm_st_chunk(uint32_t ta, const uint32_t* r);
+template <>
+__device__ __forceinline__ void tc_tm_ld_chunk<2>(uint32_t ta, uint32_t* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x2.b32 {%0,%1}, [%2];" : TC_TM_R2(0) : "r"(ta));
+}
+template <>
+__device__ __forceinline__ void tc_tm_ld_chunk<4>(uint32_t ta, uint32_t* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];" : TC_TM_R2(0), TC_TM_R2(2) : "r"(ta));
+}
+template <>
+__device__ __forceinline__ void tc_tm_ld_chunk<8>(uint32_t ta, uint32_t* r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+               : TC_TM_R2(0), TC_TM_R2(2), TC_TM_R2(4), TC_TM_R2(6)
+               : "r"(ta));
+}
+template <>
+__device__ __forceinline__ void tc_tm_ld_chunk<16>(uint32_t ta, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : TC_TM_R2(0), TC_TM_R2(2), TC_TM_R2(4), TC_TM_R2(6), TC_TM_R2(8), TC_TM_R2(10), TC_TM_R2(12), TC_TM_R2(14)
+      : "r"(ta));
+}
+template <>
+__device__ __forceinline__ void tc_tm_st_chunk<2>(uint32_t ta, const uint32_t* r) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x2.b32 [%0], {%1,%2};" ::"r"(ta), TC_TM_W2(0) : "memory");
+}
+template <>
+__device__ __forceinline__ void tc_tm_st_chunk<4>(uint32_t ta, const uint32_t* r) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(ta), TC_TM_W2(0), TC_TM_W2(2)
+               : "memory");
+}
+template <>
+__device__ __forceinline__ void tc_tm_st_chunk<8>(uint32_t ta, const uint32_t* r) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(ta), TC_TM_W2(0),
+               TC_TM_W2(2), TC_TM_W2(4), TC_TM_W2(6)
+               : "memory");
+}
+template <>
+__device__ __forceinline__ void tc_tm_st_chunk<16>(uint32_t ta, const uint32_t* r) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+          ta),
+      TC_TM_W2(0), TC_TM_W2(2), TC_TM_W2(4), TC_TM_W2(6), TC_TM_W2(8), TC_TM_W2(10), TC_TM_W2(12), TC_TM_W2(14)
+      : "memory");
+}
+#undef TC_TM_R2
+#undef TC_TM_W2
+
+// C (even) consecutive columns, as chunks of 16, 8, 4, 2; loads complete at tc_tm_wait_ld
+template <int C, int OFF = 0>
+__device__ __forceinline__ void tc_tm_ld(uint32_t ta, uint32_t* r) {
+  if constexpr (C >= 16) {
+    tc_tm_ld_chunk<16>(ta + OFF, r + OFF);
+    tc_tm_ld<C - 16, OFF + 16>(ta, r);
+  } else if constexpr (C >= 8) {
+    tc_tm_ld_chunk<8>(ta + OFF, r + OFF);
+    tc_tm_ld<C - 8, OFF + 8>(ta, r);
+  } else if constexpr (C >= 4) {
+    tc_tm_ld_chunk<4>(ta + OFF, r + OFF);
+    tc_tm_ld<C - 4, OFF + 4>(ta, r);
+  } else if constexpr (C >= 2) {
+    tc_tm_ld_chunk<2>(ta + OFF, r + OFF);
+  }
+}
+template <int C, int OFF = 0>
+__device__ __forceinline__ void tc_tm_st(uint32_t ta, const uint32_t* r) {
+  if constexpr (C >= 16) {
+    tc_tm_st_chunk<16>(ta + OFF, r + OFF);
+    tc_tm_st<C - 16, OFF + 16>(ta, r);
+  } else if constexpr (C >= 8) {
+    tc_tm_st_chunk<8>(ta + OFF, r + OFF);
+    tc_tm_st<C - 8, OFF + 8>(ta, r);
+  } else if constexpr (C >= 4) {
+    tc_tm_st_chunk<4>(ta + OFF, r + OFF);
+    tc_tm_st<C - 4, OFF + 4>(ta, r);
+  } else if constexpr (C >= 2) {
+    tc_tm_st_chunk<2>(ta + OFF, r + OFF);
+  }
+}
+__device__ __forceinline__ void tc_tm_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_tm_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// the 2 K columns of K doubles -> registers (after tc_tm_ld and tc_tm_wait_ld)
+template <int K>
+__device__ __forceinline__ void tc_tm_to_f64(uint32_t* r, double* v) {
+#pragma unroll
+  for (int k = 0; k < K; k++) {
+    asm volatile("" : "+r"(r[2 * k]), "+r"(r[2 * k + 1]));  // every use stays after the wait
+    v[k] = __hiloint2double((int)r[2 * k + 1], (int)r[2 * k]);
+  }
+}
 
 template <int P, int N>
 __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int lane, cd ez1, cd ex1,
-                                            double* acc, int acol, bool valid) {
+                                            uint32_t tacc, bool valid) {
   double l[2 * N + 1], o[2 * N + 1];
 #pragma unroll
   for (int k = 0; k < 2 * N + 1; k++) l[k] = 0.0;
@@ -151,19 +279,29 @@ __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int 
 #pragma unroll
     for (int k = 0; k < 2 * N + 1; k++) l[k] = o[k];
   }
-  if (valid) {
+  // read-modify-write of this lane's accumulator columns (every lane takes part)
+  uint32_t r[2 * (2 * N + 1)];
+  double a[2 * N + 1];
+  tc_tm_ld<2 * (2 * N + 1)>(tacc, r);
+  tc_tm_wait_ld();
+  tc_tm_to_f64<2 * N + 1>(r, a);
 #pragma unroll
-    for (int k = 0; k < 2 * N + 1; k++) acc[(N * N + k) * (32 * TcM2LGroups<P>::G) + acol] += l[k];
+  for (int k = 0; k < 2 * N + 1; k++) {
+    const double v = a[k] + (valid ? l[k] : 0.0);
+    r[2 * k] = (uint32_t)__double2loint(v);
+    r[2 * k + 1] = (uint32_t)__double2hiint(v);
   }
+  tc_tm_st<2 * (2 * N + 1)>(tacc, r);
 }
 
-// shared-memory layout of one M2L CTA (doubles): buf[G groups] | acc (32 G columns)
+// shared-memory layout of one M2L CTA (doubles): buf[G groups]; after the last batch the same
+// space holds the accumulators of all 32 G lanes for the ordered final sum
 template <int P>
 struct TcM2LSmem {
   static constexpr int NT = (P + 1) * (P + 1);
   static constexpr int G = TcM2LGroups<P>::G;
-  static constexpr int BUF = 0, ACC = G * NT * 32;
-  static constexpr int TOTAL = G * NT * 32 + NT * 32 * G;
+  static constexpr int BUF = 0;
+  static constexpr int TOTAL = G * NT * 32;
 };
 
 // Warp w of each 4-warp group owns the degrees TcDegSets<P>::d[w][*] (balanced by a
@@ -178,11 +316,35 @@ struct TcDegSeq {
       TcDegSeq<Q, QUIRK, W, I + 1>::fwd(Ms, ez1, ex1, buf, lane);
     }
   }
-  static __device__ __forceinline__ void back(const double* buf, double rinv, int lane, cd ez1, cd ex1, double* acc,
-                                              int acol, bool valid) {
+  static constexpr int COL = TcM2LTmem<Q>::cols_before(W, I);
+  static __device__ __forceinline__ void back(const double* buf, double rinv, int lane, cd ez1, cd ex1,
+                                              uint32_t twarp, bool valid) {
     if constexpr (D >= 0) {
-      tc_m2l_back<Q, D>(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-      TcDegSeq<Q, QUIRK, W, I + 1>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+      tc_m2l_back<Q, D>(buf, rinv, lane, ez1, ex1, twarp + COL, valid);
+      TcDegSeq<Q, QUIRK, W, I + 1>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
+    }
+  }
+  // zero this warp's accumulator columns
+  static __device__ __forceinline__ void zero(uint32_t twarp) {
+    if constexpr (D >= 0) {
+      uint32_t z[2 * (2 * D + 1)];
+#pragma unroll
+      for (int k = 0; k < 2 * (2 * D + 1); k++) z[k] = 0u;
+      tc_tm_st<2 * (2 * D + 1)>(twarp + COL, z);
+      TcDegSeq<Q, QUIRK, W, I + 1>::zero(twarp);
+    }
+  }
+  // accumulators -> shared memory, row (coefficient) major with 32 G columns
+  static __device__ __forceinline__ void readout(uint32_t twarp, double* sc, int acol) {
+    if constexpr (D >= 0) {
+      uint32_t r[2 * (2 * D + 1)];
+      double a[2 * D + 1];
+      tc_tm_ld<2 * (2 * D + 1)>(twarp + COL, r);
+      tc_tm_wait_ld();
+      tc_tm_to_f64<2 * D + 1>(r, a);
+#pragma unroll
+      for (int k = 0; k < 2 * D + 1; k++) sc[(D * D + k) * (32 * TcM2LGroups<Q>::G) + acol] = a[k];
+      TcDegSeq<Q, QUIRK, W, I + 1>::readout(twarp, sc, acol);
     }
   }
 };
@@ -196,11 +358,27 @@ __device__ __forceinline__ void tc_m2l_fwd_warp(int w, const double* Ms, cd ez1,
 }
 template <int Q, bool QUIRK>
 __device__ __forceinline__ void tc_m2l_back_warp(int w, const double* buf, double rinv, int lane, cd ez1, cd ex1,
-                                                 double* acc, int acol, bool valid) {
-  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
-  else TcDegSeq<Q, QUIRK, 3, 0>::back(buf, rinv, lane, ez1, ex1, acc, acol, valid);
+                                                 uint32_t twarp, bool valid) {
+  tc_tm_wait_st();  // the previous batch's accumulator stores
+  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
+  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
+  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
+  else TcDegSeq<Q, QUIRK, 3, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
+}
+template <int Q, bool QUIRK>
+__device__ __forceinline__ void tc_m2l_zero_warp(int w, uint32_t twarp) {
+  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::zero(twarp);
+  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::zero(twarp);
+  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::zero(twarp);
+  else TcDegSeq<Q, QUIRK, 3, 0>::zero(twarp);
+}
+template <int Q, bool QUIRK>
+__device__ __forceinline__ void tc_m2l_readout_warp(int w, uint32_t twarp, double* sc, int acol) {
+  tc_tm_wait_st();
+  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::readout(twarp, sc, acol);
+  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::readout(twarp, sc, acol);
+  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::readout(twarp, sc, acol);
+  else TcDegSeq<Q, QUIRK, 3, 0>::readout(twarp, sc, acol);
 }
 
 __device__ __forceinline__ void tc_bar_group(int grp) {
@@ -211,30 +389,43 @@ template <int Q>
 constexpr int tc_m2l_threads() { return 128 * TcM2LGroups<Q>::G; }
 
 // M2L of order Q <= P over a per-target list; expansions are stored with order P.  Adds
-// into L (zeroed before the first M2L launch of an evaluation).
+// into L (zeroed before the first M2L launch of an evaluation).  One CTA per SM (shared
+// memory), which owns the tensor memory it allocates.
 template <int P, int Q, bool JERK>
 __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __restrict__ tlist, int ntl,
                                                                const int* __restrict__ tstart,
                                                                const int* __restrict__ src, TcCells c) {
   using SM = TcM2LSmem<Q>;
+  using TM = TcM2LTmem<Q>;
   constexpr int NTQ = SM::NT, NTP = (P + 1) * (P + 1);
   constexpr int G = SM::G;
   constexpr bool QUIRK = Q == P;
   extern __shared__ double tc_m2l_smem[];
-  double* acc = tc_m2l_smem + SM::ACC;
+  __shared__ uint32_t s_tmem;
   int ti = blockIdx.x;
   if (ti >= ntl) return;
   int t = tlist[ti];
   if (!c.has_sink[t]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = warp >> 2, w = warp & 3, acol = grp * 32 + lane;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(&s_tmem)),
+                 "r"(TM::ALLOC)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  tc_bar_cta();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // this warp's columns in its lane quarter
+  const uint32_t twarp = s_tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(grp * TM::CW);
   double* buf = tc_m2l_smem + SM::BUF + grp * NTQ * 32;
   const int s_beg = tstart[t], s_end = tstart[t + 1];
   const double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
   for (int arr = 0; arr < (JERK ? 2 : 1); arr++) {
     const double* Mbase = arr ? c.Md : c.M;
-    for (int i = threadIdx.x; i < NTQ * 32 * G; i += blockDim.x) acc[i] = 0.0;
-    tc_bar_cta();
+    tc_m2l_zero_warp<Q, QUIRK>(w, twarp);
     for (int b0 = s_beg + grp * 32; b0 < s_end; b0 += 32 * G) {
       int idx = b0 + lane;
       bool valid = idx < s_end;
@@ -242,19 +433,26 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
       TcPairGeo pg = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
       tc_m2l_fwd_warp<Q, QUIRK>(w, Mbase + (size_t)s * NTP, pg.ez1, pg.ex1, buf, lane);
       tc_bar_group(grp);
-      tc_m2l_back_warp<Q, QUIRK>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, acc, acol, valid);
+      tc_m2l_back_warp<Q, QUIRK>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, twarp, valid);
       tc_bar_group(grp);
     }
+    tc_bar_cta();  // every group is done with its buffer
+    double* sc = tc_m2l_smem;  // NT x 32 G accumulators
+    tc_m2l_readout_warp<Q, QUIRK>(w, twarp, sc, acol);
     tc_bar_cta();
     double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NTP;
     for (int r = threadIdx.x; r < NTQ; r += blockDim.x) {
       double v = 0.0;
 #pragma unroll 8
-      for (int q = 0; q < 32 * G; q++) v += acc[r * (32 * G) + q];
+      for (int q = 0; q < 32 * G; q++) v += sc[r * (32 * G) + q];
       Lt[r] += v;
     }
     tc_bar_cta();
   }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  tc_bar_cta();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(TM::ALLOC) : "memory");
 }
 
 }  // namespace tc

@@ -17,20 +17,37 @@ template <int P, int Q>
 __global__ void __launch_bounds__(128) k_m2l_pairs(int K, const int* __restrict__ pt, const int* __restrict__ ps,
                                                    TcCells c, double* __restrict__ out) {
   constexpr int NTQ = (Q + 1) * (Q + 1), NTP = (P + 1) * (P + 1), G = TcM2LGroups<Q>::G;
+  constexpr int CW = TcM2LTmem<Q>::CW;
+  constexpr int ALLOC = CW <= 32 ? 32 : CW <= 64 ? 64 : CW <= 128 ? 128 : 256;  // one group
   extern __shared__ double tc_m2lp_smem[];
+  __shared__ uint32_t s_tmem;
   double* buf = tc_m2lp_smem;
-  double* acc = tc_m2lp_smem + NTQ * 32;
+  double* acc = tc_m2lp_smem + NTQ * 32;  // NTQ x 32 G (columns 0..31 used)
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int k = blockIdx.x * 32 + lane;
   const bool valid = k < K;
   const int t = pt[valid ? k : 0], s = ps[valid ? k : 0];
-  for (int i = threadIdx.x; i < NTQ * 32 * G; i += blockDim.x) acc[i] = 0.0;
+  if (w == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     (uint32_t)__cvta_generic_to_shared(&s_tmem)),
+                 "r"(ALLOC)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t twarp = s_tmem + ((uint32_t)(32 * w) << 16);
+  tc_m2l_zero_warp<Q, false>(w, twarp);
   TcPairGeo pg = tc_pair_geo(c.X[t] - c.X[s], c.Y[t] - c.Y[s], c.Z[t] - c.Z[s]);
   tc_m2l_fwd_warp<Q, false>(w, c.M + (size_t)s * NTP, pg.ez1, pg.ex1, buf, lane);
   __syncthreads();
-  tc_m2l_back_warp<Q, false>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, acc, lane, valid);
+  tc_m2l_back_warp<Q, false>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, twarp, valid);
+  tc_m2l_readout_warp<Q, false>(w, twarp, acc, lane);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
+  if (w == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(ALLOC) : "memory");
   for (int i = 0; i < 32; i++) {
     int kk = blockIdx.x * 32 + i;
     if (kk >= K) break;

@@ -8,17 +8,17 @@
 // The reference's factorial table stops at (2P-1)! (kernel_fast_lean.h:127), so the scaled
 // (P, +-P) entries are zero; that is reproduced here.
 //
-// Layout: one CTA per target cell, 1 or 2 groups of 4 warps; each group takes 32 (target,
-// source) pairs at a time, one pair per lane.  Warp w of a group owns a fixed set of degrees
-// (m2l_schedule.h, balanced by a per-degree cost model) and runs every per-degree step --
-// including the constant swap matrices, emitted as straight-line code with immediate
+// Layout: one CTA per target cell, 4 groups of 4 warps (2 at p >= 14); each group takes 32
+// (target, source) pairs at a time, one pair per lane.  Warp w of a group owns a fixed set of
+// degrees (m2l_schedule.h, balanced by a per-degree cost model) and runs every per-degree
+// step -- including the constant swap matrices, emitted as straight-line code with immediate
 // coefficients -- in registers.  The only exchange is the z-translation, which mixes
 // degrees and goes through shared memory (NT x 32 doubles per group).  Each lane
-// accumulates its pairs' locals in its own column of a shared accumulator; one fixed-order
-// sum over the columns per
-// coefficient gives deterministic results.  Instruction footprint limits this kernel (the
-// code of all degrees exceeds the instruction caches), so each pass applies its two swaps
-// through a rolled two-step loop over one copy of the degree's swap code.
+// accumulates its pairs' locals in its own tensor-memory columns (TcM2LTmem), so shared
+// memory holds only the exchange buffers and 16 warps fit on an SM; one fixed-order sum over
+// the lanes per coefficient gives deterministic results.  Instruction footprint limits this
+// kernel (the code of all degrees exceeds the instruction caches), so each pass applies its
+// two swaps through a rolled two-step loop over one copy of the degree's swap code.
 #pragma once
 #include "swap_tables.h"
 #include "tc_harmonics.cuh"
@@ -103,7 +103,7 @@ __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1
 // Pair batches processed at once by one CTA (each batch by 4 warps); limited by shared memory.
 template <int P>
 struct TcM2LGroups {
-  static constexpr int G = (P >= 14) ? 2 : (P >= 12) ? 3 : 4;
+  static constexpr int G = (P >= 14) ? 2 : 4;
 };
 
 // ---------------------------------------------------------------------------------------

@@ -440,12 +440,16 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
     double* sc = tc_m2l_smem;  // NT x 32 G accumulators
     tc_m2l_readout_warp<Q, QUIRK>(w, twarp, sc, acol);
     tc_bar_cta();
+    // ordered sum over the 32 G lanes of each coefficient: warp per coefficient, lane j adds
+    // columns j, j + 32, ... in order, then a fixed butterfly over the lanes
     double* Lt = (arr ? c.Ld : c.L) + (size_t)t * NTP;
-    for (int r = threadIdx.x; r < NTQ; r += blockDim.x) {
+    for (int r = warp; r < NTQ; r += 4 * G) {
       double v = 0.0;
-#pragma unroll 8
-      for (int q = 0; q < 32 * G; q++) v += sc[r * (32 * G) + q];
-      Lt[r] += v;
+#pragma unroll
+      for (int q = 0; q < G; q++) v += sc[r * (32 * G) + 32 * q + lane];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) Lt[r] += v;
     }
     tc_bar_cta();
   }

@@ -391,7 +391,7 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
                                                               const int* __restrict__ src, const TcBodies b,
                                                               const TcCells c, TcOut out) {
   // per warp source tile, three 16-byte vectors per source (one broadcast load each):
-  // (xh, yh, zh, xl) (yl, zl, mh, ml) (vx, vy, vz, -)
+  // (xh, yh, xl, yl) (zh, zl, mh, ml) (vx, vy, vz, -); x and y are consumed as packed pairs
   __shared__ float4 tile[kP2PWarps][32][3];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4(*T)[3] = tile[w];
@@ -418,8 +418,11 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
         tc_split(b.z[i], Zc, zh, zl);
         if (JERK) { vxi = (float)b.vx[i]; vyi = (float)b.vy[i]; vzi = (float)b.vz[i]; }
       }
+      // negated target terms: x + (-y) rounds exactly as x - y, so the packed sums below
+      // give bit for bit the scalar tc_pair32 values used by the strongest-pair correction
+      const float2 nh = make_float2(-xh, -yh), nl = make_float2(-xl, -yl), nv = make_float2(-vxi, -vyi);
       TcF2 pot = {0, 0}, ax = {0, 0}, ay = {0, 0}, az = {0, 0}, jx = {0, 0}, jy = {0, 0}, jz = {0, 0};
-      float best = 0.f;
+      unsigned bestkey = 0u;  // strength bits of the strongest pair so far, low 5 bits cleared
       int bj = -1;
       for (int q = sb; q < se; q++) {
         int s = src[q];
@@ -430,40 +433,56 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
           if (lane < cnt) {
             int j = jb + j0 + lane;
             float4 s0, s1;
-            tc_split(b.x[j], Xc, s0.x, s0.w);
-            tc_split(b.y[j], Yc, s0.y, s1.x);
-            tc_split(b.z[j], Zc, s0.z, s1.y);
+            tc_split(b.x[j], Xc, s0.x, s0.z);
+            tc_split(b.y[j], Yc, s0.y, s0.w);
+            tc_split(b.z[j], Zc, s1.x, s1.y);
             tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, s1.z, s1.w);
             T[lane][0] = s0;
             T[lane][1] = s1;
             if (JERK) T[lane][2] = make_float4((float)b.vx[j], (float)b.vy[j], (float)b.vz[j], 0.f);
           }
           __syncwarp();
-          float sp = 0, sx = 0, sy = 0, sz = 0, qx = 0, qy = 0, qz = 0;
+          float sp = 0, sz = 0, qz = 0;
+          float2 sxy = make_float2(0.f, 0.f), qxy = make_float2(0.f, 0.f);
+          unsigned key = 0u;  // (strength bits & ~31) | jj of this tile's strongest pair
           if (vi) {
             for (int jj = grp; jj < cnt; jj += ng) {
               const float4 s0 = T[jj][0], s1 = T[jj][1];
-              const float4 s2 = JERK ? T[jj][2] : make_float4(0.f, 0.f, 0.f, 0.f);
-              TcPair32 v = tc_pair32<JERK>(s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w, s2.x, s2.y, s2.z, xh, yh,
-                                           zh, xl, yl, zl, vxi, vyi, vzi);
-              sp = __fadd_rn(sp, v.f0);
-              sx = __fmaf_rn(v.dx, v.f, sx);
-              sy = __fmaf_rn(v.dy, v.f, sy);
-              sz = __fmaf_rn(v.dz, v.f, sz);
+              const float2 dxy = __fadd2_rn(__fadd2_rn(make_float2(s0.x, s0.y), nh),
+                                            __fadd2_rn(make_float2(s0.z, s0.w), nl));
+              const float dz = __fadd_rn(__fsub_rn(s1.x, zh), __fsub_rn(s1.y, zl));
+              const float r2 = __fmaf_rn(dxy.x, dxy.x, __fmaf_rn(dxy.y, dxy.y, __fmul_rn(dz, dz)));
+              float ri = 0.f;
+              if (r2 > 0.f) {
+                const float y = rsqrtf(r2);
+                const float e = __fmaf_rn(-__fmul_rn(r2, y), y, 1.f);
+                ri = __fmaf_rn(__fmul_rn(0.5f, y), e, y);
+              }
+              const float f0 = __fmaf_rn(s1.w, ri, __fmul_rn(s1.z, ri));
+              const float ri2 = __fmul_rn(ri, ri);
+              const float f = __fmul_rn(f0, ri2);
+              sp = __fadd_rn(sp, f0);
+              sxy = __ffma2_rn(dxy, make_float2(f, f), sxy);
+              sz = __fmaf_rn(dz, f, sz);
               if (JERK) {
-                qx = __fmaf_rn(v.dx, v.g, __fmaf_rn(v.dvx, v.f, qx));
-                qy = __fmaf_rn(v.dy, v.g, __fmaf_rn(v.dvy, v.f, qy));
-                qz = __fmaf_rn(v.dz, v.g, __fmaf_rn(v.dvz, v.f, qz));
+                const float4 s2 = T[jj][2];
+                const float2 dv = __fadd2_rn(make_float2(s2.x, s2.y), nv);
+                const float dvz = __fsub_rn(s2.z, vzi);
+                const float vr = __fmul_rn(3.f, __fmaf_rn(dxy.x, dv.x, __fmaf_rn(dxy.y, dv.y, __fmul_rn(dz, dvz))));
+                const float g = __fmul_rn(__fmul_rn(-f, ri2), vr);
+                qxy = __ffma2_rn(dxy, make_float2(g, g), __ffma2_rn(dv, make_float2(f, f), qxy));
+                qz = __fmaf_rn(dz, g, __fmaf_rn(dvz, f, qz));
               }
-              float strength = __fmul_rn(v.f0, v.ri);  // m / r^2
-              if (strength > best) {
-                best = strength;
-                bj = jb + j0 + jj;
-              }
+              // m / r^2 >= 0, so its bits order like the value
+              key = max(key, (__float_as_uint(__fmul_rn(f0, ri)) & ~31u) | (unsigned)jj);
             }
           }
-          pot.add(sp); ax.add(sx); ay.add(sy); az.add(sz);
-          if (JERK) { jx.add(qx); jy.add(qy); jz.add(qz); }
+          if ((key & ~31u) > bestkey) {
+            bestkey = key & ~31u;
+            bj = jb + j0 + (int)(key & 31u);
+          }
+          pot.add(sp); ax.add(sxy.x); ay.add(sxy.y); az.add(sz);
+          if (JERK) { jx.add(qxy.x); jy.add(qxy.y); jz.add(qz); }
         }
       }
       TcAcc<JERK> a;

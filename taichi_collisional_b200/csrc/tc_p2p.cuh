@@ -26,6 +26,24 @@ struct TcAcc {
       jz += __shfl_xor_sync(0xffffffffu, jz, o);
     }
   }
+  // sum of the ng lane groups (group g = lanes [g gsz, (g + 1) gsz)) into group 0 by a fixed
+  // tree: at step s, group g (a multiple of 2 s) adds group g + s
+  __device__ __forceinline__ void add_groups(int gsz, int ng, int grp) {
+    for (int st = 1; st < ng; st <<= 1) {
+      const int off = st * gsz;
+      const bool take = (grp % (2 * st)) == 0 && grp + st < ng;
+      double v;
+      v = __shfl_down_sync(0xffffffffu, pot, off); if (take) pot += v;
+      v = __shfl_down_sync(0xffffffffu, ax, off); if (take) ax += v;
+      v = __shfl_down_sync(0xffffffffu, ay, off); if (take) ay += v;
+      v = __shfl_down_sync(0xffffffffu, az, off); if (take) az += v;
+      if (JERK) {
+        v = __shfl_down_sync(0xffffffffu, jx, off); if (take) jx += v;
+        v = __shfl_down_sync(0xffffffffu, jy, off); if (take) jy += v;
+        v = __shfl_down_sync(0xffffffffu, jz, off); if (take) jz += v;
+      }
+    }
+  }
 };
 
 template <bool JERK>
@@ -67,16 +85,14 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p(const int* __restrict__ 
     if (!c.has_sink[t]) continue;
     int tb = c.begin[t], nt = c.nbody[t];
     int sb = tstart[t], se = tstart[t + 1];
-    int gsz = 32, ng = 1;
-    if (nt <= 16) {
-      gsz = 1;
-      while (gsz < nt) gsz <<= 1;
-      ng = 32 / gsz;
-    }
-    int grp = lane / gsz, ti = lane % gsz;
-    for (int t0 = 0; t0 < nt; t0 += gsz) {
+    for (int t0 = 0; t0 < nt; t0 += 32) {
+      // up to 32 targets per pass; a last pass of r <= 16 targets runs floor(32 / r) lane
+      // groups of r lanes, each over every ng-th source
+      const int r = min(32, nt - t0);
+      const int gsz = r > 16 ? 32 : r, ng = 32 / gsz;
+      const int grp = lane / gsz, ti = lane % gsz;
       int i = tb + t0 + ti;
-      bool vi = (t0 + ti) < nt;
+      bool vi = grp < ng && (t0 + ti) < nt;
       double xi = 0, yi = 0, zi = 0, vxi = 0, vyi = 0, vzi = 0;
       if (vi) {
         xi = b.x[i]; yi = b.y[i]; zi = b.z[i];
@@ -91,7 +107,7 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p(const int* __restrict__ 
           for (int j = jb + grp; j < je; j += ng) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, j, a);
         }
       }
-      for (int o = gsz; o < 32; o <<= 1) a.add_xor(o);
+      a.add_groups(gsz, ng, grp);
       if (vi && grp == 0 && (b.flags[i] & 1)) {
         out.pot[i] += a.pot;
         out.ax[i] += a.ax;
@@ -401,16 +417,14 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
     const double Xc = c.X[t], Yc = c.Y[t], Zc = c.Z[t];
     int tb = c.begin[t], nt = c.nbody[t];
     int sb = tstart[t], se = tstart[t + 1];
-    int gsz = 32, ng = 1;
-    if (nt <= 16) {
-      gsz = 1;
-      while (gsz < nt) gsz <<= 1;
-      ng = 32 / gsz;
-    }
-    int grp = lane / gsz, ti = lane % gsz;
-    for (int t0 = 0; t0 < nt; t0 += gsz) {
+    for (int t0 = 0; t0 < nt; t0 += 32) {
+      // up to 32 targets per pass; a last pass of r <= 16 targets runs floor(32 / r) lane
+      // groups of r lanes, each over every ng-th source
+      const int r = min(32, nt - t0);
+      const int gsz = r > 16 ? 32 : r, ng = 32 / gsz;
+      const int grp = lane / gsz, ti = lane % gsz;
       int i = tb + t0 + ti;
-      bool vi = (t0 + ti) < nt;
+      bool vi = grp < ng && (t0 + ti) < nt;
       float xh = 0, yh = 0, zh = 0, xl = 0, yl = 0, zl = 0, vxi = 0, vyi = 0, vzi = 0;
       if (vi) {
         tc_split(b.x[i], Xc, xh, xl);
@@ -511,7 +525,7 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
         tc_p2p_one<JERK>(b.x[i], b.y[i], b.z[i], JERK ? b.vx[i] : 0.0, JERK ? b.vy[i] : 0.0, JERK ? b.vz[i] : 0.0,
                          b, j, a);
       }
-      for (int o = gsz; o < 32; o <<= 1) a.add_xor(o);
+      a.add_groups(gsz, ng, grp);
       if (vi && grp == 0 && (b.flags[i] & 1)) {
         out.pot[i] += a.pot;
         out.ax[i] += a.ax;

@@ -9,24 +9,37 @@
 
 namespace tc {
 
-// L2L into cell ci (level >= 1) from its parent; one warp per cell
+// L2L into cell ci (level >= 1) from its parent; one warp per cell.  The parent's local (and
+// Ldot) is staged in shared memory as complex full storage.
 template <int P, bool JERK>
-__global__ void __launch_bounds__(kUpWarps * 32) k_l2l_level(int l, TcCells c, const int* __restrict__ lv_start,
-                                                             const int* __restrict__ lv_count) {
+__global__ void __launch_bounds__(TcTransW<P>::W * 32) k_l2l_level(int l, TcCells c,
+                                                                   const int* __restrict__ lv_start,
+                                                                   const int* __restrict__ lv_count) {
+  constexpr int W = TcTransW<P>::W;
   constexpr int NT = (P + 1) * (P + 1);
   constexpr int NOUT = (P + 1) * (P + 2) / 2;
   constexpr int PER = (NOUT + 31) / 32;
-  __shared__ cd sG[kUpWarps][NT];
+  __shared__ cd sG[W][NT];
+  __shared__ cd sL[W][NT];
+  __shared__ cd sLd[W][JERK ? NT : 1];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int cnt = lv_count[l], st = lv_start[l];
-  for (int k = blockIdx.x * kUpWarps + w; k < cnt; k += gridDim.x * kUpWarps) {
+  for (int k = blockIdx.x * W + w; k < cnt; k += gridDim.x * W) {
     int ci = st + k;
     if (!c.has_sink[ci]) continue;
     int pa = c.parent[ci];
     cd* G = sG[w];
-    tc_warp_gnm_smem<P>(c.X[pa] - c.X[ci], c.Y[pa] - c.Y[ci], c.Z[pa] - c.Z[ci], G);
+    cd* SL = sL[w];
+    cd* SLd = sLd[w];
     const double* Lp = c.L + (size_t)pa * NT;
     const double* Ldp = JERK ? c.Ld + (size_t)pa * NT : nullptr;
+    for (int i = lane; i < NT; i += 32) {
+      int n = 0;
+      while ((n + 1) * (n + 1) <= i) n++;
+      SL[i] = tc_r2c(Lp, n, i - n * n - n);
+      if (JERK) SLd[i] = tc_r2c(Ldp, n, i - n * n - n);
+    }
+    tc_warp_gnm_smem<P>(c.X[pa] - c.X[ci], c.Y[pa] - c.Y[ci], c.Z[pa] - c.Z[ci], G);  // ends with __syncwarp
     double* Lc = c.L + (size_t)ci * NT;
     double* Ldc = JERK ? c.Ld + (size_t)ci * NT : nullptr;
 #pragma unroll
@@ -37,12 +50,14 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_l2l_level(int l, TcCells c, c
       while ((n + 1) * (n + 2) / 2 <= o) n++;
       int m = o - n * (n + 1) / 2;
       cd s = mk(0, 0), sd = mk(0, 0);
-      for (int kk = 0; kk <= P - n; kk++)
+      for (int kk = 0; kk <= P - n; kk++) {
+        const int nn = n + kk, base = nn * nn + nn + m;  // local (n + kk, m + ll)
         for (int ll = -kk; ll <= kk; ll++) {
           cd g = conj(G[kk * kk + kk + ll]);
-          s += tc_r2c(Lp, n + kk, m + ll) * g;
-          if (JERK) sd += tc_r2c(Ldp, n + kk, m + ll) * g;
+          s += SL[base + ll] * g;
+          if (JERK) sd += SLd[base + ll] * g;
         }
+      }
       int is = n * n + n;
       Lc[is + m] += s.x;
       if (m > 0) Lc[is - m] += s.y;

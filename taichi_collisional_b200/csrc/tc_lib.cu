@@ -637,9 +637,9 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   }
   for (int l = maxl; l >= 0; l--) {
     int cnt = ctx->lv.count[l];
-    int g = nblocks(cnt, kUpWarps);
+    int g = nblocks(cnt, TcTransW<P>::W);
     if (g > 148 * 16) g = 148 * 16;
-    k_upward_level<P, JERK><<<g, kUpWarps * 32, 0, st>>>(l, b, cv, d_start, d_count, ctx->d_err);
+    k_upward_level<P, JERK><<<g, TcTransW<P>::W * 32, 0, st>>>(l, b, cv, d_start, d_count, ctx->d_err);
   }
   if (ctx->events) cudaEventRecord(ctx->ev[2], st);
   // ---- traversal
@@ -784,9 +784,9 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   ctx->launches += maxl + (ctx->nleaf > 0);
   for (int l = 1; l <= maxl; l++) {
     int cnt = ctx->lv.count[l];
-    int g = nblocks(cnt, kUpWarps);
+    int g = nblocks(cnt, TcTransW<P>::W);
     if (g > 148 * 16) g = 148 * 16;
-    k_l2l_level<P, JERK><<<g, kUpWarps * 32, 0, st>>>(l, cv, d_start, d_count);
+    k_l2l_level<P, JERK><<<g, TcTransW<P>::W * 32, 0, st>>>(l, cv, d_start, d_count);
   }
   if (ctx->nleaf > 0) {
     int g = nblocks(ctx->nleaf, kUpWarps);

@@ -372,9 +372,11 @@ __device__ __forceinline__ void tc_warp_gnm_smem(double dx, double dy, double dz
   __syncwarp();
 }
 
-// M2M into cell ci from its children (O(p^4) complex translation, kernel_fast_lean.h:921-931)
+// M2M into cell ci from its children (O(p^4) complex translation, kernel_fast_lean.h:921-931).
+// Each child's multipole (and Mdot) is staged in shared memory as complex full storage
+// (negative orders by symmetry), so every term is two shared loads and a complex FMA.
 template <int P, bool JERK>
-__device__ void tc_m2m_warp(int ci, const TcCells& c, cd* G) {
+__device__ void tc_m2m_warp(int ci, const TcCells& c, cd* G, cd* SM, cd* SMd) {
   constexpr int NT = (P + 1) * (P + 1);
   constexpr int NOUT = (P + 1) * (P + 2) / 2;
   constexpr int PER = (NOUT + 31) / 32;
@@ -384,9 +386,15 @@ __device__ void tc_m2m_warp(int ci, const TcCells& c, cd* G) {
   for (int k = 0; k < PER; k++) { acc[k] = mk(0, 0); accd[k] = mk(0, 0); }
   int ch0 = c.child[ci], nch = c.nchild[ci];
   for (int ch = ch0; ch < ch0 + nch; ch++) {
-    tc_warp_gnm_smem<P>(c.X[ch] - c.X[ci], c.Y[ch] - c.Y[ci], c.Z[ch] - c.Z[ci], G);
     const double* Mc = c.M + (size_t)ch * NT;
     const double* Mdc = JERK ? c.Md + (size_t)ch * NT : nullptr;
+    for (int i = lane; i < NT; i += 32) {
+      int n = 0;
+      while ((n + 1) * (n + 1) <= i) n++;
+      SM[i] = tc_r2c(Mc, n, i - n * n - n);
+      if (JERK) SMd[i] = tc_r2c(Mdc, n, i - n * n - n);
+    }
+    tc_warp_gnm_smem<P>(c.X[ch] - c.X[ci], c.Y[ch] - c.Y[ci], c.Z[ch] - c.Z[ci], G);  // ends with __syncwarp
 #pragma unroll
     for (int k = 0; k < PER; k++) {
       int o = lane + 32 * k;
@@ -396,11 +404,12 @@ __device__ void tc_m2m_warp(int ci, const TcCells& c, cd* G) {
       int m = o - n * (n + 1) / 2;
       cd s = mk(0, 0), sd = mk(0, 0);
       for (int kk = 0; kk <= n; kk++) {
-        int lo = max(-kk, m - n + kk), hi = min(kk, m + n - kk);
+        const int lo = max(-kk, m - n + kk), hi = min(kk, m + n - kk);
+        const int nn = n - kk, base = nn * nn + nn + m;  // source (n - kk, m - l)
         for (int l = lo; l <= hi; l++) {
           cd g = G[kk * kk + kk + l];
-          s += tc_r2c(Mc, n - kk, m - l) * g;
-          if (JERK) sd += tc_r2c(Mdc, n - kk, m - l) * g;
+          s += SM[base - l] * g;
+          if (JERK) sd += SMd[base - l] * g;
         }
       }
       acc[k] += s;
@@ -426,6 +435,13 @@ __device__ void tc_m2m_warp(int ci, const TcCells& c, cd* G) {
     }
   }
 }
+
+// warps per block of the M2M and L2L level kernels (three NT-complex arrays per warp in
+// static shared memory, at most 48 KB)
+template <int P>
+struct TcTransW {
+  static constexpr int W = P >= 14 ? 2 : 4;
+};
 
 constexpr int kUpWarps = 4;
 
@@ -498,19 +514,23 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_leaf_balls(int ncell, const T
 
 // inner cells of level l: ball over the children's points, then M2M from the children
 template <int P, bool JERK>
-__global__ void __launch_bounds__(kUpWarps * 32) k_upward_level(int l, const TcBodies b, TcCells c,
-                                                                const int* __restrict__ lv_start,
-                                                                const int* __restrict__ lv_count, unsigned int* err) {
-  __shared__ cd sG[kUpWarps][(P + 1) * (P + 1)];
+__global__ void __launch_bounds__(TcTransW<P>::W * 32) k_upward_level(int l, const TcBodies b, TcCells c,
+                                                                      const int* __restrict__ lv_start,
+                                                                      const int* __restrict__ lv_count,
+                                                                      unsigned int* err) {
+  constexpr int W = TcTransW<P>::W, NT = (P + 1) * (P + 1);
+  __shared__ cd sG[W][NT];
+  __shared__ cd sM[W][NT];
+  __shared__ cd sMd[W][JERK ? NT : 1];
   __shared__ double s_td[193];
   tc_load_tdesign(s_td);
   int w = threadIdx.x >> 5;
   int cnt = lv_count[l], st = lv_start[l];
-  for (int k = blockIdx.x * kUpWarps + w; k < cnt; k += gridDim.x * kUpWarps) {
+  for (int k = blockIdx.x * W + w; k < cnt; k += gridDim.x * W) {
     int ci = st + k;
     if (c.nchild[ci] == 0) continue;
     tc_cell_ball(ci, b, c, s_td, err);
-    tc_m2m_warp<P, JERK>(ci, c, sG[w]);
+    tc_m2m_warp<P, JERK>(ci, c, sG[w], sM[w], sMd[w]);
     __syncwarp();
   }
 }

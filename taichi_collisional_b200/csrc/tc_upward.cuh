@@ -74,26 +74,38 @@ __device__ bool tc_circumsphere(int k, const double (*q)[3], double* c, double* 
   return true;
 }
 
-// smallest ball with q on its boundary enclosing the support set s; updates s
+// Smallest ball with q on its boundary enclosing the support set s; updates s.  Every subset
+// of s (at most 3 points, with q) is one lane's candidate; the warp keeps the valid candidate
+// of least radius, ties to the lowest subset index -- the subset a loop over the subsets in
+// index order keeps -- and every lane ends with the same result.
 __device__ bool tc_mb_small(double (*s)[3], int& ns, const double* q, double* c, double* r2) {
-  int best = -1;
-  double bc[3] = {0, 0, 0}, br2 = INFINITY;
-  for (int mask = 0; mask < (1 << ns); mask++) {
-    if (__popc(mask) > 3) continue;
+  const int lane = threadIdx.x & 31;
+  const int mask = lane;
+  double rr = INFINITY, cc[3] = {0, 0, 0};
+  bool ok = false;
+  if (mask < (1 << ns) && __popc(mask) <= 3) {
     double pts[4][3];
     int k = 0;
     pts[k][0] = q[0]; pts[k][1] = q[1]; pts[k][2] = q[2]; k++;
     for (int i = 0; i < ns; i++)
       if (mask & (1 << i)) { pts[k][0] = s[i][0]; pts[k][1] = s[i][1]; pts[k][2] = s[i][2]; k++; }
-    double cc[3], rr;
-    if (!tc_circumsphere(k, pts, cc, &rr)) continue;
-    if (rr >= br2) continue;
-    bool ok = true;
-    for (int i = 0; i < ns && ok; i++)
-      if (!(mask & (1 << i)) && tc_d2(s[i], cc) > rr * (1 + 1e-13) + 1e-300) ok = false;
-    if (ok) { br2 = rr; bc[0] = cc[0]; bc[1] = cc[1]; bc[2] = cc[2]; best = mask; }
+    if (tc_circumsphere(k, pts, cc, &rr)) {
+      ok = true;
+      for (int i = 0; i < ns && ok; i++)
+        if (!(mask & (1 << i)) && tc_d2(s[i], cc) > rr * (1 + 1e-13) + 1e-300) ok = false;
+    }
   }
-  if (best < 0) return false;
+  double krr = ok ? rr : INFINITY;
+  int km = ok ? mask : 0x7fffffff;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double orr = __shfl_xor_sync(0xffffffffu, krr, o);
+    const int om = __shfl_xor_sync(0xffffffffu, km, o);
+    if (orr < krr || (orr == krr && om < km)) { krr = orr; km = om; }
+  }
+  if (km == 0x7fffffff) return false;
+  const int best = km;
+  const double bc0 = __shfl_sync(0xffffffffu, cc[0], best), bc1 = __shfl_sync(0xffffffffu, cc[1], best),
+               bc2 = __shfl_sync(0xffffffffu, cc[2], best);
   double nsv[4][3];
   int k = 0;
   nsv[k][0] = q[0]; nsv[k][1] = q[1]; nsv[k][2] = q[2]; k++;
@@ -101,8 +113,8 @@ __device__ bool tc_mb_small(double (*s)[3], int& ns, const double* q, double* c,
     if (best & (1 << i)) { nsv[k][0] = s[i][0]; nsv[k][1] = s[i][1]; nsv[k][2] = s[i][2]; k++; }
   for (int i = 0; i < k; i++) { s[i][0] = nsv[i][0]; s[i][1] = nsv[i][1]; s[i][2] = nsv[i][2]; }
   ns = k;
-  c[0] = bc[0]; c[1] = bc[1]; c[2] = bc[2];
-  *r2 = br2;
+  c[0] = bc0; c[1] = bc1; c[2] = bc2;
+  *r2 = krr;
   return true;
 }
 

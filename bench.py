@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--accuracy-targets", type=int, default=4096,
                     help="seeded bodies at which both forms are compared with FP64 direct sums (untimed)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="launch each evaluation's kernels directly instead of replaying one captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -222,6 +224,7 @@ def main():
     prec = {"fp64": tcb.PREC_FP64, "mixed": tcb.PREC_MIXED, "mixed_m2l": tcb.PREC_MIXED_M2L}[args.precision]
     g = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
                     precision=prec, device=local, judge_n=args.judge)
+    g.set_graph(not args.no_graph)  # the first evaluation captures, the later ones replay
     dt = 1.0 / 4096
 
     def evaluate():
@@ -283,6 +286,7 @@ def main():
     if not args.no_fp64_arm and args.precision != "fp64":
         g64 = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
                           precision=tcb.PREC_FP64, device=local, judge_n=args.judge)
+        g64.set_graph(not args.no_graph)
         out64 = {k: torch.empty_like(v) for k, v in out.items()}
         g64.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"], out=out64)
         if dist:
@@ -363,7 +367,8 @@ def main():
                 "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded Plummer sphere, Kroupa IMF masses)",
                 "config": dict(WORKLOAD, n=n, p=p, precision=args.precision,
-                               parallelism="replicas" if world > 1 else "single"),
+                               parallelism="replicas" if world > 1 else "single",
+                               evaluation="one CUDA graph replay" if g.graph_ready() else "direct launches"),
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb, "clocks": clocks,
                 "accuracy": accuracy,
                 "fp64_form": fp64,

@@ -100,6 +100,21 @@ tc_status tc_destroy(tc_ctx* ctx);
 /* Run work on this CUDA stream (cudaStream_t passed as void*; NULL = legacy default). */
 tc_status tc_set_stream(tc_ctx* ctx, void* stream);
 
+/* The whole evaluation as one CUDA graph (SURVEY's boundary call (B) as a graph; no counterpart
+ * in the reference, which has no device).  With on != 0, tc_evaluate replays a captured graph
+ * when the call matches the one it was captured for (same n, memory kind, every input/output
+ * pointer and every tc_params field); any other call runs the normal path, returns its results
+ * and then captures the graph for that call.  The captured sequence reads every count on the
+ * device and sizes its launches by capacities 25 % over the planning call's tree and lists; an
+ * overflow (reported in the status block the graph copies back) re-runs the call on the normal
+ * path and re-plans.  Host buffers (TC_MEM_HOST) must be pinned to be captured; with pageable
+ * host buffers, the time-step pass, the order selector or TC_PREC_MIXED_M2L the normal path
+ * runs.  tc_graph_ready reports whether the next matching call will replay. */
+tc_status tc_set_graph(tc_ctx* ctx, int on);
+int tc_graph_ready(const tc_ctx* ctx);
+/* Why the last capture was abandoned (stage and CUDA error), or "" when it succeeded. */
+const char* tc_graph_note(const tc_ctx* ctx);
+
 /* One force evaluation: the replacement of get_force_and_potential(bodies, false).
  *   x,y,z,m          positions and masses (required)
  *   vx,vy,vz         velocities (jerks tree; may be NULL for the top tree)

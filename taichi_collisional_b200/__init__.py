@@ -59,7 +59,7 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
-           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps"]
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -84,6 +84,12 @@ def load_library(path=LIB_PATH):
     L.tc_destroy.restype = C.c_int
     L.tc_set_stream.argtypes = [C.c_void_p, C.c_void_p]
     L.tc_set_stream.restype = C.c_int
+    L.tc_set_graph.argtypes = [C.c_void_p, C.c_int]
+    L.tc_set_graph.restype = C.c_int
+    L.tc_graph_ready.argtypes = [C.c_void_p]
+    L.tc_graph_ready.restype = C.c_int
+    L.tc_graph_note.argtypes = [C.c_void_p]
+    L.tc_graph_note.restype = C.c_char_p
     L.tc_evaluate.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8 + [C.c_void_p] * 7 + [C.c_int]
     L.tc_evaluate.restype = C.c_int
     L.tc_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
@@ -196,6 +202,20 @@ class Gravity:
 
     def set_stream(self, stream_ptr):
         self._L.tc_set_stream(self._h, C.c_void_p(stream_ptr))
+
+    def set_graph(self, on=True):
+        """Run evaluate as one captured CUDA graph (tc_set_graph): the first call with a given set
+        of buffers runs normally and captures; matching calls replay.  Host buffers must be
+        pinned to be captured."""
+        self._check(self._L.tc_set_graph(self._h, 1 if on else 0), "tc_set_graph")
+
+    def graph_ready(self):
+        """True when the next evaluate with the same buffers replays the captured graph."""
+        return bool(self._L.tc_graph_ready(self._h))
+
+    def graph_note(self):
+        """Why the last capture was abandoned ('' when it succeeded)."""
+        return self._L.tc_graph_note(self._h).decode()
 
     def _check(self, rc, what):
         if rc != 0:

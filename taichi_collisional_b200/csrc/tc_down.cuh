@@ -110,13 +110,15 @@ __device__ __forceinline__ void tc_l2p_acc(const cd* sl, double dx, double dy, d
 // tabulated recurrence of the P2M (TcColTab, tc_col_next).
 template <int P, bool JERK>
 __global__ void __launch_bounds__(kUpWarps * 32) k_l2p(const int* __restrict__ leaves, int nleaf, const TcBodies b,
-                                                       const TcCells c, TcOut out) {
+                                                       const TcCells c, TcOut out,
+                                                       const unsigned* nldev = nullptr) {
   constexpr int NT = (P + 1) * (P + 1);
   __shared__ cd sL[kUpWarps][NT];
   __shared__ cd sLd[kUpWarps][JERK ? NT : 1];
   __shared__ TcColTab<P> tab;
   tab.fill();
   __syncthreads();
+  if (nldev) nleaf = (int)*nldev;  // device-sized launch (graph)
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int k = blockIdx.x * kUpWarps + w; k < nleaf; k += gridDim.x * kUpWarps) {
     int ci = leaves[k];

@@ -59,6 +59,21 @@ struct DBuf {
   }
 };
 
+// what a captured evaluation was recorded for (a call must match to replay it)
+struct TcGraphKey {
+  int n = -1, mem = -1;
+  const void* ptr[15] = {};
+  tc_params prm;
+};
+
+// read back after a replay (small device structs, copied by the graph into pinned memory)
+struct TcGraphStatus {
+  unsigned err;
+  unsigned small[4];
+  TcLevels lv;
+  TcTravCounters cnt;
+};
+
 struct EvalTimes {
   cudaEvent_t e[8];
 };
@@ -87,7 +102,8 @@ struct tc_ctx {
   DBuf<double> cdbl;   // 7 * ccap
   DBuf<uint8_t> csink;
   DBuf<int> split_off;
-  DBuf<double> expn;   // (2 or 4) * ncell * NT
+  DBuf<double> expn;   // (2 or 4) * expn_stride * NT
+  size_t expn_stride = 0;  // cells per expansion array: ncell, or ccap in a captured graph
   size_t ccap = 0;
   // lists
   DBuf<int2> front[2];
@@ -123,7 +139,8 @@ struct tc_ctx {
   TcLevels* d_lv = nullptr;
   TcTravCounters* d_cnt = nullptr;
   unsigned int* d_err = nullptr;
-  unsigned int* d_small = nullptr;  // [0] m2l targets, [1] p2p targets, [2] leaves, [9] tensor M2L counter
+  unsigned int* d_small = nullptr;  // [0] m2l targets, [1] p2p targets, [2] leaves, [9] tensor M2L counter,
+                                    // [10] target counter of the persistent FP64 M2L (graph)
   DBuf<float> tc_bins;  // tensor-core M2L bin matrices (hi, lo) of order tc_bins_q
   int tc_bins_q = -1;
   int nsm = 0;
@@ -138,6 +155,19 @@ struct tc_ctx {
   unsigned long long n_inter = 0;
   cudaEvent_t ev[8];
   bool events = false;
+  // CUDA graph of the whole evaluation (tc_set_graph)
+  bool graph_on = false, gvalid = false;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
+  cudaStream_t gstream = nullptr;
+  TcGraphKey gkey;
+  TcGraphStatus* hstat = nullptr;  // pinned: written by the graph's last copies
+  double* hjudge = nullptr;        // pinned: 7 x judge targets (FP64 direct sums and FMM values)
+  size_t hjudge_cap = 0;
+  int gjudge_nt = 0;
+  long long glaunches = 0;
+  int gsbits = 1;
+  std::string gfail;  // why the last capture was abandoned (empty: captured)
 };
 
 static bool g_const_init[64];
@@ -282,7 +312,7 @@ static TcCells cells_view(tc_ctx* c, int NT) {
   v.gx = cd; v.gy = cd + cc; v.gz = cd + 2 * cc; v.X = cd + 3 * cc; v.Y = cd + 4 * cc; v.Z = cd + 5 * cc;
   v.R = cd + 6 * cc;
   v.has_sink = c->csink.p;
-  size_t ne = (size_t)c->ncell * NT;
+  size_t ne = c->expn_stride * NT;
   bool jerk = c->prm.variant == TC_VARIANT_JERKS;
   v.M = c->expn.p;
   v.L = c->expn.p ? c->expn.p + ne : nullptr;
@@ -322,7 +352,8 @@ __global__ void k_nan_check(int n, const double* x, const double* y, const doubl
   if (i < n && !(isfinite(x[i]) && isfinite(y[i]) && isfinite(z[i]) && isfinite(m[i]))) tc_set_err(err, TC_EBIT_NAN);
 }
 
-__global__ void k_leaf_list(int ncell, const int* nchild, int* leaves, unsigned* cnt) {
+__global__ void k_leaf_list(int ncell, const int* nchild, int* leaves, unsigned* cnt, const int* ncdev = nullptr) {
+  if (ncdev) ncell = *ncdev;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool has = i < ncell && nchild[i] == 0;
   unsigned mask = __ballot_sync(0xffffffffu, has);
@@ -336,7 +367,8 @@ __global__ void k_leaf_list(int ncell, const int* nchild, int* leaves, unsigned*
 // sum over the P2P list of (sink-cell bodies) x (source-cell bodies)
 __global__ void k_p2p_count(const unsigned long long* __restrict__ keys, unsigned long long n, int sbits,
                             const int* __restrict__ nbody, const uint8_t* __restrict__ has_sink,
-                            unsigned long long* total) {
+                            unsigned long long* total, const unsigned long long* ndev = nullptr) {
+  if (ndev && *ndev < n) n = *ndev;
   unsigned long long loc = 0, mask = (1ull << sbits) - 1ull;
   for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (unsigned long long)gridDim.x * blockDim.x) {
@@ -620,6 +652,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   // ---- expansions
   size_t ne = (size_t)ctx->ncell * NT;
   TC_CK(ctx->expn.ensure(ne * (JERK ? 4 : 2)));
+  ctx->expn_stride = (size_t)ctx->ncell;
   cv = cells_view(ctx, NT);
   TC_CK(cudaMemsetAsync(cv.L, 0, ne * sizeof(double), st));
   if (JERK) TC_CK(cudaMemsetAsync(cv.Ld, 0, ne * sizeof(double), st));
@@ -797,6 +830,131 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   return TC_OK;
 }
 
+// timing event inside a capture: an external record node, so the replay records it
+static inline void graph_event(tc_ctx* ctx, int i, cudaStream_t st) {
+  if (ctx->events) cudaEventRecordWithFlags(ctx->ev[i], st, cudaEventRecordExternal);
+}
+
+// first failing stage of a capture (a launch that fails is left out of the graph without
+// invalidating the capture, so every stage is checked)
+static void graph_check(tc_ctx* ctx, const char* stage) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess && ctx->gfail.empty()) ctx->gfail = std::string(stage) + ": " + cudaGetErrorString(e);
+}
+
+// Device-sized form of run_fmm for a captured CUDA graph (tc_set_graph): no host reads.  Every
+// launch is sized by the capacities fixed when the graph was planned (ccap cells, mcap / pcap
+// list entries, fcap frontier pairs) and reads its count on the device (levels, list sizes,
+// target and leaf counts); loops over levels run to TC_MAX_LEVEL (empty levels exit at once).
+// An overflow sets d_err bits (the tree then stays consistent, the lists are clamped), which
+// the host reads after the replay before it uses the outputs.  FP64 / MIXED far field, fixed
+// order, no time-step pass.
+template <int P, bool JERK>
+static void run_fmm_graph(tc_ctx* ctx, int n) {
+  constexpr int NT = (P + 1) * (P + 1);
+  cudaStream_t st = ctx->stream;
+  const tc_params& prm = ctx->prm;
+  TcBodies b = bodies_view(ctx, n, JERK);
+  TcCells cv = cells_view(ctx, NT);
+  const int ccap = (int)ctx->ccap;
+  const int* d_ncell = &ctx->d_lv->ncell;
+  int* d_start = &ctx->d_lv->start[0];
+  int* d_count = &ctx->d_lv->count[0];
+  long long L = 0;
+  // ---- tree levels (as run_fmm)
+  k_tree_root<<<1, 1, 0, st>>>(n, cv, ctx->d_root, ctx->d_lv);
+  const int tgrid = 148 * 8;
+  for (int l = 0; l < TC_MAX_LEVEL + 1; l++) {
+    k_tree_split<<<tgrid, 128, 0, st>>>(l, prm.ncrit, b, cv, ctx->d_lv, ctx->split_off.p, ctx->d_err);
+    k_tree_scan<<<1, 1024, 0, st>>>(l, cv, ctx->d_lv, ccap, ctx->d_err);
+    k_tree_emit<<<tgrid, 128, 0, st>>>(l, cv, ctx->d_lv, ctx->split_off.p, ctx->d_root);
+  }
+  L += 1 + 3 * (TC_MAX_LEVEL + 1);
+  graph_check(ctx, "tree");
+  graph_event(ctx, 1, st);
+  // ---- expansions (capacity-strided) and upward pass
+  const size_t ne = (size_t)ccap * NT;
+  cudaMemsetAsync(cv.L, 0, ne * sizeof(double), st);
+  if (JERK) cudaMemsetAsync(cv.Ld, 0, ne * sizeof(double), st);
+  {
+    int g = std::min(nblocks(ccap, kUpWarps), 148 * 16);
+    k_leaf_balls<<<g, kUpWarps * 32, 0, st>>>(ccap, b, cv, ctx->d_err, ctx->d_lv);
+    g = std::min(nblocks(ccap, kP2MWarps), 148 * 16);
+    k_p2m_leaves<P, JERK><<<g, kP2MWarps * 32, 0, st>>>(ccap, b, cv, ctx->d_lv);
+  }
+  for (int l = TC_MAX_LEVEL; l >= 0; l--)
+    k_upward_level<P, JERK><<<148 * 16, TcTransW<P>::W * 32, 0, st>>>(l, b, cv, d_start, d_count, ctx->d_err);
+  L += 2 + TC_MAX_LEVEL + 1;
+  graph_check(ctx, "upward pass");
+  graph_event(ctx, 2, st);
+  // ---- traversal
+  const int sbits = ctx->gsbits;
+  const double theta2 = prm.theta * prm.theta;
+  k_trav_init<<<1, 1, 0, st>>>(ctx->front[0].p, ctx->d_cnt);
+  const int nsteps = 2 * (TC_MAX_LEVEL + 1) + 2;
+  for (int s = 0; s < nsteps; s++)
+    k_trav_step<<<148 * 8, 256, 0, st>>>(s, ctx->front[s & 1].p, ctx->front[(s + 1) & 1].p, ctx->fcap, ctx->d_cnt, cv,
+                                         theta2, prm.variant == TC_VARIANT_TOP, sbits, ctx->m2l.p, ctx->mcap,
+                                         ctx->p2p.p, ctx->pcap, ctx->d_err);
+  L += 1 + nsteps;
+  graph_check(ctx, "traversal");
+  // ---- sort lists (counts on the device) and per-target offsets
+  const int kbits = 2 * sbits;
+  unsigned long long *km = nullptr, *kp = nullptr;
+  L += radix_sort(ctx->m2l.p, nullptr, ctx->m2l_alt.p, nullptr, (int)ctx->mcap, kbits, ctx->hist.p, st, 0,
+                  &ctx->d_cnt->n_m2l, &km);
+  L += radix_sort(ctx->p2p.p, nullptr, ctx->p2p_alt.p, nullptr, (int)ctx->pcap, kbits, ctx->hist.p, st, 0,
+                  &ctx->d_cnt->n_p2p, &kp);
+  k_list_csr<<<148 * 8, 256, 0, st>>>(km, ctx->mcap, ccap, sbits, ctx->m2l_start.p, ctx->m2l_src.p,
+                                      &ctx->d_cnt->n_m2l, d_ncell);
+  k_list_csr<<<148 * 8, 256, 0, st>>>(kp, ctx->pcap, ccap, sbits, ctx->p2p_start.p, ctx->p2p_src.p,
+                                      &ctx->d_cnt->n_p2p, d_ncell);
+  cudaMemsetAsync(ctx->d_small, 0, 4 * sizeof(unsigned), st);
+  cudaMemsetAsync(&ctx->d_cnt->frontier[0], 0, sizeof(unsigned long long), st);
+  k_p2p_count<<<148 * 4, 256, 0, st>>>(kp, ctx->pcap, sbits, cv.nbody, cv.has_sink, &ctx->d_cnt->frontier[0],
+                                       &ctx->d_cnt->n_p2p);
+  k_list_targets<<<nblocks(ccap, 256), 256, 0, st>>>(ctx->m2l_start.p, ccap, ctx->m2l_tl.p, ctx->d_small, d_ncell);
+  k_list_targets<<<nblocks(ccap, 256), 256, 0, st>>>(ctx->p2p_start.p, ccap, ctx->p2p_tl.p, ctx->d_small + 1,
+                                                     d_ncell);
+  k_leaf_list<<<nblocks(ccap, 256), 256, 0, st>>>(ccap, cv.nchild, ctx->leaves.p, ctx->d_small + 2, d_ncell);
+  L += 6;
+  graph_check(ctx, "list sort and offsets");
+  graph_event(ctx, 3, st);
+  // ---- far field and near field
+  TcOut o = out_view(ctx, n, JERK);
+  cudaMemsetAsync(ctx->outs.p, 0, sizeof(double) * (size_t)n * (JERK ? 7 : 4), st);
+  cudaMemsetAsync(ctx->d_small + 10, 0, sizeof(unsigned), st);
+  k_m2l<P, P, JERK><<<ctx->nsm, tc_m2l_threads<P>(), (size_t)TcM2LSmem<P>::TOTAL * sizeof(double), st>>>(
+      ctx->m2l_tl.p, ccap, ctx->m2l_start.p, ctx->m2l_src.p, cv, ctx->d_small, ctx->d_small + 10);
+  graph_check(ctx, "M2L");
+  graph_event(ctx, 4, st);
+  {
+    const int g = nblocks(ccap, kP2PWarps);  // a warp per target slot; warps past the count exit
+    if (prm.precision != TC_PREC_FP64)
+      k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o,
+                                                       ctx->d_small + 1);
+    else
+      k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o,
+                                                 ctx->d_small + 1);
+  }
+  L += 2;
+  graph_check(ctx, "P2P");
+  graph_event(ctx, 5, st);
+  // ---- downward
+  for (int l = 1; l <= TC_MAX_LEVEL; l++)
+    k_l2l_level<P, JERK><<<148 * 16, TcTransW<P>::W * 32, 0, st>>>(l, cv, d_start, d_count);
+  {
+    const int g = std::min(nblocks(ccap, kUpWarps), 148 * 32);
+    k_l2p<P, JERK><<<g, kUpWarps * 32, 0, st>>>(ctx->leaves.p, ccap, b, cv, o, ctx->d_small + 2);
+  }
+  L += TC_MAX_LEVEL + 1;
+  graph_check(ctx, "downward pass");
+  graph_event(ctx, 6, st);
+  ctx->glaunches += L;
+}
+
+typedef void (*graph_fn)(tc_ctx*, int);
+
 typedef tc_status (*run_fn)(tc_ctx*, int);
 
 // RMS relative acceleration error of the last evaluation (Morton-order outputs) at nt seeded
@@ -855,6 +1013,18 @@ static run_fn pick(int p, bool jerk) {
 #define TC_CASE(P) \
   case P:          \
     return jerk ? run_fmm<P, true> : run_fmm<P, false>;
+    TC_ORDERS(TC_CASE)
+#undef TC_CASE
+    default:
+      return nullptr;
+  }
+}
+
+static graph_fn pick_graph(int p, bool jerk) {
+  switch (p) {
+#define TC_CASE(P) \
+  case P:          \
+    return jerk ? run_fmm_graph<P, true> : run_fmm_graph<P, false>;
     TC_ORDERS(TC_CASE)
 #undef TC_CASE
     default:
@@ -1003,6 +1173,8 @@ tc_status tc_create(const tc_params* prm, tc_ctx** out) {
   return TC_OK;
 }
 
+static void graph_drop(tc_ctx* ctx);
+
 tc_status tc_destroy(tc_ctx* ctx) {
   if (!ctx) return TC_ERR_ARG;
   cudaSetDevice(ctx->prm.device);
@@ -1025,6 +1197,10 @@ tc_status tc_destroy(tc_ctx* ctx) {
   if (ctx->d_small) cudaFree(ctx->d_small);
   if (ctx->events)
     for (int i = 0; i < 8; i++) cudaEventDestroy(ctx->ev[i]);
+  graph_drop(ctx);
+  if (ctx->gstream) cudaStreamDestroy(ctx->gstream);
+  if (ctx->hstat) cudaFreeHost(ctx->hstat);
+  if (ctx->hjudge) cudaFreeHost(ctx->hjudge);
   delete ctx;
   return TC_OK;
 }
@@ -1035,16 +1211,64 @@ tc_status tc_set_stream(tc_ctx* ctx, void* stream) {
   return TC_OK;
 }
 
+// statistics of the last evaluation and its status from the error bits
+static tc_status finish_stats(tc_ctx* ctx, int n, unsigned herr) {
+  tc_stats& S = ctx->stats;
+  S.n_bodies = n;
+  S.n_cells = ctx->ncell;
+  S.n_leaves = ctx->nleaf;
+  S.n_m2l = (long long)ctx->n_m2l;
+  S.n_p2p = (long long)ctx->n_p2p;
+  S.max_level = ctx->max_level;
+  S.n_p2p_inter = ctx->direct ? (long long)n * n : (long long)ctx->n_inter;
+  S.n_launches = ctx->launches;
+  S.flags = herr | ctx->tree_flags;
+  S.n_classes = ctx->n_classes;
+  for (int i = 0; i < 6; i++) {
+    S.class_order[i] = i < ctx->n_classes ? ctx->class_order[i] : 0;
+    S.class_pairs[i] = i < ctx->n_classes ? ctx->class_pairs[i] : 0;
+  }
+  S.m2l_flop_fraction = ctx->flop_frac;
+  S.judge_rms = ctx->judge_rms;
+  S.judge_redo = ctx->judge_redo;
+  if (ctx->events) {
+    float t[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    bool ok = true;
+    for (int i = 1; i < 8; i++) ok = ok && cudaEventElapsedTime(&t[i], ctx->ev[i - 1], ctx->ev[i]) == cudaSuccess;
+    ok = ok && cudaEventElapsedTime(&t[0], ctx->ev[0], ctx->ev[7]) == cudaSuccess;
+    if (!ok) {
+      cudaGetLastError();
+      for (int i = 0; i < 8; i++) t[i] = 0.f;
+    }
+    S.ms_total = t[0]; S.ms_tree = t[1]; S.ms_upward = t[2]; S.ms_traverse = t[3]; S.ms_m2l = t[4];
+    S.ms_p2p = t[5]; S.ms_downward = t[6];
+  }
+  if (herr & TC_EBIT_TIMEOUT) {
+    ctx->err = "a device-side wait of the tensor-core far field gave up";
+    return TC_ERR_TIMEOUT;
+  }
+  if ((herr | ctx->tree_flags) & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
+  if ((herr | ctx->tree_flags) & TC_EBIT_DEPTH) return TC_ERR_DEPTH;
+  return TC_OK;
+}
+
+
 static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
                                const double* vx, const double* vy, const double* vz, const double* m,
                                const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
                                double* jx, double* jy, double* jz, int mem, double* timestep);
+
+static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+                                const double* vx, const double* vy, const double* vz, const double* m,
+                                const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                                double* jx, double* jy, double* jz, int mem);
 
 tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
                       const double* vy, const double* vz, const double* m, const unsigned char* flags, double* ax,
                       double* ay, double* az, double* pot, double* jx, double* jy, double* jz, int mem) {
   if (!ctx) return TC_ERR_ARG;
   ctx->steps = false;
+  if (ctx->graph_on) return evaluate_graph(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, mem);
   return evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, mem, nullptr);
 }
 
@@ -1071,6 +1295,7 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
   if (jerk && (!vx || !vy || !vz)) return TC_ERR_ARG;
   if (mem != TC_MEM_HOST && mem != TC_MEM_DEVICE) return TC_ERR_ARG;
   TC_CK(cudaSetDevice(ctx->prm.device));
+  cudaGetLastError();  // an error left by an earlier, unrelated call is not this evaluation's
   cudaStream_t st = ctx->stream;
   ctx->n = n;
   ctx->launches = 0;
@@ -1203,40 +1428,289 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
   }
   TC_CK(cudaStreamSynchronize(st));
   TC_CK(cudaGetLastError());
-  // ---- statistics
-  tc_stats& S = ctx->stats;
-  S.n_bodies = n;
-  S.n_cells = ctx->ncell;
-  S.n_leaves = ctx->nleaf;
-  S.n_m2l = (long long)ctx->n_m2l;
-  S.n_p2p = (long long)ctx->n_p2p;
-  S.max_level = ctx->max_level;
-  S.n_p2p_inter = ctx->direct ? (long long)n * n : (long long)ctx->n_inter;
-  S.n_launches = ctx->launches;
-  S.flags = herr | ctx->tree_flags;
-  S.n_classes = ctx->n_classes;
-  for (int i = 0; i < 6; i++) {
-    S.class_order[i] = i < ctx->n_classes ? ctx->class_order[i] : 0;
-    S.class_pairs[i] = i < ctx->n_classes ? ctx->class_pairs[i] : 0;
+  return finish_stats(ctx, n, herr);
+}
+
+// ---------------------------------------------------------------------------------------
+// The evaluation as one CUDA graph (tc_set_graph).  A call that cannot replay (first call,
+// other pointers, sizes or parameters, or a capacity overflow reported by the last replay)
+// runs the normal path, whose results it returns, and then plans and captures: capacities
+// with headroom over that evaluation, every buffer allocated, the judge's targets uploaded,
+// and the whole device-sized sequence (inputs, tree, FMM, judge kernels, outputs and a status
+// block) recorded into a graph on a private stream.  A matching call replays the graph and
+// reads the status block: an overflow bit re-runs the call on the normal path (and re-plans).
+// ---------------------------------------------------------------------------------------
+static void graph_drop(tc_ctx* ctx) {
+  if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+  if (ctx->graph) cudaGraphDestroy(ctx->graph);
+  ctx->gexec = nullptr;
+  ctx->graph = nullptr;
+  ctx->gvalid = false;
+}
+
+static bool graph_key_equal(const TcGraphKey& a, const TcGraphKey& b) {
+  if (a.n != b.n || a.mem != b.mem) return false;
+  for (int i = 0; i < 15; i++)
+    if (a.ptr[i] != b.ptr[i]) return false;
+  return memcmp(&a.prm, &b.prm, sizeof(tc_params)) == 0;
+}
+
+static bool host_pinned(const void* p) {
+  if (!p) return true;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
   }
-  S.m2l_flop_fraction = ctx->flop_frac;
-  S.judge_rms = ctx->judge_rms;
-  S.judge_redo = ctx->judge_redo;
-  if (ctx->events) {
-    float t[8];
-    for (int i = 1; i < 8; i++) cudaEventElapsedTime(&t[i], ctx->ev[i - 1], ctx->ev[i]);
-    cudaEventElapsedTime(&t[0], ctx->ev[0], ctx->ev[7]);
-    S.ms_total = t[0]; S.ms_tree = t[1]; S.ms_upward = t[2]; S.ms_traverse = t[3]; S.ms_m2l = t[4];
-    S.ms_p2p = t[5]; S.ms_downward = t[6];
+  return a.type == cudaMemoryTypeHost;
+}
+
+// the captured sequence; ctx->stream is the capture stream
+static void graph_issue(tc_ctx* ctx, int n, const double* const* in, const unsigned char* flags, double* const* outp,
+                        int mem, bool jerk, graph_fn f) {
+  cudaStream_t st = ctx->stream;
+  const size_t N = (size_t)n;
+  long long L = 0;
+  graph_event(ctx, 0, st);
+  const double *dx = in[0], *dy = in[1], *dz = in[2], *dm = in[3], *dvx = in[4], *dvy = in[5], *dvz = in[6];
+  const uint8_t* df = flags;
+  if (mem == TC_MEM_HOST) {
+    double* s = ctx->in_d.p;
+    for (int a = 0; a < 7; a++)
+      if (in[a]) cudaMemcpyAsync(s + a * N, in[a], N * sizeof(double), cudaMemcpyHostToDevice, st);
+    dx = s; dy = s + N; dz = s + 2 * N; dm = s + 3 * N;
+    dvx = in[4] ? s + 4 * N : nullptr; dvy = in[5] ? s + 5 * N : nullptr; dvz = in[6] ? s + 6 * N : nullptr;
+    if (flags) {
+      cudaMemcpyAsync(ctx->in_f.p, flags, N, cudaMemcpyHostToDevice, st);
+      df = ctx->in_f.p;
+    }
   }
-  if (herr & TC_EBIT_TIMEOUT) {
-    ctx->err = "a device-side wait of the tensor-core far field gave up";
-    return TC_ERR_TIMEOUT;
+  cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st);
+  TcBodies b = bodies_view(ctx, n, jerk);
+  const int nb = 148 * 4;
+  k_bounds_partial<<<nb, 256, 0, st>>>(n, dx, dy, dz, dm, ctx->bpart.p, ctx->d_err);
+  k_bounds_final<<<1, 1, 0, st>>>(nb, ctx->bpart.p, ctx->d_root, ctx->prm.use_shift, ctx->prm.shift_u[0],
+                                  ctx->prm.shift_u[1], ctx->prm.shift_u[2]);
+  k_morton<<<nblocks(n, 256), 256, 0, st>>>(n, dx, dy, dz, ctx->d_root, ctx->keys.p, ctx->vals.p);
+  L += 4 + radix_sort(ctx->keys.p, ctx->vals.p, ctx->keys_alt.p, ctx->vals_alt.p, n, 63, ctx->hist.p, st);
+  k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->vals.p, dx, dy, dz, dm, dvx, dvy, dvz, df, b);
+  graph_check(ctx, "inputs and Morton sort");
+  f(ctx, n);
+  graph_check(ctx, "FMM");
+  TcOut o = out_view(ctx, n, jerk);
+  const int nt = ctx->gjudge_nt;
+  if (nt > 0) {
+    const int nchunk = std::max(1, std::min(4 * ctx->nsm, n / 1024));
+    double* part = ctx->judge_out.p + 7 * (size_t)nt;
+    k_direct_targets<false><<<dim3(nchunk, (nt + kJudgeTile - 1) / kJudgeTile), kJudgeTile, 0, st>>>(
+        n, nt, nchunk, ctx->judge_idx.p, b, part);
+    k_direct_targets_sum<<<nblocks(nt, 128), 128, 0, st>>>(nt, nchunk, ctx->judge_idx.p, part, o, ctx->judge_out.p);
+    cudaMemcpyAsync(ctx->hjudge, ctx->judge_out.p, 7 * (size_t)nt * sizeof(double), cudaMemcpyDeviceToHost, st);
+    L += 2;
   }
-  if ((herr | ctx->tree_flags) & TC_EBIT_NAN) return TC_ERR_NAN_INPUT;
-  if ((herr | ctx->tree_flags) & TC_EBIT_DEPTH) return TC_ERR_DEPTH;
+  double *opot = outp[3], *oax = outp[0], *oay = outp[1], *oaz = outp[2], *ojx = outp[4], *ojy = outp[5],
+         *ojz = outp[6];
+  if (mem == TC_MEM_HOST) {
+    double* s = ctx->out_d.p;
+    opot = s; oax = s + N; oay = s + 2 * N; oaz = s + 3 * N;
+    ojx = outp[4] ? s + 4 * N : nullptr; ojy = outp[4] ? s + 5 * N : nullptr; ojz = outp[4] ? s + 6 * N : nullptr;
+  }
+  k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, o, opot, oax, oay, oaz, ojx, ojy, ojz);
+  L += 1;
+  graph_event(ctx, 7, st);
+  if (mem == TC_MEM_HOST) {
+    double* s = ctx->out_d.p;
+    double* dst[7] = {outp[3], outp[0], outp[1], outp[2], outp[4], outp[5], outp[6]};
+    for (int a = 0; a < 7; a++)
+      if (dst[a] && (a < 4 || outp[4])) cudaMemcpyAsync(dst[a], s + a * N, N * sizeof(double), cudaMemcpyDeviceToHost, st);
+  }
+  TcGraphStatus* h = ctx->hstat;
+  cudaMemcpyAsync(&h->err, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(h->small, ctx->d_small, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&h->lv, ctx->d_lv, sizeof(TcLevels), cudaMemcpyDeviceToHost, st);
+  cudaMemcpyAsync(&h->cnt, ctx->d_cnt, sizeof(TcTravCounters), cudaMemcpyDeviceToHost, st);
+  graph_check(ctx, "judge, outputs and status");
+  ctx->glaunches += L;
+}
+
+// after a successful normal evaluation of the same call: plan capacities and capture
+static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* const* in, const unsigned char* flags,
+                       double* const* outp, int mem, bool jerk) {
+  graph_drop(ctx);
+  if (ctx->direct || ctx->prm.selector > 0 || ctx->prm.precision == TC_PREC_MIXED_M2L) return;
+  graph_fn f = pick_graph(ctx->prm.p, jerk);
+  if (!f) return;
+  if (mem == TC_MEM_HOST) {
+    for (int a = 0; a < 7; a++)
+      if (!host_pinned(in[a]) || !host_pinned(outp[a])) return;  // pageable memory cannot be captured
+    if (!host_pinned(flags)) return;
+  }
+  const int NT = TC_NTERM(ctx->prm.p);
+  const size_t N = (size_t)n;
+  // capacities: 25 % over this evaluation
+  size_t ccap = std::max(ctx->ccap, (size_t)(ctx->ncell * 1.25) + 1024);
+  if (ccap > 2 * N + 1024) ccap = std::max(ctx->ccap, 2 * N + 1024);
+  if (ctx->cint.ensure(6 * ccap) || ctx->cdbl.ensure(7 * ccap) || ctx->csink.ensure(ccap) ||
+      ctx->split_off.ensure(8 * ccap))
+    return;
+  ctx->ccap = ccap;
+  size_t mcap = std::max(ctx->mcap, (size_t)(ctx->n_m2l * 1.25) + 4096);
+  size_t pcap = std::max(ctx->pcap, (size_t)(ctx->n_p2p * 1.25) + 4096);
+  size_t fcap = (size_t)(ctx->fcap * 1.25) + 4096;
+  if (ctx->m2l.ensure(mcap) || ctx->p2p.ensure(pcap) || ctx->front[0].ensure(fcap) || ctx->front[1].ensure(fcap)) return;
+  ctx->mcap = ctx->m2l.n;
+  ctx->pcap = ctx->p2p.n;
+  ctx->fcap = std::min(ctx->front[0].n, ctx->front[1].n);
+  size_t mx = std::max(std::max(ctx->mcap, ctx->pcap), N);
+  if (ctx->m2l_alt.ensure(ctx->mcap + 1) || ctx->p2p_alt.ensure(ctx->pcap + 1) ||
+      ctx->hist.ensure(257 * ((mx + kRsTile - 1) / kRsTile + 1) + 1024) || ctx->m2l_start.ensure(ccap + 1) ||
+      ctx->p2p_start.ensure(ccap + 1) || ctx->m2l_src.ensure(ctx->mcap + 1) || ctx->p2p_src.ensure(ctx->pcap + 1) ||
+      ctx->m2l_tl.ensure(ccap) || ctx->p2p_tl.ensure(ccap) || ctx->leaves.ensure(ccap) ||
+      ctx->expn.ensure(ccap * NT * (jerk ? 4 : 2)) || ctx->bpart.ensure(6 * 148 * 4))
+    return;
+  int sb = 1;
+  while (((size_t)1 << sb) < ccap) sb++;
+  ctx->gsbits = sb;
+  // judge targets (the same seeded bodies as the normal path's judge)
+  ctx->gjudge_nt = 0;
+  if (ctx->prm.judge_n > 0) {
+    const int nt = std::min(ctx->prm.judge_n, n);
+    std::vector<int> idx(nt);
+    std::mt19937_64 rng(ctx->prm.judge_seed);
+    std::uniform_int_distribution<int> U(0, n - 1);
+    for (int k = 0; k < nt; k++) idx[k] = U(rng);
+    const int nchunk = std::max(1, std::min(4 * ctx->nsm, n / 1024));
+    if (ctx->judge_idx.ensure(nt) || ctx->judge_out.ensure(7 * (size_t)nt + 8 * (size_t)nt * nchunk)) return;
+    if (cudaMemcpy(ctx->judge_idx.p, idx.data(), nt * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess) return;
+    if (ctx->hjudge_cap < 7 * (size_t)nt) {
+      if (ctx->hjudge) cudaFreeHost(ctx->hjudge);
+      ctx->hjudge = nullptr;
+      ctx->hjudge_cap = 0;
+      if (cudaMallocHost((void**)&ctx->hjudge, 7 * (size_t)nt * sizeof(double)) != cudaSuccess) return;
+      ctx->hjudge_cap = 7 * (size_t)nt;
+    }
+    ctx->gjudge_nt = nt;
+  }
+  if (!ctx->hstat && cudaMallocHost((void**)&ctx->hstat, sizeof(TcGraphStatus)) != cudaSuccess) {
+    ctx->hstat = nullptr;
+    return;
+  }
+  if (!ctx->gstream && cudaStreamCreateWithFlags(&ctx->gstream, cudaStreamNonBlocking) != cudaSuccess) {
+    ctx->gstream = nullptr;
+    return;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return;
+  // capture
+  cudaStream_t saved = ctx->stream;
+  const size_t saved_stride = ctx->expn_stride;
+  ctx->stream = ctx->gstream;
+  ctx->expn_stride = ccap;
+  ctx->glaunches = 0;
+  ctx->gfail.clear();
+  cudaGraph_t g = nullptr;
+  cudaGetLastError();
+  cudaError_t e = cudaStreamBeginCapture(ctx->gstream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    graph_issue(ctx, n, in, flags, outp, mem, jerk, f);
+    e = cudaStreamEndCapture(ctx->gstream, &g);
+  } else {
+    ctx->gfail = std::string("begin capture: ") + cudaGetErrorString(e);
+  }
+  ctx->stream = saved;
+  ctx->expn_stride = saved_stride;
+  if (e != cudaSuccess || !g || !ctx->gfail.empty()) {
+    if (ctx->gfail.empty()) ctx->gfail = std::string("end capture: ") + cudaGetErrorString(e);
+    cudaGetLastError();
+    if (g) cudaGraphDestroy(g);
+    return;
+  }
+  if (cudaGraphInstantiate(&ctx->gexec, g, 0) != cudaSuccess) {
+    cudaGetLastError();
+    cudaGraphDestroy(g);
+    ctx->gexec = nullptr;
+    return;
+  }
+  ctx->graph = g;
+  ctx->gkey = key;
+  ctx->gvalid = true;
+  graph_check(ctx, "instantiate");
+  if (!ctx->gfail.empty()) graph_drop(ctx);
+}
+
+static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
+                                const double* vx, const double* vy, const double* vz, const double* m,
+                                const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                                double* jx, double* jy, double* jz, int mem) {
+  TcGraphKey key;
+  key.n = n;
+  key.mem = mem;
+  const void* ptrs[15] = {x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz};
+  for (int i = 0; i < 15; i++) key.ptr[i] = ptrs[i];
+  key.prm = ctx->prm;
+  const bool jerk = ctx->prm.variant == TC_VARIANT_JERKS;
+  if (ctx->gvalid && graph_key_equal(key, ctx->gkey)) {
+    TC_CK(cudaSetDevice(ctx->prm.device));
+    TC_CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
+    TC_CK(cudaStreamSynchronize(ctx->stream));
+    const TcGraphStatus& h = *ctx->hstat;
+    const unsigned cap_bits = TC_EBIT_CELL_CAP | TC_EBIT_M2L_CAP | TC_EBIT_P2P_CAP | TC_EBIT_FRONTIER_CAP;
+    if (!(h.err & cap_bits)) {
+      ctx->n = n;
+      ctx->direct = 0;
+      ctx->ncell = h.lv.ncell;
+      ctx->nleaf = (int)h.small[2];
+      ctx->n_m2l = h.cnt.n_m2l;
+      ctx->n_p2p = h.cnt.n_p2p;
+      ctx->n_inter = h.cnt.frontier[0];
+      ctx->lv = h.lv;
+      int maxl = 0;
+      for (int l = 0; l <= TC_MAX_LEVEL; l++)
+        if (h.lv.count[l] > 0) maxl = l;
+      ctx->max_level = maxl;
+      ctx->sbits = ctx->gsbits;
+      ctx->expn_stride = ctx->ccap;
+      ctx->launches = ctx->glaunches;
+      ctx->tree_flags = 0;
+      ctx->n_classes = 1;
+      ctx->class_order[0] = ctx->prm.p;
+      ctx->class_pairs[0] = (long long)ctx->n_m2l;
+      ctx->flop_frac = 1.0;
+      ctx->judge_redo = 0;
+      ctx->judge_rms = 0.0;
+      if (ctx->gjudge_nt > 0) {
+        double sacc = 0.0;
+        for (int k = 0; k < ctx->gjudge_nt; k++) {
+          const double* r = ctx->hjudge + 7 * (size_t)k;
+          double ex = r[4] - r[1], ey = r[5] - r[2], ez = r[6] - r[3];
+          double an = r[1] * r[1] + r[2] * r[2] + r[3] * r[3];
+          sacc += (ex * ex + ey * ey + ez * ez) / (an > 0 ? an : 1.0);
+        }
+        ctx->judge_rms = sqrt(sacc / ctx->gjudge_nt);
+      }
+      return finish_stats(ctx, n, h.err);
+    }
+    ctx->gvalid = false;  // a capacity overflowed: re-run on the normal path and re-plan
+  }
+  tc_status rs = evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, mem, nullptr);
+  if (rs == TC_OK) {
+    const double* in[7] = {x, y, z, m, vx, vy, vz};
+    double* outp[7] = {ax, ay, az, pot, jx, jy, jz};
+    graph_plan(ctx, n, key, in, flags, outp, mem, jerk);
+  }
+  return rs;
+}
+
+tc_status tc_set_graph(tc_ctx* ctx, int on) {
+  if (!ctx) return TC_ERR_ARG;
+  cudaSetDevice(ctx->prm.device);
+  ctx->graph_on = on != 0;
+  if (!ctx->graph_on) graph_drop(ctx);
   return TC_OK;
 }
+
+int tc_graph_ready(const tc_ctx* ctx) { return ctx && ctx->gvalid ? 1 : 0; }
+
+const char* tc_graph_note(const tc_ctx* ctx) { return ctx ? ctx->gfail.c_str() : ""; }
 
 tc_status tc_direct_sums(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
                          const double* vy, const double* vz, const double* m, const unsigned char* flags, int nt,

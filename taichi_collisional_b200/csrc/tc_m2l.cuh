@@ -390,11 +390,14 @@ constexpr int tc_m2l_threads() { return 128 * TcM2LGroups<Q>::G; }
 
 // M2L of order Q <= P over a per-target list; expansions are stored with order P.  Adds
 // into L (zeroed before the first M2L launch of an evaluation).  One CTA per SM (shared
-// memory), which owns the tensor memory it allocates.
+// memory), which owns the tensor memory it allocates.  One target per CTA, or, with `next`
+// (a counter zeroed before the launch), a persistent grid whose CTAs take targets in turn.
 template <int P, int Q, bool JERK>
 __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __restrict__ tlist, int ntl,
                                                                const int* __restrict__ tstart,
-                                                               const int* __restrict__ src, TcCells c) {
+                                                               const int* __restrict__ src, TcCells c,
+                                                               const unsigned* ntldev = nullptr,
+                                                               unsigned* next = nullptr) {
   using SM = TcM2LSmem<Q>;
   using TM = TcM2LTmem<Q>;
   constexpr int NTQ = SM::NT, NTP = (P + 1) * (P + 1);
@@ -402,10 +405,16 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
   constexpr bool QUIRK = Q == P;
   extern __shared__ double tc_m2l_smem[];
   __shared__ uint32_t s_tmem;
+  __shared__ int s_ti;
   int ti = blockIdx.x;
+  if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
+  if (next) {
+    if (threadIdx.x == 0) s_ti = (int)atomicAdd(next, 1u);
+    __syncthreads();
+    ti = s_ti;
+  }
   if (ti >= ntl) return;
-  int t = tlist[ti];
-  if (!c.has_sink[t]) return;
+  if (!next && !c.has_sink[tlist[ti]]) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int grp = warp >> 2, w = warp & 3, acol = grp * 32 + lane;
   if (warp == 0) {
@@ -421,9 +430,11 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
   // this warp's columns in its lane quarter
   const uint32_t twarp = s_tmem + ((uint32_t)(32 * w) << 16) + (uint32_t)(grp * TM::CW);
   double* buf = tc_m2l_smem + SM::BUF + grp * NTQ * 32;
+  for (;;) {
+  const int t = tlist[ti];
   const int s_beg = tstart[t], s_end = tstart[t + 1];
   const double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
-  for (int arr = 0; arr < (JERK ? 2 : 1); arr++) {
+  for (int arr = 0; arr < (c.has_sink[t] ? (JERK ? 2 : 1) : 0); arr++) {
     const double* Mbase = arr ? c.Md : c.M;
     tc_m2l_zero_warp<Q, QUIRK>(w, twarp);
     for (int b0 = s_beg + grp * 32; b0 < s_end; b0 += 32 * G) {
@@ -452,6 +463,13 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
       if (lane == 0) Lt[r] += v;
     }
     tc_bar_cta();
+  }
+  if (!next) break;
+  if (threadIdx.x == 0) s_ti = (int)atomicAdd(next, 1u);
+  tc_bar_cta();
+  ti = s_ti;
+  tc_bar_cta();
+  if (ti >= ntl) break;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   tc_bar_cta();

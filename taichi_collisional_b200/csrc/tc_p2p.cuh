@@ -78,7 +78,9 @@ constexpr int kP2PWarps = 4;
 template <bool JERK>
 __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p(const int* __restrict__ tlist, int ntl,
                                                         const int* __restrict__ tstart, const int* __restrict__ src,
-                                                        const TcBodies b, const TcCells c, TcOut out) {
+                                                        const TcBodies b, const TcCells c, TcOut out,
+    const unsigned* ntldev = nullptr) {
+  if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
     int t = tlist[k];
@@ -405,7 +407,9 @@ template <bool JERK>
 __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
                                                               const int* __restrict__ tstart,
                                                               const int* __restrict__ src, const TcBodies b,
-                                                              const TcCells c, TcOut out) {
+                                                              const TcCells c, TcOut out,
+    const unsigned* ntldev = nullptr) {
+  if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
   // per warp source tile, three 16-byte vectors per source (one broadcast load each):
   // (xh, yh, xl, yl) (zh, zl, mh, ml) (vx, vy, vz, -); x and y are consumed as packed pairs
   __shared__ float4 tile[kP2PWarps][32][3];

@@ -108,8 +108,12 @@ __global__ void k_trav_step(int s, const int2* __restrict__ fin, int2* __restric
 }
 
 // (target << sbits | source) keys, sorted: per-target CSR offsets (targets in [0, ncell))
+// (ndev, ncdev optional: counts on the device for device-sized launches; n is then the capacity)
 __global__ void k_list_csr(const unsigned long long* __restrict__ keys, unsigned long long n, int ncell, int sbits,
-                           int* __restrict__ tgt_start, int* __restrict__ src) {
+                           int* __restrict__ tgt_start, int* __restrict__ src,
+                           const unsigned long long* ndev = nullptr, const int* ncdev = nullptr) {
+  if (ndev && *ndev < n) n = *ndev;
+  if (ncdev) ncell = *ncdev;
   const unsigned long long smask = (1ull << sbits) - 1ull;
   for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (unsigned long long)gridDim.x * blockDim.x) {
@@ -127,7 +131,8 @@ __global__ void k_list_csr(const unsigned long long* __restrict__ keys, unsigned
 
 // compact list of targets that have at least one entry
 __global__ void k_list_targets(const int* __restrict__ tgt_start, int ncell, int* __restrict__ tlist,
-                               unsigned int* __restrict__ ntl) {
+                               unsigned int* __restrict__ ntl, const int* ncdev = nullptr) {
+  if (ncdev) ncell = *ncdev;
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool has = i < ncell && tgt_start[i + 1] > tgt_start[i];
   unsigned mask = __ballot_sync(0xffffffffu, has);

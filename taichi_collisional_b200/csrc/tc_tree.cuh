@@ -107,12 +107,19 @@ __global__ void k_morton(int n, const double* __restrict__ x, const double* __re
 // Stable LSD radix sort, 8 bits per pass: per-tile digit histograms, one exclusive scan in
 // (digit, tile) order, then a stable scatter (ranks from warp match + per-warp counts).
 // ---------------------------------------------------------------------------------------
-__global__ void k_rs_hist(const unsigned long long* __restrict__ keys, int n, int shift, uint32_t* __restrict__ hist) {
+// ndev (optional): the key count on the device (device-sized launches); n is then the capacity
+__global__ void k_rs_hist(const unsigned long long* __restrict__ keys, int n, int shift, uint32_t* __restrict__ hist,
+                          const unsigned long long* ndev = nullptr) {
   __shared__ uint32_t h[256];
+  if (ndev && *ndev < (unsigned long long)n) n = (int)*ndev;
   int t = threadIdx.x;
+  int base = blockIdx.x * kRsTile;
+  if (base >= n) {  // a tile past the keys (device-sized launch): an empty histogram
+    hist[t * gridDim.x + blockIdx.x] = 0u;
+    return;
+  }
   h[t] = 0;
   __syncthreads();
-  int base = blockIdx.x * kRsTile;
 #pragma unroll
   for (int r = 0; r < kRsItems; r++) {
     int idx = base + r * kRsThreads + t;
@@ -198,8 +205,11 @@ inline int excl_scan(uint32_t* a, int total, uint32_t* sums, cudaStream_t st) {
 template <bool kVals>
 __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long long* __restrict__ kin, const int* __restrict__ vin,
                                                            unsigned long long* __restrict__ kout, int* __restrict__ vout, int n,
-                                                           int shift, const uint32_t* __restrict__ hist) {
+                                                           int shift, const uint32_t* __restrict__ hist,
+                                                           const unsigned long long* ndev = nullptr) {
   __shared__ uint32_t s_base[256];
+  if (ndev && *ndev < (unsigned long long)n) n = (int)*ndev;
+  if ((long long)blockIdx.x * kRsTile >= n) return;  // a tile past the keys: nothing to move
   __shared__ uint32_t s_wcnt[kRsThreads / 32][257];
   int t = threadIdx.x, w = t >> 5, lane = t & 31;
   s_base[t] = hist[t * gridDim.x + blockIdx.x];
@@ -231,9 +241,13 @@ __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long l
 }
 
 // Sorts (keys, vals) by key bits [0, bits).  Uses alt buffers; the result ends in keys/vals.
+// Device-sized form (ndev given, n = capacity): no copy back; *kfinal receives the buffer that
+// holds the sorted keys.
 inline int radix_sort(unsigned long long* keys, int* vals, unsigned long long* keys_alt, int* vals_alt, int n, int bits, uint32_t* hist,
-                      cudaStream_t st, int begin_bit = 0) {
-  if (n <= 1) return 0;
+                      cudaStream_t st, int begin_bit = 0, const unsigned long long* ndev = nullptr,
+                      unsigned long long** kfinal = nullptr) {
+  if (kfinal) *kfinal = keys;
+  if (n <= 1 && !ndev) return 0;
   int launches = 0;
   int nblk = (n + kRsTile - 1) / kRsTile;
   int passes = (bits - begin_bit + 7) / 8;
@@ -241,14 +255,18 @@ inline int radix_sort(unsigned long long* keys, int* vals, unsigned long long* k
   int *va = vals, *vb = vals_alt;
   for (int p = 0; p < passes; p++) {
     int shift = begin_bit + 8 * p;
-    k_rs_hist<<<nblk, kRsThreads, 0, st>>>(ka, n, shift, hist);
+    k_rs_hist<<<nblk, kRsThreads, 0, st>>>(ka, n, shift, hist, ndev);
     launches += 2 + excl_scan(hist, 256 * nblk, hist + 256 * (size_t)nblk, st);
     if (vals)
-      k_rs_scatter<true><<<nblk, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, hist);
+      k_rs_scatter<true><<<nblk, kRsThreads, 0, st>>>(ka, va, kb, vb, n, shift, hist, ndev);
     else
-      k_rs_scatter<false><<<nblk, kRsThreads, 0, st>>>(ka, nullptr, kb, nullptr, n, shift, hist);
+      k_rs_scatter<false><<<nblk, kRsThreads, 0, st>>>(ka, nullptr, kb, nullptr, n, shift, hist, ndev);
     unsigned long long* tk = ka; ka = kb; kb = tk;
     int* tv = va; va = vb; vb = tv;
+  }
+  if (kfinal) {
+    *kfinal = ka;
+    return launches;
   }
   if (ka != keys) {
     cudaMemcpyAsync(keys, ka, sizeof(unsigned long long) * n, cudaMemcpyDeviceToDevice, st);
@@ -347,14 +365,22 @@ __global__ void k_tree_scan(int l, TcCells c, TcLevels* lv, int cell_cap, unsign
   }
   int next = st + cnt;
   int run = s[t] - loc;
+  // over capacity: the level's cells stay leaves, so the (flagged) tree remains consistent for
+  // launches that follow without a host check (a captured graph)
+  const bool over = next + s[T - 1] > cell_cap;
   for (int i = b; i < e; i++) {
     int nc = c.nchild[st + i];
+    if (over) {
+      c.nchild[st + i] = 0;
+      c.child[st + i] = -1;
+      continue;
+    }
     c.child[st + i] = nc ? next + run : -1;
     run += nc;
   }
   if (t == T - 1) {
     int total = s[t];
-    if (next + total > cell_cap) {
+    if (over) {
       tc_set_err(err, TC_EBIT_CELL_CAP);
       total = 0;
     }

@@ -265,7 +265,8 @@ constexpr int kP2MWarps = 4;
 #endif
 
 template <int P, bool JERK>
-__global__ void __launch_bounds__(kP2MWarps * 32, JERK ? TC_P2M_JERK_BLOCKS : 4) k_p2m_leaves(int ncell, const TcBodies b, TcCells c) {
+__global__ void __launch_bounds__(kP2MWarps * 32, JERK ? TC_P2M_JERK_BLOCKS : 4) k_p2m_leaves(int ncell, const TcBodies b, TcCells c,
+                                                                                      const TcLevels* lvd = nullptr) {
   constexpr int NT = (P + 1) * (P + 1);
   constexpr int LW = (P + 1 <= 16) ? 16 : 32;  // lanes per body
   constexpr int NH = 32 / LW;                  // bodies per pass
@@ -273,6 +274,7 @@ __global__ void __launch_bounds__(kP2MWarps * 32, JERK ? TC_P2M_JERK_BLOCKS : 4)
   __shared__ double sbod[kP2MWarps][32][9];    // dx dy dz q vx vy vz (row padded to 9)
   tab.fill();
   __syncthreads();
+  if (lvd) ncell = lvd->ncell;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int a = lane % LW, h = lane / LW;
   // columns a-1, a, a+1 (column -1 is -conj(column 1), so a = 0 runs column 1 twice)
@@ -516,9 +518,10 @@ __device__ void tc_cell_ball(int ci, const TcBodies& b, TcCells& c, const double
 
 // balls of every leaf (they depend on the leaf's own bodies only)
 __global__ void __launch_bounds__(kUpWarps * 32) k_leaf_balls(int ncell, const TcBodies b, TcCells c,
-                                                              unsigned int* err) {
+                                                              unsigned int* err, const TcLevels* lvd = nullptr) {
   __shared__ double s_td[193];
   tc_load_tdesign(s_td);
+  if (lvd) ncell = lvd->ncell;  // device-sized launch (graph): the cell count of this tree
   int w = threadIdx.x >> 5;
   for (int ci = blockIdx.x * kUpWarps + w; ci < ncell; ci += gridDim.x * kUpWarps)
     if (c.nchild[ci] == 0) tc_cell_ball(ci, b, c, s_td, err);

@@ -100,6 +100,20 @@ tc_status tc_destroy(tc_ctx* ctx);
 /* Run work on this CUDA stream (cudaStream_t passed as void*; NULL = legacy default). */
 tc_status tc_set_stream(tc_ctx* ctx, void* stream);
 
+/* The top tree's own traversal: the error-controlled MAC of horizontalPassHigh
+ * (traverse_eager.h:61-148), which get_force_and_potential uses (integrator.h:459-562:
+ * horizontalPass(cells, cells, 1, get_steps)), preceded by the reference's low-order pre-pass
+ * (integrator.h:476-493, kernel_fast_lean.h:1358-1647) that estimates each body's acceleration
+ * (acc_old) for the cells' min_acc.  force_accuracy is the reference's global (exafmm.h:95,
+ * default 2e-7).  With on != 0, tc_evaluate and tc_evaluate_steps of this context build their
+ * lists with it instead of the theta MAC.  The top tree only (TC_ERR_UNSUPPORTED for the jerks
+ * tree, whose traversal is theta only); not captured by tc_set_graph.  As the reference's
+ * first call: acc_old starts at zero every evaluation (the reference's global body array
+ * carries it from call to call). */
+tc_status tc_set_error_mac(tc_ctx* ctx, int on, double force_accuracy);
+/* The pre-pass's acc_old of the last evaluation with the error MAC, per body (caller order, host). */
+tc_status tc_get_acc_old(tc_ctx* ctx, double* acc_old);
+
 /* The whole evaluation as one CUDA graph (SURVEY's boundary call (B) as a graph; no counterpart
  * in the reference, which has no device).  With on != 0, tc_evaluate replays a captured graph
  * when the call matches the one it was captured for (same n, memory kind, every input/output

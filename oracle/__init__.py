@@ -209,6 +209,11 @@ def ref_lib(variant, p):
         L.tcr_list.argtypes = [C.c_int, _ip, _ip]
         L.tcr_list.restype = C.c_longlong
         L.tcr_shift_uniforms.argtypes = [C.c_long, _dp]
+        if hasattr(L, "tcr_evaluate_high"):
+            L.tcr_evaluate_high.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_int] + [_dp] * 4
+            L.tcr_evaluate_high.restype = C.c_int
+            L.tcr_acc_old.argtypes = [_dp]
+            L.tcr_min_acc.argtypes = [_dp, _dp]
         if hasattr(L, "tcr_evaluate_steps"):
             L.tcr_evaluate_steps.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_double,
                                                                      C.c_int] + [_dp] * 5
@@ -253,6 +258,27 @@ def ref_evaluate_steps(x, y, z, m, vx, vy, vz, *, p, theta, ncrit, dt_param, nth
                               None if fl is None else fl.ctypes.data_as(_u8p), theta, ncrit, dt_param, nthreads,
                               *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "timestep")])
     out["ncell"] = nc
+    return out
+
+
+def ref_evaluate_high(x, y, z, m, *, p, ncrit, force_accuracy, nthreads=1, flags=None):
+    """The top tree's own get_force_and_potential (integrator.h:459-562): low-order pre-pass,
+    then the error-controlled MAC.  Also returns the pre-pass's per-body acc_old (caller order)
+    and the per-cell min_acc and Pn of the reference's cells."""
+    L = ref_lib(VARIANT_TOP, p)
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot")}
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    nc = L.tcr_evaluate_high(n, _d(x), _d(y), _d(z), None, None, None, _d(m),
+                             None if fl is None else fl.ctypes.data_as(_u8p), force_accuracy, ncrit, nthreads,
+                             *[_d(out[k]) for k in ("ax", "ay", "az", "pot")])
+    out["ncell"] = nc
+    out["acc_old"] = np.zeros(n)
+    L.tcr_acc_old(_d(out["acc_old"]))
+    out["min_acc"] = np.zeros(nc)
+    out["pn"] = np.zeros((nc, p + 1))
+    L.tcr_min_acc(_d(out["min_acc"]), _d(out["pn"]))
     return out
 
 

@@ -31,6 +31,7 @@ static const int kJerks = 0;
 static Cells g_cells;
 static std::vector<int> g_list_t[2], g_list_s[2];
 static int g_init = 0;
+static int g_high = 0;  // last evaluation used the error-controlled MAC (top tree)
 
 static double now_s() {
   struct timeval tv;
@@ -62,10 +63,51 @@ static void record(Cell* Ci, Cell* Cj) {
   }
 }
 
+#ifndef TCR_JERKS
+// same decisions as horizontalPassHigh (traverse_eager.h:61-148) on the reference's own cells
+// (Pn, min_acc, R, X after its upwardPass), for recording the error-MAC lists
+static void record_high(Cell* Ci, Cell* Cj) {
+  real_t d[3];
+  for (int k = 0; k < 3; k++) d[k] = Ci->X[k] - Cj->X[k];
+  real_t R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  real_t f1 = 10, f2 = 10;
+  real_t Ra = Ci->R, Rb = Cj->R, Ra_p_Rb = Ra + Rb;
+  if (R2 > Ra_p_Rb * Ra_p_Rb) {
+    real_t R = sqrt(R2), Rp = R2, pa = 1, pb = 1, Eba = 0, Eab = 0;
+    for (int k = 0; k <= P; k++) {
+      real_t fac = combinator_coef[P][k];
+      Eab += Ci->Pn[P - k] * pb * fac;
+      Eba += Cj->Pn[P - k] * pa * fac;
+      pa *= Ra;
+      pb *= Rb;
+      Rp *= R;
+    }
+    real_t fac = 8 * fmax(Ra, Rb) / Ra_p_Rb / Rp;
+    Eab *= fac;
+    f1 = Eab / (force_accuracy * Cj->min_acc);
+    Eba *= fac;
+    f2 = Eba / (force_accuracy * Ci->min_acc);
+  }
+  int ci = (int)(Ci - &g_cells[0]), cj = (int)(Cj - &g_cells[0]);
+  if (f2 < 1 && f1 < 1) {
+    int k = ((Ci->NBODY <= 2 && Cj->NBODY <= 8) || (Cj->NBODY <= 2 && Ci->NBODY <= 8)) ? 1 : 0;
+    g_list_t[k].push_back(ci);
+    g_list_s[k].push_back(cj);
+  } else if (Ci->NCHILD == 0 && Cj->NCHILD == 0) {
+    g_list_t[1].push_back(ci);
+    g_list_s[1].push_back(cj);
+  } else if (Cj->NCHILD == 0 || (Ci->R >= Cj->R && Ci->NCHILD != 0)) {
+    for (Cell* c = Ci->CHILD; c != Ci->CHILD + Ci->NCHILD; c++) record_high(c, Cj);
+  } else {
+    for (Cell* c = Cj->CHILD; c != Cj->CHILD + Cj->NCHILD; c++) record_high(Ci, c);
+  }
+}
+#endif
+
 static int run(int n, const double* x, const double* y, const double* z, const double* vx, const double* vy,
                const double* vz, const double* m, const unsigned char* flags, double th, int nc, long seed,
                int nthreads, double* ax, double* ay, double* az, double* pot, double* jx, double* jy,
-               double* jz, double* times, bool get_steps, double* timestep);
+               double* jz, double* times, bool get_steps, double* timestep, bool high = false);
 
 extern "C" {
 
@@ -101,12 +143,24 @@ int tcr_evaluate_steps(int n, const double* x, const double* y, const double* z,
              true, timestep);
 }
 
+#ifndef TCR_JERKS
+// The top tree's own get_force_and_potential (integrator.h:459-562): low-order pre-pass
+// (acc_old), then the error-controlled MAC (horizontalPass(cells, cells, 1, get_steps)) with
+// force_accuracy (exafmm.h:95, the global).  Same outputs as tcr_evaluate.
+int tcr_evaluate_high(int n, const double* x, const double* y, const double* z, const double* vx,
+                      const double* vy, const double* vz, const double* m, const unsigned char* flags,
+                      double fa, int nc, int nthreads, double* ax, double* ay, double* az, double* pot) {
+  force_accuracy = fa;
+  return run(n, x, y, z, vx, vy, vz, m, flags, 0.4, nc, 0, nthreads, ax, ay, az, pot, nullptr, nullptr, nullptr,
+             nullptr, false, nullptr, true);
+}
+#endif
 }  // extern "C"
 
 static int run(int n, const double* x, const double* y, const double* z, const double* vx, const double* vy,
                const double* vz, const double* m, const unsigned char* flags, double th, int nc, long seed,
                int nthreads, double* ax, double* ay, double* az, double* pot, double* jx, double* jy,
-               double* jz, double* times, bool get_steps, double* timestep) {
+               double* jz, double* times, bool get_steps, double* timestep, bool high) {
   if (!g_init) {
     P = EXPANSION;
     initKernel();
@@ -137,10 +191,44 @@ static int run(int n, const double* x, const double* y, const double* z, const d
   double t0 = now_s();
   g_cells = buildTree(bodies);
   double t1 = now_s();
-  for (size_t c = 0; c < g_cells.size(); c++) g_cells[c].has_sink = false;
-  upwardPass(g_cells);
+  g_high = 0;
+#ifndef TCR_JERKS
+  if (high) {
+    // integrator.h:476-539, in order
+    g_high = 1;
+    upwardPass_low(g_cells);
+    horizontalPass_low(g_cells, g_cells);
+    downwardPass_low(g_cells);
+    for (size_t b = 0; b < bodies.size(); b++) {
+      bodies[b].F[0] = bodies[b].F[1] = bodies[b].F[2] = 0;
+      bodies[b].p = 0;
+      bodies[b].timestep = 0;
+    }
+    for (size_t i = 0; i < g_cells.size(); i++)
+      for (int term = 0; term < NTERM; term++) {
+        g_cells[i].L[term] = 0;
+        g_cells[i].M[term] = 0;
+        g_cells[i].min_acc = HUGE;
+        g_cells[i].has_sink = false;
+      }
+    upwardPass(g_cells);
+    for (size_t i = 0; i < g_cells.size(); i++)
+      for (int nn = 0; nn <= P; nn++) {
+        for (int mm = -nn; mm <= nn; mm++) {
+          int index = nn * nn + nn + mm;
+          g_cells[i].Pn[nn] += g_cells[i].M[index] * g_cells[i].M[index] * factorial_table[nn + mm] *
+                               factorial_table[nn - mm];
+        }
+        g_cells[i].Pn[nn] = sqrt(g_cells[i].Pn[nn]);
+      }
+  } else
+#endif
+  {
+    for (size_t c = 0; c < g_cells.size(); c++) g_cells[c].has_sink = false;
+    upwardPass(g_cells);
+  }
   double t2 = now_s();
-  horizontalPass(g_cells, g_cells, 0, get_steps);
+  horizontalPass(g_cells, g_cells, high ? 1 : 0, get_steps);
   double t3 = now_s();
   downwardPass(g_cells);
   double t4 = now_s();
@@ -180,6 +268,18 @@ void tcr_cells(int* begin, int* nbody, int* nchild, int* child, double* X, doubl
     for (size_t i = 0; i < bodies.size(); i++) index[i] = bodies[i].index;
 }
 
+// per body acc_old of the last evaluation (caller order) and per cell min_acc, Pn[0..P]
+void tcr_acc_old(double* out) {
+  for (size_t b = 0; b < bodies.size(); b++) out[bodies[b].index] = bodies[b].acc_old;
+}
+void tcr_min_acc(double* out, double* pn) {
+  for (size_t c = 0; c < g_cells.size(); c++) {
+    out[c] = g_cells[c].min_acc;
+    if (pn)
+      for (int k = 0; k <= P; k++) pn[c * (P + 1) + k] = g_cells[c].Pn[k];
+  }
+}
+
 void tcr_expansions(double* M, double* L) {
   for (size_t c = 0; c < g_cells.size(); c++) {
     memcpy(M + c * NTERM, g_cells[c].M, NTERM * sizeof(double));
@@ -189,6 +289,9 @@ void tcr_expansions(double* M, double* L) {
 
 // kind 0 = M2L, 1 = P2P.  First call with tgt == NULL walks the tree and returns the count.
 long long tcr_list(int kind, int* tgt, int* src) {
+#ifndef TCR_JERKS
+  if (g_list_t[0].empty() && g_list_t[1].empty() && g_high) record_high(&g_cells[0], &g_cells[0]);
+#endif
   if (g_list_t[0].empty() && g_list_t[1].empty()) record(&g_cells[0], &g_cells[0]);
   long long n = (long long)g_list_t[kind].size();
   if (tgt) memcpy(tgt, g_list_t[kind].data(), n * sizeof(int));

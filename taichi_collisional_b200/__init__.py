@@ -59,7 +59,7 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
-           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note"]
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note", "tc_set_error_mac", "tc_get_acc_old"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -90,6 +90,10 @@ def load_library(path=LIB_PATH):
     L.tc_graph_ready.restype = C.c_int
     L.tc_graph_note.argtypes = [C.c_void_p]
     L.tc_graph_note.restype = C.c_char_p
+    L.tc_set_error_mac.argtypes = [C.c_void_p, C.c_int, C.c_double]
+    L.tc_set_error_mac.restype = C.c_int
+    L.tc_get_acc_old.argtypes = [C.c_void_p, _dp]
+    L.tc_get_acc_old.restype = C.c_int
     L.tc_evaluate.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8 + [C.c_void_p] * 7 + [C.c_int]
     L.tc_evaluate.restype = C.c_int
     L.tc_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
@@ -212,6 +216,17 @@ class Gravity:
     def graph_ready(self):
         """True when the next evaluate with the same buffers replays the captured graph."""
         return bool(self._L.tc_graph_ready(self._h))
+
+    def set_error_mac(self, on=True, force_accuracy=2.0e-7):
+        """The top tree's error-controlled MAC with the reference's low-order pre-pass
+        (tc_set_error_mac)."""
+        self._check(self._L.tc_set_error_mac(self._h, 1 if on else 0, force_accuracy), "tc_set_error_mac")
+
+    def acc_old(self):
+        """The pre-pass's per-body acceleration estimate of the last evaluation (caller order)."""
+        a = np.zeros(int(self.stats()["n_bodies"]))
+        self._check(self._L.tc_get_acc_old(self._h, a.ctypes.data_as(_dp)), "tc_get_acc_old")
+        return a
 
     def graph_note(self):
         """Why the last capture was abandoned ('' when it succeeded)."""

@@ -27,6 +27,7 @@
 #include "tc_m2l.cuh"
 #include "tc_m2l_mixed.cuh"
 #include "tc_m2l_tc.cuh"
+#include "tc_emac.cuh"
 #include "tc_down.cuh"
 #include "tc_p2p.cuh"
 #include "tc_select.cuh"
@@ -168,6 +169,11 @@ struct tc_ctx {
   long long glaunches = 0;
   int gsbits = 1;
   std::string gfail;  // why the last capture was abandoned (empty: captured)
+  // error-controlled MAC of the top tree (tc_set_error_mac) and its low-order pre-pass
+  bool emac = false;
+  double emac_fa = 2.0e-7;
+  DBuf<double> low_rgeo, low_m9, low_l9, acc_old, min_acc, pn_ref;
+  DBuf<int> cell_of;
 };
 
 static bool g_const_init[64];
@@ -675,11 +681,14 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     k_upward_level<P, JERK><<<g, TcTransW<P>::W * 32, 0, st>>>(l, b, cv, d_start, d_count, ctx->d_err);
   }
   if (ctx->events) cudaEventRecord(ctx->ev[2], st);
-  // ---- traversal
+  // ---- traversal, list sort and per-target offsets (lists of the acceptance test `mac` over the
+  // cells `cvm`: the error-MAC pre-pass runs it on the geometric cells first)
   int sbits = 1;
   while ((1 << sbits) < ctx->ncell) sbits++;
   ctx->sbits = sbits;
   double theta2 = prm.theta * prm.theta;
+  unsigned hs[4];
+  auto build_lists = [&](const TcCells& cvm, const TcMac& mac) -> tc_status {
   for (int attempt = 0; attempt < 6; attempt++) {
     size_t want_m = ctx->mcap ? ctx->mcap : (size_t)ctx->ncell * 640 + 65536;
     size_t want_p = ctx->pcap ? ctx->pcap : (size_t)ctx->ncell * 240 + 65536;
@@ -697,8 +706,8 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     ctx->launches += 1 + nsteps;
     for (int s = 0; s < nsteps; s++)
       k_trav_step<<<148 * 8, 256, 0, st>>>(s, ctx->front[s & 1].p, ctx->front[(s + 1) & 1].p, ctx->fcap, ctx->d_cnt,
-                                           cv, theta2, prm.variant == TC_VARIANT_TOP, sbits, ctx->m2l.p, ctx->mcap,
-                                           ctx->p2p.p, ctx->pcap, ctx->d_err);
+                                           cvm, theta2, prm.variant == TC_VARIANT_TOP, sbits, ctx->m2l.p, ctx->mcap,
+                                           ctx->p2p.p, ctx->pcap, ctx->d_err, mac);
     TcTravCounters hc;
     TC_CK(cudaMemcpyAsync(&hc, ctx->d_cnt, sizeof(hc), cudaMemcpyDeviceToHost, st));
     TC_CK(cudaMemcpyAsync(&herr, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
@@ -746,10 +755,59 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     k_list_targets<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->p2p_start.p, ctx->ncell, ctx->p2p_tl.p, ctx->d_small + 1);
     k_leaf_list<<<nblocks(ctx->ncell, 256), 256, 0, st>>>(ctx->ncell, cv.nchild, ctx->leaves.p, ctx->d_small + 2);
   }
-  unsigned hs[4];
   TC_CK(cudaMemcpyAsync(hs, ctx->d_small, sizeof(hs), cudaMemcpyDeviceToHost, st));
   TC_CK(cudaMemcpyAsync(&ctx->n_inter, &ctx->d_cnt->frontier[0], sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
   TC_CK(cudaStreamSynchronize(st));
+    return TC_OK;
+  };
+  TcMac mac;  // theta
+  if (ctx->emac && prm.variant == TC_VARIANT_TOP) {
+    // ---- low-order pre-pass on the geometric cells -> acc_old (integrator.h:476-493)
+    const int nc = ctx->ncell;
+    TC_CK(ctx->low_rgeo.ensure(nc));
+    TC_CK(ctx->low_m9.ensure((size_t)nc * kLowNT));
+    TC_CK(ctx->low_l9.ensure((size_t)nc * kLowNT));
+    TC_CK(ctx->acc_old.ensure(n));
+    TC_CK(ctx->cell_of.ensure(n));
+    TC_CK(ctx->min_acc.ensure(nc));
+    TC_CK(ctx->pn_ref.ensure((size_t)nc * (P + 1)));
+    const int gc = std::min(nblocks(nc, 128), 148 * 16);
+    const int gb = std::min(nblocks(n, 128), 148 * 16);
+    k_low_rgeo<<<gc, 128, 0, st>>>(nc, cv.level, ctx->d_root, ctx->low_rgeo.p);
+    k_low_p2m<<<gc, 128, 0, st>>>(nc, b, cv, ctx->low_m9.p);
+    for (int l = maxl; l >= 0; l--) k_low_m2m<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->low_m9.p);
+    TcCells geo = cv;
+    geo.X = cv.gx; geo.Y = cv.gy; geo.Z = cv.gz; geo.R = ctx->low_rgeo.p;
+    TcMac low;
+    low.mode = 1;
+    tc_status rl = build_lists(geo, low);
+    if (rl != TC_OK) return rl;
+    TC_CK(cudaMemsetAsync(ctx->low_l9.p, 0, sizeof(double) * (size_t)nc * kLowNT, st));
+    k_low_m2l<<<gc, 128, 0, st>>>(nc, cv, ctx->m2l_start.p, ctx->m2l_src.p, ctx->low_m9.p, ctx->low_l9.p);
+    k_low_cell_of<<<gc, 128, 0, st>>>(nc, cv, ctx->cell_of.p);
+    k_low_p2p<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->p2p_start.p, ctx->p2p_src.p, ctx->acc_old.p);
+    for (int l = 0; l < maxl; l++) k_low_l2l<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->low_l9.p);
+    k_low_l2p<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->low_l9.p, ctx->acc_old.p);
+    // ---- MAC inputs: min_acc (bottom-up) and Pn of the reference's form
+    for (int l = maxl; l >= 0; l--)
+      k_min_acc<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->acc_old.p, ctx->min_acc.p);
+    k_cell_pn_ref<P><<<gc, 128, 0, st>>>(nc, cv.M, ctx->pn_ref.p);
+    ctx->launches += 7 + 3 * (maxl + 1);
+    mac.mode = 2;
+    mac.p = P;
+    mac.fa = ctx->emac_fa;
+    mac.pn = ctx->pn_ref.p;
+    mac.min_acc = ctx->min_acc.p;
+    // combinator_coef[P][k] = P! / (k! (P-k)!) as the reference forms it (kernel_fast_lean.h:139)
+    double fact[2 * TC_PMAX_DEV + 2];
+    fact[0] = 1.0;
+    for (int i = 1; i < 2 * TC_PMAX_DEV + 2; i++) fact[i] = fact[i - 1] * (double)i;
+    for (int k = 0; k <= P; k++) mac.comb[k] = fact[P] * (1.0 / fact[k]) * (1.0 / fact[P - k]);
+  }
+  {
+    tc_status rh = build_lists(cv, mac);
+    if (rh != TC_OK) return rh;
+  }
   ctx->nleaf = (int)hs[2];
   if (ctx->events) cudaEventRecord(ctx->ev[3], st);
   // ---- far field and near field
@@ -1537,7 +1595,7 @@ static void graph_issue(tc_ctx* ctx, int n, const double* const* in, const unsig
 static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* const* in, const unsigned char* flags,
                        double* const* outp, int mem, bool jerk) {
   graph_drop(ctx);
-  if (ctx->direct || ctx->prm.selector > 0 || ctx->prm.precision == TC_PREC_MIXED_M2L) return;
+  if (ctx->direct || ctx->prm.selector > 0 || ctx->prm.precision == TC_PREC_MIXED_M2L || ctx->emac) return;
   graph_fn f = pick_graph(ctx->prm.p, jerk);
   if (!f) return;
   if (mem == TC_MEM_HOST) {
@@ -1698,6 +1756,26 @@ static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const doubl
     graph_plan(ctx, n, key, in, flags, outp, mem, jerk);
   }
   return rs;
+}
+
+tc_status tc_set_error_mac(tc_ctx* ctx, int on, double force_accuracy) {
+  if (!ctx || (on && !(force_accuracy > 0.0))) return TC_ERR_ARG;
+  if (on && ctx->prm.variant != TC_VARIANT_TOP) return TC_ERR_UNSUPPORTED;
+  ctx->emac = on != 0;
+  ctx->emac_fa = force_accuracy;
+  graph_drop(ctx);  // a captured graph used the theta MAC
+  return TC_OK;
+}
+
+tc_status tc_get_acc_old(tc_ctx* ctx, double* acc_old) {
+  if (!ctx || !acc_old) return TC_ERR_ARG;
+  if (!ctx->emac || !ctx->acc_old.p || ctx->direct) return TC_ERR_UNSUPPORTED;
+  std::vector<double> a(ctx->n);
+  std::vector<int> perm(ctx->n);
+  TC_CK(cudaMemcpy(a.data(), ctx->acc_old.p, ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
+  TC_CK(cudaMemcpy(perm.data(), ctx->perm.p, ctx->n * sizeof(int), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < ctx->n; i++) acc_old[perm[i]] = a[i];
+  return TC_OK;
 }
 
 tc_status tc_set_graph(tc_ctx* ctx, int on) {

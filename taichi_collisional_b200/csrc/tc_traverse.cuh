@@ -13,6 +13,18 @@
 
 namespace tc {
 
+// acceptance test of a traversal (mode 0: theta, traverse_eager.h:151-203; 1: the low-order
+// pre-pass, |d|^2 > 3 (Ri + Rj)^2 on geometric cells, :220-245; 2: the error-controlled MAC of
+// horizontalPassHigh, :61-148, with the reference's binomials comb[k] = combinator_coef[P][k])
+struct TcMac {
+  int mode = 0;
+  int p = 0;
+  double fa = 0.0;
+  const double* pn = nullptr;       // (p + 1) per cell
+  const double* min_acc = nullptr;  // per cell
+  double comb[TC_PMAX_DEV + 1];
+};
+
 struct TcTravCounters {
   unsigned long long frontier[3];  // rotating frontier sizes
   unsigned long long n_m2l, n_p2p;
@@ -43,7 +55,8 @@ __global__ void k_trav_init(int2* frontier, TcTravCounters* cnt) {
 __global__ void k_trav_step(int s, const int2* __restrict__ fin, int2* __restrict__ fout, unsigned long long fcap,
                             TcTravCounters* cnt, const TcCells c, double theta2, int top_variant, int sbits,
                             unsigned long long* __restrict__ m2l, unsigned long long m2l_cap,
-                            unsigned long long* __restrict__ p2p, unsigned long long p2p_cap, unsigned int* err) {
+                            unsigned long long* __restrict__ p2p, unsigned long long p2p_cap, unsigned int* err,
+                            const TcMac mac = TcMac()) {
   unsigned long long nin = cnt->frontier[s % 3];
   if (nin > fcap) nin = fcap;  // an overflowed step was flagged; never read past the buffer
   if (blockIdx.x == 0 && threadIdx.x == 0) cnt->frontier[(s + 2) % 3] = 0;
@@ -58,12 +71,41 @@ __global__ void k_trav_step(int s, const int2* __restrict__ fin, int2* __restric
       i = pr.x;
       j = pr.y;
       double dx = c.X[i] - c.X[j], dy = c.Y[i] - c.Y[j], dz = c.Z[i] - c.Z[j];
-      double R2 = (dx * dx + dy * dy + dz * dz) * theta2;
       double rs = c.R[i] + c.R[j];
       int nci = c.nchild[i], ncj = c.nchild[j];
-      if (R2 > rs * rs) {
+      bool accept;
+      if (mac.mode == 0) {
+        double R2 = (dx * dx + dy * dy + dz * dz) * theta2;
+        accept = R2 > rs * rs;
+      } else if (mac.mode == 1) {
+        accept = dx * dx + dy * dy + dz * dz > rs * rs * 3;
+      } else {
+        const double R2 = dx * dx + dy * dy + dz * dz;
+        double f1 = 10, f2 = 10;
+        const double Ra = c.R[i], Rb = c.R[j];
+        if (R2 > rs * rs) {
+          const double R = sqrt(R2);
+          double Rp = R2, pa = 1, pb = 1, Eba = 0, Eab = 0;
+          const int P = mac.p;
+          for (int k = 0; k <= P; k++) {
+            const double fac = mac.comb[k];
+            Eab += mac.pn[(size_t)i * (P + 1) + P - k] * pb * fac;
+            Eba += mac.pn[(size_t)j * (P + 1) + P - k] * pa * fac;
+            pa *= Ra;
+            pb *= Rb;
+            Rp *= R;
+          }
+          const double fac = 8 * fmax(Ra, Rb) / rs / Rp;
+          Eab *= fac;
+          f1 = Eab / (mac.fa * mac.min_acc[j]);
+          Eba *= fac;
+          f2 = Eba / (mac.fa * mac.min_acc[i]);
+        }
+        accept = f2 < 1 && f1 < 1;
+      }
+      if (accept) {
         int ni = c.nbody[i], nj = c.nbody[j];
-        act = (top_variant && ((ni <= 2 && nj <= 8) || (nj <= 2 && ni <= 8))) ? 1 : 0;
+        act = (mac.mode != 1 && top_variant && ((ni <= 2 && nj <= 8) || (nj <= 2 && ni <= 8))) ? 1 : 0;
       } else if (nci == 0 && ncj == 0) {
         act = 1;
       } else if (ncj == 0 || (c.R[i] >= c.R[j] && nci != 0)) {

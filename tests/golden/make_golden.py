@@ -10,9 +10,11 @@ Each case stores its inputs, the reference's per-body outputs (single-threaded, 
 sums are reproducible), the reference's cells (begin, nbody, nchild, child, centre,
 radius) and its M2L / P2P lists as visited by the reference recursion.  The steps_* cases
 store the time-step pass of the top-level tree (get_steps = true): near-field pot / acc and
-each body's accumulated 1 / tau^4, with a sink / source subset.
+each body's accumulated 1 / tau^4, with a sink / source subset.  The emac_* cases store the
+top tree's own get_force_and_potential: the low-order pre-pass (acc_old per body, min_acc per
+cell) and the error-controlled MAC's lists and forces.
 
-    python tests/golden/make_golden.py [--steps-only]
+    python tests/golden/make_golden.py [--emac-only | --steps-only]
 """
 import os
 import sys
@@ -41,6 +43,28 @@ STEPS_CASES = [
 ]
 
 
+EMAC_CASES = [
+    # name, generator, n, seed, p, ncrit, force_accuracy  (top tree, error-controlled MAC)
+    ("emac_top_kroupa3k_p8", "plummer_kroupa", 3000, 31, 8, 32, 2.0e-7),
+    ("emac_top_plummer2k_p12", "plummer", 2000, 32, 12, 64, 1.0e-8),
+]
+
+
+def make_emac(out_dir):
+    for name, gen, n, seed, p, ncrit, fa in EMAC_CASES:
+        x, y, z, vx, vy, vz, m = getattr(ics, gen)(n, seed)
+        r = oracle.ref_evaluate_high(x, y, z, m, p=p, ncrit=ncrit, force_accuracy=fa)
+        cells = oracle.ref_cells(oracle.VARIANT_TOP, p, r["ncell"], n)
+        lists = oracle.ref_lists(oracle.VARIANT_TOP, p)
+        np.savez_compressed(
+            os.path.join(out_dir, name + ".npz"), p=p, ncrit=ncrit, force_accuracy=fa,
+            x=x, y=y, z=z, m=m, ax=r["ax"], ay=r["ay"], az=r["az"], pot=r["pot"], acc_old=r["acc_old"],
+            min_acc=r["min_acc"], cell_begin=cells["begin"], cell_nbody=cells["nbody"],
+            cell_nchild=cells["nchild"], cell_child=cells["child"], cell_X=cells["X"], cell_R=cells["R"],
+            m2l_t=lists["m2l"][0], m2l_s=lists["m2l"][1], p2p_t=lists["p2p"][0], p2p_s=lists["p2p"][1])
+        print(name, "cells", r["ncell"], "m2l", len(lists["m2l"][0]), "p2p", len(lists["p2p"][0]))
+
+
 def steps_flags(n):
     """every third body a sink only, every fifth (from 1) a source only, the rest both"""
     fl = np.full(n, 3, np.uint8)
@@ -64,6 +88,9 @@ def make_steps(out_dir):
 
 def main():
     out_dir = os.path.dirname(os.path.abspath(__file__))
+    make_emac(out_dir)
+    if "--emac-only" in sys.argv:
+        return
     make_steps(out_dir)
     if "--steps-only" in sys.argv:
         return

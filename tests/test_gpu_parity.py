@@ -244,3 +244,32 @@ def test_time_step_pass_is_top_tree_only():
     with pytest.raises(tcb.TaichiError):
         g.evaluate_steps(x, y, z, m, vx, vy, vz, 0.025)
     g.close()
+
+
+def test_error_mac_matches_reference():
+    """The top tree's own get_force_and_potential (integrator.h:459-562): the low-order
+    pre-pass's acc_old, the error-controlled MAC's lists, the forces -- against the reference
+    run by tests/golden/make_golden.py (emac_* fixtures)."""
+    import glob
+    files = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "emac_*.npz")))
+    assert files
+    for f in files:
+        d = dict(np.load(f))
+        name = os.path.basename(f)
+        g = tcb.Gravity(p=int(d["p"]), ncrit=int(d["ncrit"]), theta=0.4, variant=tcb.VARIANT_TOP,
+                        precision=tcb.PREC_FP64)
+        g.set_error_mac(True, float(d["force_accuracy"]))
+        out = g.evaluate(d["x"], d["y"], d["z"], d["m"])
+        acc_old = g.acc_old()
+        assert np.max(np.abs(acc_old - d["acc_old"]) / np.abs(d["acc_old"])) < 1e-12, name
+        c = g.cells()
+        ref_lev = ref_cell_levels(d["cell_nchild"], d["cell_child"])
+        rkeys = cell_keys(d["cell_begin"], d["cell_nbody"], ref_lev)
+        gkeys = cell_keys(c["begin"], c["nbody"], c["level"])
+        assert sorted(rkeys) == sorted(gkeys), name
+        lists = g.lists()
+        for k in ("m2l", "p2p"):
+            assert pair_set(lists[k][0], lists[k][1], gkeys) == pair_set(d[k + "_t"], d[k + "_s"], rkeys), (name, k)
+        assert rel_err(out["pot"], d["pot"]).max() < 1e-12, name
+        assert rel_vec_err(vec(out, "a"), vec(d, "a")).max() < 1e-12, name
+        g.close()

@@ -65,6 +65,12 @@ inline void get_force_and_potential(Bodies& bodies, bool get_steps) {
     flags[i] = (unsigned char)((b.issink ? 1 : 0) | (b.issource ? 2 : 0));
   }
   tc_status s;
+#if defined(TC_SHIM_ERROR_MAC) && !defined(TC_SHIM_JERKS)
+  // the top tree's own traversal: low-order pre-pass + error-controlled MAC with the current
+  // global force_accuracy (integrator.h:459-562; main.cxx changes force_accuracy for a while)
+  s = tc_set_error_mac(tc_shim_context(), 1, force_accuracy);
+  if (s != TC_OK) ENDRUN("tc_set_error_mac: %s\n", tc_status_string(s));
+#endif
 #ifndef TC_SHIM_JERKS
   if (get_steps)
     s = tc_evaluate_steps(tc_shim_context(), n, x.data(), y.data(), z.data(), vx.data(), vy.data(), vz.data(),

@@ -25,7 +25,8 @@ int main(int argc, char**) {
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "exafmm.h")), reason="reference tree not present")
-@pytest.mark.parametrize("tree,defs", [("", []), ("taichi_with_jerks", ["-DTC_SHIM_JERKS"])])
+@pytest.mark.parametrize("tree,defs", [("", []), ("", ["-DTC_SHIM_ERROR_MAC"]),
+                                       ("taichi_with_jerks", ["-DTC_SHIM_JERKS"])])
 def test_shim_compiles_and_links_against_reference_types(tmp_path, tree, defs):
     src = tmp_path / "shim_main.cpp"
     src.write_text(PROGRAM)

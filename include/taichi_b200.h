@@ -195,6 +195,22 @@ tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, dou
                         double* vz, const double* ax, const double* ay, const double* az,
                         double dt_kick, double dt_drift);
 
+/* Hermite 4th-order step with one shared time step (Makino & Aarseth 1992), consuming the
+ * accelerations and jerks of the jerks tree; no counterpart in the reference, whose jerks tree
+ * has no integrator that uses them.  Device pointers, the context's stream:
+ *   tc_hermite_predict: save[12 n] <- (x, v, a, j) at t; x, v <- their Taylor predictions at
+ *     t + dt (x + v dt + a dt^2/2 + j dt^3/6, v + a dt + j dt^2/2)
+ *   (the caller evaluates a1, j1 at the predicted x, v with tc_evaluate)
+ *   tc_hermite_correct: v <- v0 + (a0 + a1) dt/2 + (j0 - j1) dt^2/12,
+ *                       x <- x0 + (v0 + v) dt/2 + (a0 - a1) dt^2/12.
+ * save is the caller's device buffer (12 n doubles); nothing is allocated. */
+tc_status tc_hermite_predict(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                             const double* ax, const double* ay, const double* az, const double* jx,
+                             const double* jy, const double* jz, double* save, double dt);
+tc_status tc_hermite_correct(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                             const double* ax, const double* ay, const double* az, const double* jx,
+                             const double* jy, const double* jz, const double* save, double dt);
+
 /* Measured arithmetic throughput of this GPU in GFLOP/s (kind 0: FP64 FMA, 1: FP32 FMA),
  * used as the roofline denominator of the FP64 / FP32 kernels.  Returns < 0 on error. */
 double tc_probe_peak(tc_ctx* ctx, int kind);

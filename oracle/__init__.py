@@ -212,6 +212,9 @@ def ref_lib(variant, p):
         if hasattr(L, "tcr_evaluate_high"):
             L.tcr_evaluate_high.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_int] + [_dp] * 4
             L.tcr_evaluate_high.restype = C.c_int
+            L.tcr_evaluate_high_steps.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_double,
+                                                                          C.c_int] + [_dp] * 5
+            L.tcr_evaluate_high_steps.restype = C.c_int
             L.tcr_acc_old.argtypes = [_dp]
             L.tcr_min_acc.argtypes = [_dp, _dp]
         if hasattr(L, "tcr_evaluate_steps"):
@@ -279,6 +282,24 @@ def ref_evaluate_high(x, y, z, m, *, p, ncrit, force_accuracy, nthreads=1, flags
     out["min_acc"] = np.zeros(nc)
     out["pn"] = np.zeros((nc, p + 1))
     L.tcr_min_acc(_d(out["min_acc"]), _d(out["pn"]))
+    return out
+
+
+def ref_evaluate_high_steps(x, y, z, m, vx, vy, vz, *, p, ncrit, force_accuracy, dt_param, nthreads=1, flags=None):
+    """The top tree's own get_force_and_potential(bodies, true): pre-pass, error-controlled MAC,
+    time-step pass (near-field pot / acc and per-body sum of 1 / tau^4)."""
+    L = ref_lib(VARIANT_TOP, p)
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    vx, vy, vz = map(_f64, (vx, vy, vz))
+    out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot", "timestep")}
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    nc = L.tcr_evaluate_high_steps(n, _d(x), _d(y), _d(z), _d(vx), _d(vy), _d(vz), _d(m),
+                                   None if fl is None else fl.ctypes.data_as(_u8p), force_accuracy, ncrit, dt_param,
+                                   nthreads, *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "timestep")])
+    out["ncell"] = nc
+    out["acc_old"] = np.zeros(n)
+    L.tcr_acc_old(_d(out["acc_old"]))
     return out
 
 

@@ -154,6 +154,16 @@ int tcr_evaluate_high(int n, const double* x, const double* y, const double* z, 
   return run(n, x, y, z, vx, vy, vz, m, flags, 0.4, nc, 0, nthreads, ax, ay, az, pot, nullptr, nullptr, nullptr,
              nullptr, false, nullptr, true);
 }
+// the same with get_steps = true (the time-step pass through the error-controlled MAC)
+int tcr_evaluate_high_steps(int n, const double* x, const double* y, const double* z, const double* vx,
+                            const double* vy, const double* vz, const double* m, const unsigned char* flags,
+                            double fa, int nc, double dtp, int nthreads, double* ax, double* ay, double* az,
+                            double* pot, double* timestep) {
+  force_accuracy = fa;
+  dt_param = dtp;
+  return run(n, x, y, z, vx, vy, vz, m, flags, 0.4, nc, 0, nthreads, ax, ay, az, pot, nullptr, nullptr, nullptr,
+             nullptr, true, timestep, true);
+}
 #endif
 }  // extern "C"
 

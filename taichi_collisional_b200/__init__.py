@@ -59,7 +59,7 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
-           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note", "tc_set_error_mac", "tc_get_acc_old"]
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note", "tc_set_error_mac", "tc_get_acc_old", "tc_hermite_predict", "tc_hermite_correct"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -90,6 +90,10 @@ def load_library(path=LIB_PATH):
     L.tc_graph_ready.restype = C.c_int
     L.tc_graph_note.argtypes = [C.c_void_p]
     L.tc_graph_note.restype = C.c_char_p
+    L.tc_hermite_predict.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 13 + [C.c_double]
+    L.tc_hermite_predict.restype = C.c_int
+    L.tc_hermite_correct.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 13 + [C.c_double]
+    L.tc_hermite_correct.restype = C.c_int
     L.tc_set_error_mac.argtypes = [C.c_void_p, C.c_int, C.c_double]
     L.tc_set_error_mac.restype = C.c_int
     L.tc_get_acc_old.argtypes = [C.c_void_p, _dp]
@@ -308,6 +312,21 @@ class Gravity:
         rc = self._L.tc_kick_drift(self._h, len(x), *[_ptr(a) for a in (x, y, z, vx, vy, vz, ax, ay, az)],
                                    float(dt_kick), float(dt_drift))
         self._check(rc, "tc_kick_drift")
+
+    def hermite_predict(self, x, y, z, vx, vy, vz, a, save, dt):
+        """Hermite 4th-order predictor on CUDA tensors (tc_hermite_predict); `a` is the dict of
+        ax, ay, az, jx, jy, jz at t, `save` a CUDA float64 tensor of 12 n."""
+        rc = self._L.tc_hermite_predict(self._h, len(x), *[_ptr(v) for v in (x, y, z, vx, vy, vz)],
+                                        *[_ptr(a[k]) for k in ("ax", "ay", "az", "jx", "jy", "jz")], _ptr(save),
+                                        float(dt))
+        self._check(rc, "tc_hermite_predict")
+
+    def hermite_correct(self, x, y, z, vx, vy, vz, a, save, dt):
+        """Hermite 4th-order corrector with a (ax..jz) evaluated at the predicted state."""
+        rc = self._L.tc_hermite_correct(self._h, len(x), *[_ptr(v) for v in (x, y, z, vx, vy, vz)],
+                                        *[_ptr(a[k]) for k in ("ax", "ay", "az", "jx", "jy", "jz")], _ptr(save),
+                                        float(dt))
+        self._check(rc, "tc_hermite_correct")
 
     def probe_peak(self, kind):
         """Measured FMA throughput of this GPU in GFLOP/s (0: FP64, 1: FP32)."""

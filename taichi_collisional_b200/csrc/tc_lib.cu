@@ -1114,6 +1114,54 @@ __global__ void k_kick_drift(int n, double* x, double* y, double* z, double* vx,
   }
 }
 
+// Hermite 4th-order predictor (Makino & Aarseth 1992) in FP64: saves x0, v0, a0, j0 into
+// save[12 n] (x y z, vx vy vz, ax ay az, jx jy jz) and writes the predicted x, v
+__global__ void k_hermite_predict(int n, double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
+                                  double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
+                                  const double* __restrict__ ax, const double* __restrict__ ay,
+                                  const double* __restrict__ az, const double* __restrict__ jx,
+                                  const double* __restrict__ jy, const double* __restrict__ jz,
+                                  double* __restrict__ save, double dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* const X[3] = {x, y, z};
+  double* const V[3] = {vx, vy, vz};
+  const double* const A[3] = {ax, ay, az};
+  const double* const J[3] = {jx, jy, jz};
+  for (int d = 0; d < 3; d++) {
+    const double x0 = X[d][i], v0 = V[d][i], a0 = A[d][i], j0 = J[d][i];
+    save[(size_t)d * n + i] = x0;
+    save[(size_t)(3 + d) * n + i] = v0;
+    save[(size_t)(6 + d) * n + i] = a0;
+    save[(size_t)(9 + d) * n + i] = j0;
+    X[d][i] = x0 + dt * (v0 + dt * (a0 / 2 + dt * (j0 / 6)));
+    V[d][i] = v0 + dt * (a0 + dt * (j0 / 2));
+  }
+}
+
+// Hermite 4th-order corrector with the accelerations and jerks a1, j1 at the predicted state
+__global__ void k_hermite_correct(int n, double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
+                                  double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
+                                  const double* __restrict__ ax, const double* __restrict__ ay,
+                                  const double* __restrict__ az, const double* __restrict__ jx,
+                                  const double* __restrict__ jy, const double* __restrict__ jz,
+                                  const double* __restrict__ save, double dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* const X[3] = {x, y, z};
+  double* const V[3] = {vx, vy, vz};
+  const double* const A[3] = {ax, ay, az};
+  const double* const J[3] = {jx, jy, jz};
+  for (int d = 0; d < 3; d++) {
+    const double x0 = save[(size_t)d * n + i], v0 = save[(size_t)(3 + d) * n + i];
+    const double a0 = save[(size_t)(6 + d) * n + i], j0 = save[(size_t)(9 + d) * n + i];
+    const double a1 = A[d][i], j1 = J[d][i];
+    const double v1 = v0 + dt / 2 * (a0 + a1) + dt * dt / 12 * (j0 - j1);
+    V[d][i] = v1;
+    X[d][i] = x0 + dt / 2 * (v0 + v1) + dt * dt / 12 * (a0 - a1);
+  }
+}
+
 template <typename T>
 __global__ void k_fma_probe(T* out, int iters) {
   T a0 = (T)threadIdx.x * (T)1e-3, a1 = a0 + (T)1, a2 = a0 + (T)2, a3 = a0 + (T)3;
@@ -1853,6 +1901,30 @@ tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, dou
   if (!ctx || n <= 0 || !x || !y || !z || !vx || !vy || !vz || !ax || !ay || !az) return TC_ERR_ARG;
   TC_CK(cudaSetDevice(ctx->prm.device));
   k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, vx, vy, vz, ax, ay, az, dt_kick, dt_drift);
+  TC_CK(cudaGetLastError());
+  return TC_OK;
+}
+
+tc_status tc_hermite_predict(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                             const double* ax, const double* ay, const double* az, const double* jx,
+                             const double* jy, const double* jz, double* save, double dt) {
+  if (!ctx || n <= 0 || !x || !y || !z || !vx || !vy || !vz || !ax || !ay || !az || !jx || !jy || !jz || !save)
+    return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  k_hermite_predict<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, vx, vy, vz, ax, ay, az, jx, jy, jz, save,
+                                                              dt);
+  TC_CK(cudaGetLastError());
+  return TC_OK;
+}
+
+tc_status tc_hermite_correct(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                             const double* ax, const double* ay, const double* az, const double* jx,
+                             const double* jy, const double* jz, const double* save, double dt) {
+  if (!ctx || n <= 0 || !x || !y || !z || !vx || !vy || !vz || !ax || !ay || !az || !jx || !jy || !jz || !save)
+    return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  k_hermite_correct<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, vx, vy, vz, ax, ay, az, jx, jy, jz, save,
+                                                              dt);
   TC_CK(cudaGetLastError());
   return TC_OK;
 }

@@ -63,6 +63,17 @@ def make_emac(out_dir):
             cell_nchild=cells["nchild"], cell_child=cells["child"], cell_X=cells["X"], cell_R=cells["R"],
             m2l_t=lists["m2l"][0], m2l_s=lists["m2l"][1], p2p_t=lists["p2p"][0], p2p_s=lists["p2p"][1])
         print(name, "cells", r["ncell"], "m2l", len(lists["m2l"][0]), "p2p", len(lists["p2p"][0]))
+    # the time-step pass through the error-controlled MAC, with a sink / source subset
+    name, n, seed, p, ncrit, fa, dtp = "emac_steps_top_kroupa2k_p8", 2000, 33, 8, 32, 2.0e-7, 0.025
+    x, y, z, vx, vy, vz, m = ics.plummer_kroupa(n, seed)
+    fl = steps_flags(n)
+    r = oracle.ref_evaluate_high_steps(x, y, z, m, vx, vy, vz, p=p, ncrit=ncrit, force_accuracy=fa, dt_param=dtp,
+                                       flags=fl)
+    np.savez_compressed(
+        os.path.join(out_dir, name + ".npz"), p=p, ncrit=ncrit, force_accuracy=fa, dt_param=dtp,
+        x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m, flags=fl, ax=r["ax"], ay=r["ay"], az=r["az"], pot=r["pot"],
+        timestep=r["timestep"], acc_old=r["acc_old"])
+    print(name, "cells", r["ncell"])
 
 
 def steps_flags(n):

@@ -251,7 +251,7 @@ def test_error_mac_matches_reference():
     pre-pass's acc_old, the error-controlled MAC's lists, the forces -- against the reference
     run by tests/golden/make_golden.py (emac_* fixtures)."""
     import glob
-    files = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "emac_*.npz")))
+    files = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "emac_top_*.npz")))
     assert files
     for f in files:
         d = dict(np.load(f))
@@ -273,3 +273,21 @@ def test_error_mac_matches_reference():
         assert rel_err(out["pot"], d["pot"]).max() < 1e-12, name
         assert rel_vec_err(vec(out, "a"), vec(d, "a")).max() < 1e-12, name
         g.close()
+
+
+def test_error_mac_time_step_pass_matches_reference():
+    """get_force_and_potential(bodies, true) of the top tree: pre-pass, error-controlled MAC,
+    time-step pass with a sink / source subset, against the reference's own run."""
+    d = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "emac_steps_top_kroupa2k_p8.npz")))
+    g = tcb.Gravity(p=int(d["p"]), ncrit=int(d["ncrit"]), theta=0.4, variant=tcb.VARIANT_TOP,
+                    precision=tcb.PREC_FP64)
+    g.set_error_mac(True, float(d["force_accuracy"]))
+    out = g.evaluate_steps(d["x"], d["y"], d["z"], d["m"], d["vx"], d["vy"], d["vz"], float(d["dt_param"]),
+                           flags=d["flags"])
+    sink = (d["flags"] & 1) != 0
+    assert np.all(np.abs(out["timestep"][sink] - d["timestep"][sink]) <= 1e-12 * d["timestep"][sink])
+    for k in ("pot", "ax", "ay", "az"):
+        assert np.abs(out[k][sink] - d[k][sink]).max() <= 1e-12 * np.abs(d[k]).max(), k
+    acc_old = g.acc_old()
+    assert np.max(np.abs(acc_old - d["acc_old"]) / np.abs(d["acc_old"])) < 1e-12
+    g.close()

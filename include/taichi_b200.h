@@ -114,8 +114,8 @@ tc_status tc_set_error_mac(tc_ctx* ctx, int on, double force_accuracy);
 /* The pre-pass's acc_old of the last evaluation with the error MAC, per body (caller order, host). */
 tc_status tc_get_acc_old(tc_ctx* ctx, double* acc_old);
 
-/* The whole evaluation as one CUDA graph (SURVEY's boundary call (B) as a graph; no counterpart
- * in the reference, which has no device).  With on != 0, tc_evaluate replays a captured graph
+/* The whole evaluation as one CUDA graph (no counterpart in the reference, which has no
+ * device).  With on != 0, tc_evaluate replays a captured graph
  * when the call matches the one it was captured for (same n, memory kind, every input/output
  * pointer and every tc_params field); any other call runs the normal path, returns its results
  * and then captures the graph for that call.  The captured sequence reads every count on the
@@ -194,6 +194,55 @@ tc_status tc_mlp_predict(int ns, int n_out, const float* feat, const float* w, c
 tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy,
                         double* vz, const double* ax, const double* ay, const double* az,
                         double dt_kick, double dt_drift);
+
+/* System diagnostics on device arrays (n bodies; pot in the positive convention p = +sum m/r
+ * that tc_evaluate writes).  Replaces system_kinetic_energy (integrator.h:887-895),
+ * system_potential_energy (:897-904) and system_center_of_mass (:906-925), G = 1:
+ *   out[0] = sum m |v|^2 / 2,  out[1] = sum m pot / 2,  out[2] = sum m,
+ *   out[3..5] = sum m x / sum m,  out[6..8] = sum m v / sum m    (out: 9 host doubles).
+ * The reference sums in long double; these sums are double-double, independent of the launch
+ * shape (bitwise reproducible).  Total energy as the reference prints it: out[0] - out[1].
+ * Synchronises the context's stream. */
+tc_status tc_system_diagnostics(tc_ctx* ctx, int n, const double* m, const double* x, const double* y,
+                                const double* z, const double* vx, const double* vy, const double* vz,
+                                const double* pot, double* out);
+
+/* Compensated drift on device arrays, replacing drift (integrator.h:642-656) with COMPSUM
+ * (integrator.h:42): per axis a = x; e += dt v; x = a + e; e += a - x, where e (ex, ey, ez) is
+ * the caller's running position error (the reference's particle::pos_e), zero initially.
+ * e += dt v is one fused multiply-add, as the reference compiles for an FMA-capable x86
+ * target.  Device pointers, the context's stream. */
+tc_status tc_drift_compensated(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
+                               double* ez, const double* vx, const double* vy, const double* vz, double dt);
+
+/* One step dt of the reference's block-time-step integrator, device-resident:
+ * do_evolve (integrator.h:873-890) with evolve_split_hold_dkd (integrator.h:834-871; the HOLD
+ * build), its split by time step (integrator.h:591-640), kick_naive with time steps
+ * (integrator.h:182-311: timestep = (sum 1/tau^4)^(-1/4) from tc_evaluate_steps with dt_param),
+ * kick of sinks by sources (integrator.h:378-457, with sink / source flags through
+ * tc_evaluate), kick_cpu for systems of at most 128 bodies (integrator.h:65-96, direct sums)
+ * and the compensated drift (tc_drift_compensated).  The top-level tree only; its MAC is the
+ * context's (tc_set_error_mac(ctx, 1, force_accuracy) for the reference's own).
+ * All arrays are the caller's device arrays of n entries, permuted in place as the reference's
+ * split swaps its particles (id[] follows the bodies; fill it with 0..n-1 to track them);
+ * ex, ey, ez are the running position errors (the reference's pos_e, zero initially);
+ * timestep and pot are outputs (the last values computed, as in the reference's particles).
+ * st (may be NULL) receives counts of the step. */
+typedef struct {
+  int n_evaluations;  /* FMM evaluations (time-step passes and kicks)          */
+  int n_direct;       /* direct kicks of small systems (kick_cpu)             */
+  int n_splits;
+  int max_level;      /* deepest level of the time-step hierarchy             */
+  double simtime;     /* time advanced as the reference's diag->simtime is    */
+} tc_evolve_stats;
+/* The reference's split (integrator.h:591-640) as a permutation, without moving anything:
+ * perm[k] = index (into timestep[]) of the body that the reference's two-pointer swaps leave at
+ * position k; *nfast = fast.n (bodies with timestep < |dt| first; a single fast body counts as
+ * none, as in the reference).  timestep and perm are device arrays; synchronises the stream. */
+tc_status tc_split_order(tc_ctx* ctx, int n, const double* timestep, double dt, int* perm, int* nfast);
+tc_status tc_evolve_hold_dkd(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
+                             double* ez, double* vx, double* vy, double* vz, double* m, double* timestep,
+                             double* pot, int* id, double dt_param, double dt, tc_evolve_stats* st);
 
 /* Hermite 4th-order step with one shared time step (Makino & Aarseth 1992), consuming the
  * accelerations and jerks of the jerks tree; no counterpart in the reference, whose jerks tree

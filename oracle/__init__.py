@@ -53,8 +53,11 @@ def build():
     """Compile liboracle.so (and, when the reference tree is present, oracle/_ref)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
     if os.path.isdir(os.environ.get("TC_REFERENCE", "/root/reference")):
-        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref",
-                               "REF=" + os.environ.get("TC_REFERENCE", "/root/reference")])
+        ref = "REF=" + os.environ.get("TC_REFERENCE", "/root/reference")
+        subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", ref])
+        # the reference's integrator over this repository's force evaluation needs the CUDA library
+        if os.path.exists(os.path.join(HERE, "..", "taichi_collisional_b200", "libtaichi_b200.so")):
+            subprocess.check_call(["make", "-s", "-j2", "-C", HERE, "ref-shim", ref])
 
 
 def lib():
@@ -76,6 +79,8 @@ def lib():
         L.tco_last_list.restype = C.c_longlong
         L.tco_direct.argtypes = [C.c_int] + [_dp] * 7 + [C.c_int, _ip] + [_dp] * 7
         L.tco_init.argtypes = [C.c_int]
+        L.tco_system_diagnostics.argtypes = [C.c_int] + [_dp] * 9
+        L.tco_drift_compsum.argtypes = [C.c_int, _dp, _dp, _dp, C.c_double]
         L.tco_make_gnm.argtypes = [_dp, _dp, _dp, C.c_int]
         L.tco_swap_xz.argtypes = [_dp, C.c_int]
         L.tco_p2m.argtypes = [C.c_int, C.c_int] + [_dp] * 10
@@ -175,6 +180,51 @@ def direct(x, y, z, m, vx=None, vy=None, vz=None, targets=None):
                  None if tg is None else tg.ctypes.data_as(_ip),
                  *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")])
     return out
+
+
+DIAG_KEYS = ("kinetic", "potential", "mass", "cm_pos", "cm_vel")
+
+
+def _diag_dict(out):
+    return {"kinetic": out[0], "potential": out[1], "mass": out[2], "cm_pos": tuple(out[3:6]),
+            "cm_vel": tuple(out[6:9])}
+
+
+def system_diagnostics(m, x, y, z, vx, vy, vz, pot):
+    """The reference's system_kinetic_energy / system_potential_energy / system_center_of_mass
+    (integrator.h:887-925), restated in C with long-double sums (tco_system_diagnostics)."""
+    out = np.zeros(9)
+    a = [_f64(v) for v in (m, x, y, z, vx, vy, vz, pot)]
+    lib().tco_system_diagnostics(len(a[0]), *[_d(v) for v in a], _d(out))
+    return _diag_dict(out)
+
+
+def drift_compsum(s, e, v, dt):
+    """drift with COMPSUM (integrator.h:42, :642-656) on one axis; returns new (s, e)."""
+    s = np.array(s, dtype=np.float64)
+    e = np.array(e, dtype=np.float64)
+    v = _f64(v)
+    lib().tco_drift_compsum(len(s), _d(s), _d(e), _d(v), float(dt))
+    return s, e
+
+
+def split_order(ts, dt):
+    """The reference's split(dt, s, &slow, &fast) (integrator.h:591-640), restated: the order the
+    bodies end in (ids) and the number of fast bodies.  Two pointers walk in from both ends and
+    swap a slow body (timestep >= |dt|) found on the left with a fast one (timestep < |dt|)
+    found on the right, so the k-th slow body inside the final fast prefix swaps with the k-th
+    fast body, counted from the right, inside the final slow suffix; a single fast body is
+    reported as none (fast.n = 1 -> 0)."""
+    ts = np.asarray(ts, dtype=np.float64)
+    n = len(ts)
+    dt = abs(dt)
+    fast = ts < dt
+    nf = int(fast.sum())
+    perm = np.arange(n)
+    left = np.nonzero(~fast[:nf])[0]               # slow bodies in the fast prefix, left to right
+    right = nf + np.nonzero(fast[nf:])[0][::-1]    # fast bodies in the slow suffix, right to left
+    perm[left], perm[right] = right, left
+    return perm, (0 if nf == 1 else nf)
 
 
 # ----------------------------------------------------------------------------------------
@@ -325,3 +375,77 @@ def ref_lists(variant, p):
         L.tcr_list(kind, t.ctypes.data_as(_ip), s.ctypes.data_as(_ip))
         out[name] = (t, s)
     return out
+
+
+def integ_ref_path():
+    return os.path.join(HERE, "_ref", "libtcref_integ_%s.so" % _isa())
+
+
+def integ_ref_available():
+    return os.path.exists(integ_ref_path())
+
+
+def _integ_ref():
+    key = "integ"
+    if key not in _ref_libs:
+        L = C.CDLL(integ_ref_path())
+        L.tcr_system_diagnostics.argtypes = [C.c_int] + [_dp] * 9
+        L.tcr_drift.argtypes = [C.c_int] + [_dp] * 9 + [C.c_double]
+        L.tcr_split.argtypes = [C.c_int, _dp, C.c_double, _ip]
+        L.tcr_split.restype = C.c_int
+        _ref_libs[key] = L
+    return _ref_libs[key]
+
+
+def ref_system_diagnostics(m, x, y, z, vx, vy, vz, pot):
+    """The reference's own diagnostics (oracle/_ref/libtcref_integ_*)."""
+    out = np.zeros(9)
+    a = [_f64(v) for v in (m, x, y, z, vx, vy, vz, pot)]
+    _integ_ref().tcr_system_diagnostics(len(a[0]), *[_d(v) for v in a], _d(out))
+    return _diag_dict(out)
+
+
+def ref_drift(x, y, z, ex, ey, ez, vx, vy, vz, dt):
+    """The reference's own drift (COMPSUM); returns new (x, y, z, ex, ey, ez)."""
+    st = [np.array(a, dtype=np.float64) for a in (x, y, z, ex, ey, ez)]
+    v = [_f64(a) for a in (vx, vy, vz)]
+    _integ_ref().tcr_drift(len(st[0]), *[_d(a) for a in st], *[_d(a) for a in v], float(dt))
+    return tuple(st)
+
+
+def ref_split(ts, dt):
+    """The reference's own split: (order of ids, fast.n)."""
+    ts = _f64(ts)
+    perm = np.zeros(len(ts), dtype=np.int32)
+    nf = _integ_ref().tcr_split(len(ts), _d(ts), float(dt), perm.ctypes.data_as(_ip))
+    return perm, nf
+
+
+def integ_shim_path():
+    return os.path.join(HERE, "_ref", "libtcref_integ_shim_%s.so" % _isa())
+
+
+def _evolve_lib(shim):
+    key = "integ_shim" if shim else "integ"
+    if shim and key not in _ref_libs:
+        _ref_libs[key] = C.CDLL(integ_shim_path())
+    L = _ref_libs[key] if shim else _integ_ref()
+    L.tcr_evolve_hold.argtypes = [C.c_int] + [_dp] * 12 + [_ip, C.c_int, C.c_double, C.c_double, C.c_double,
+                                                           C.c_double]
+    L.tcr_evolve_hold.restype = C.c_double
+    return L
+
+
+EVOLVE_KEYS = ("x", "y", "z", "ex", "ey", "ez", "vx", "vy", "vz", "m", "timestep", "pot")
+
+
+def ref_evolve_hold(state, *, ncrit, theta, force_accuracy, dt_param, dt, shim=False):
+    """One do_evolve step of the reference's HOLD scheme (evolve_split_hold_dkd) on a dict of
+    arrays (EVOLVE_KEYS + "id"), with the reference's own force evaluation (p = 8), or -- shim=True
+    -- with this repository's, through the C++ shim.  Returns (new state, simtime)."""
+    st = {k: np.array(state[k], dtype=np.float64) for k in EVOLVE_KEYS}
+    st["id"] = np.array(state["id"], dtype=np.int32)
+    L = _evolve_lib(shim)
+    t = L.tcr_evolve_hold(len(st["x"]), *[_d(st[k]) for k in EVOLVE_KEYS], st["id"].ctypes.data_as(_ip), ncrit,
+                          theta, force_accuracy, dt_param, dt)
+    return st, t

@@ -1022,3 +1022,45 @@ long long tco_last_list(int kind, int* tgt, int* src) {
   if (src) memcpy(src, kind ? T.p2p_s : T.m2l_s, sizeof(int) * n);
   return n;
 }
+
+/* ---- integrator diagnostics and compensated drift (integrator.h:42, :642-656, :887-925) ---- */
+void tco_system_diagnostics(int n, const double* m, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz, const double* pot,
+                            double* out) {
+  long double kin = 0, pe = 0, mass = 0, pos[3] = {0, 0, 0}, vel[3] = {0, 0, 0};
+  for (int i = 0; i < n; i++) {
+    volatile double v2 = vx[i] * vx[i];
+    volatile double t;
+    v2 = v2 + vy[i] * vy[i];
+    v2 = v2 + vz[i] * vz[i];
+    t = m[i] * v2;
+    kin += t / 2;
+    t = m[i] * pot[i];
+    pe += t / 2;
+  }
+  for (int i = 0; i < n; i++) {
+    pos[0] += (long double)m[i] * x[i];
+    pos[1] += (long double)m[i] * y[i];
+    pos[2] += (long double)m[i] * z[i];
+    vel[0] += (long double)m[i] * vx[i];
+    vel[1] += (long double)m[i] * vy[i];
+    vel[2] += (long double)m[i] * vz[i];
+    mass += (long double)m[i];
+  }
+  out[0] = (double)kin;
+  out[1] = (double)pe;
+  out[2] = (double)mass;
+  for (int d = 0; d < 3; d++) {
+    out[3 + d] = (double)(pos[d] / mass);
+    out[6 + d] = (double)(vel[d] / mass);
+  }
+}
+
+void tco_drift_compsum(int n, double* s, double* e, const double* v, double dt) {
+  for (int i = 0; i < n; i++) {
+    double a = s[i];
+    e[i] = fma(dt, v[i], e[i]);
+    s[i] = a + e[i];
+    e[i] += a - s[i];
+  }
+}

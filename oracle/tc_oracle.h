@@ -88,6 +88,16 @@ void tco_l2p(int p, const double* L, const double* Ld, const double* dX, const d
              double* out7 /* pot, ax, ay, az, jx, jy, jz (accumulated) */);
 int tco_miniball(int np, const double* pts /*3*np*/, double* c, double* r2);
 
+/* system_kinetic_energy, system_potential_energy, system_center_of_mass (integrator.h:887-925):
+ * per-term FP64 expressions summed in order in long double, as the reference does (G = 1).
+ * out[9] = kinetic, potential, mass, centre of mass (3), centre-of-mass velocity (3). */
+void tco_system_diagnostics(int n, const double* m, const double* x, const double* y, const double* z,
+                            const double* vx, const double* vy, const double* vz, const double* pot,
+                            double* out);
+/* drift with COMPSUM (integrator.h:42, :642-656) on one axis: a = s; e += dt v (fused);
+ * s = a + e; e += a - s. */
+void tco_drift_compsum(int n, double* s, double* e, const double* v, double dt);
+
 #ifdef __cplusplus
 }
 #endif

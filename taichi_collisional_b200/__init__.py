@@ -59,7 +59,8 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_get_cells", "tc_get_lists", "tc_get_expansions", "tc_status_string", "tc_last_error_string",
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
-           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note", "tc_set_error_mac", "tc_get_acc_old", "tc_hermite_predict", "tc_hermite_correct"]
+           "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note", "tc_set_error_mac", "tc_get_acc_old", "tc_hermite_predict", "tc_hermite_correct",
+           "tc_system_diagnostics", "tc_drift_compensated", "tc_split_order", "tc_evolve_hold_dkd"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -117,6 +118,15 @@ def load_library(path=LIB_PATH):
     L.tc_order_supported.restype = C.c_int
     L.tc_kick_drift.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 9 + [C.c_double, C.c_double]
     L.tc_kick_drift.restype = C.c_int
+    L.tc_system_diagnostics.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 8 + [C.POINTER(C.c_double)]
+    L.tc_system_diagnostics.restype = C.c_int
+    L.tc_drift_compensated.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 9 + [C.c_double]
+    L.tc_drift_compensated.restype = C.c_int
+    L.tc_split_order.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.POINTER(C.c_int)]
+    L.tc_split_order.restype = C.c_int
+    L.tc_evolve_hold_dkd.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 13 + [C.c_double, C.c_double,
+                                                                                 C.POINTER(EvolveStats)]
+    L.tc_evolve_hold_dkd.restype = C.c_int
     L.tc_probe_peak.argtypes = [C.c_void_p, C.c_int]
     L.tc_probe_peak.restype = C.c_double
     L.tc_evaluate_direct_noalloc.argtypes = [C.c_int] + [C.c_void_p] * 8 + [C.c_void_p] * 7 + [C.c_int, C.c_void_p]
@@ -165,6 +175,14 @@ def default_params(**kw):
         else:
             setattr(prm, k, v)
     return prm
+
+
+class EvolveStats(C.Structure):
+    _fields_ = [("n_evaluations", C.c_int), ("n_direct", C.c_int), ("n_splits", C.c_int), ("max_level", C.c_int),
+                ("simtime", C.c_double)]
+
+
+EVOLVE_KEYS = ("x", "y", "z", "ex", "ey", "ez", "vx", "vy", "vz", "m", "timestep", "pot")
 
 
 def _ptr(a):
@@ -312,6 +330,43 @@ class Gravity:
         rc = self._L.tc_kick_drift(self._h, len(x), *[_ptr(a) for a in (x, y, z, vx, vy, vz, ax, ay, az)],
                                    float(dt_kick), float(dt_drift))
         self._check(rc, "tc_kick_drift")
+
+    def system_diagnostics(self, m, x, y, z, vx, vy, vz, pot):
+        """Kinetic and potential energy, total mass, centre of mass and its velocity of CUDA
+        float64 tensors (tc_system_diagnostics; the reference's system_kinetic_energy,
+        system_potential_energy, system_center_of_mass).  Returns a dict of floats."""
+        out = (C.c_double * 9)()
+        rc = self._L.tc_system_diagnostics(self._h, len(m), *[_ptr(a) for a in (m, x, y, z, vx, vy, vz, pot)], out)
+        self._check(rc, "tc_system_diagnostics")
+        return {"kinetic": out[0], "potential": out[1], "mass": out[2], "cm_pos": tuple(out[3:6]),
+                "cm_vel": tuple(out[6:9])}
+
+    def drift_compensated(self, x, y, z, ex, ey, ez, vx, vy, vz, dt):
+        """Compensated drift x += v dt with running errors ex, ey, ez (tc_drift_compensated;
+        the reference's drift with COMPSUM)."""
+        rc = self._L.tc_drift_compensated(self._h, len(x), *[_ptr(a) for a in (x, y, z, ex, ey, ez, vx, vy, vz)],
+                                          float(dt))
+        self._check(rc, "tc_drift_compensated")
+
+    def split_order(self, timestep, dt):
+        """The reference's split by time step as a permutation (tc_split_order) of a CUDA float64
+        tensor: returns (perm, nfast), perm an int32 CUDA tensor."""
+        import torch
+        perm = torch.empty(len(timestep), dtype=torch.int32, device=timestep.device)
+        nf = C.c_int(0)
+        rc = self._L.tc_split_order(self._h, len(timestep), _ptr(timestep), float(dt), _ptr(perm), C.byref(nf))
+        self._check(rc, "tc_split_order")
+        return perm, nf.value
+
+    def evolve_hold_dkd(self, state, dt_param, dt):
+        """One step dt of the reference's HOLD block-time-step scheme (tc_evolve_hold_dkd) on a
+        dict of CUDA tensors: float64 EVOLVE_KEYS and int32 "id", permuted in place.  Returns the
+        step's counts as a dict."""
+        st = EvolveStats()
+        rc = self._L.tc_evolve_hold_dkd(self._h, len(state["x"]), *[_ptr(state[k]) for k in EVOLVE_KEYS],
+                                        _ptr(state["id"]), float(dt_param), float(dt), C.byref(st))
+        self._check(rc, "tc_evolve_hold_dkd")
+        return {k: getattr(st, k) for k, _ in EvolveStats._fields_}
 
     def hermite_predict(self, x, y, z, vx, vy, vz, a, save, dt):
         """Hermite 4th-order predictor on CUDA tensors (tc_hermite_predict); `a` is the dict of

@@ -33,6 +33,7 @@
 #include "tc_select.cuh"
 #include "tc_mlp.cuh"
 #include "tc_train.cuh"
+#include "tc_diag.cuh"
 #include "tdesign.h"
 
 using namespace tc;
@@ -132,6 +133,13 @@ struct tc_ctx {
   DBuf<double> tsum;
   // tc_direct_sums: bodies in caller order, targets, partial and final sums
   DBuf<double> ds_bod, ds_out;
+  DBuf<double> diag;  // system diagnostics: block partials + the 9 results
+  // block-time-step integrator: accelerations, potential, 1/tau^4 sums; split counters, pair
+  // positions, kick flags
+  DBuf<double> ev_d;
+  DBuf<uint32_t> ev_u;
+  DBuf<int> ev_i;
+  DBuf<uint8_t> ev_f;
   DBuf<uint8_t> ds_flags;
   DBuf<int> ds_idx, ds_tgt;
   size_t fcap = 0, mcap = 0, pcap = 0;
@@ -1295,7 +1303,8 @@ tc_status tc_destroy(tc_ctx* ctx) {
   ctx->cell_pn.release(); ctx->cls_start.release(); ctx->cls_tl.release(); ctx->mlp_w.release();
   ctx->judge_idx.release(); ctx->judge_out.release();
   ctx->ds_bod.release(); ctx->ds_out.release(); ctx->ds_flags.release(); ctx->ds_idx.release(); ctx->ds_tgt.release();
-  ctx->tsum.release();
+  ctx->tsum.release(); ctx->diag.release();
+  ctx->ev_d.release(); ctx->ev_u.release(); ctx->ev_i.release(); ctx->ev_f.release();
   if (ctx->d_root) cudaFree(ctx->d_root);
   if (ctx->d_lv) cudaFree(ctx->d_lv);
   if (ctx->d_cnt) cudaFree(ctx->d_cnt);
@@ -1905,6 +1914,34 @@ tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, dou
   return TC_OK;
 }
 
+tc_status tc_system_diagnostics(tc_ctx* ctx, int n, const double* m, const double* x, const double* y,
+                                const double* z, const double* vx, const double* vy, const double* vz,
+                                const double* pot, double* out) {
+  if (!ctx || n <= 0 || !m || !x || !y || !z || !vx || !vy || !vz || !pot || !out) return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->prm.device);
+  const int nblk = std::max(1, std::min(4 * nsm, (n + kDiagThreads - 1) / kDiagThreads));
+  TC_CK(ctx->diag.ensure((size_t)nblk * kDiagQ * 2 + kDiagQ));
+  double* res = ctx->diag.p + (size_t)nblk * kDiagQ * 2;
+  cudaStream_t st = ctx->stream;
+  k_sys_diag_part<<<nblk, kDiagThreads, 0, st>>>(n, m, x, y, z, vx, vy, vz, pot, ctx->diag.p);
+  k_sys_diag_final<<<1, kDiagThreads, 0, st>>>(nblk, ctx->diag.p, res);
+  TC_CK(cudaGetLastError());
+  TC_CK(cudaMemcpyAsync(out, res, kDiagQ * sizeof(double), cudaMemcpyDeviceToHost, st));
+  TC_CK(cudaStreamSynchronize(st));
+  return TC_OK;
+}
+
+tc_status tc_drift_compensated(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
+                               double* ez, const double* vx, const double* vy, const double* vz, double dt) {
+  if (!ctx || n <= 0 || !x || !y || !z || !ex || !ey || !ez || !vx || !vy || !vz) return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  k_drift_compsum<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, ex, ey, ez, vx, vy, vz, dt);
+  TC_CK(cudaGetLastError());
+  return TC_OK;
+}
+
 tc_status tc_hermite_predict(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
                              const double* ax, const double* ay, const double* az, const double* jx,
                              const double* jy, const double* jz, double* save, double dt) {
@@ -2213,3 +2250,5 @@ tc_status tc_get_expansions(tc_ctx* ctx, double* M, double* Md, double* L, doubl
 }
 
 }  // extern "C"
+
+#include "tc_integrate.cuh"

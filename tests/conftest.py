@@ -40,7 +40,7 @@ def golden_cases():
     out = {}
     for f in sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz"))):
         name = os.path.basename(f)[:-4]
-        if name.startswith(("steps_", "emac_")):  # the time-step pass and error-MAC cases have their own tests
+        if name.startswith(("steps_", "emac_", "integ_", "evolve_")):  # cases with tests of their own
             continue
         out[name] = dict(np.load(f))
     return out

@@ -12,9 +12,12 @@ radius) and its M2L / P2P lists as visited by the reference recursion.  The step
 store the time-step pass of the top-level tree (get_steps = true): near-field pot / acc and
 each body's accumulated 1 / tau^4, with a sink / source subset.  The emac_* cases store the
 top tree's own get_force_and_potential: the low-order pre-pass (acc_old per body, min_acc per
-cell) and the error-controlled MAC's lists and forces.
+cell) and the error-controlled MAC's lists and forces.  The integ_* case stores the
+reference integrator's diagnostics (kinetic / potential energy, centre of mass), three
+compensated drifts and one split by time step.  The evolve_* case stores one do_evolve step
+of the reference's HOLD block-time-step scheme with its own force evaluation (p = 8).
 
-    python tests/golden/make_golden.py [--emac-only | --steps-only]
+    python tests/golden/make_golden.py [--evolve-only | --integ-only | --emac-only | --steps-only]
 """
 import os
 import sys
@@ -97,8 +100,56 @@ def make_steps(out_dir):
         print(name, "cells", r["ncell"])
 
 
+INTEG_CASE = ("integ_plummer_kroupa2k", "plummer_kroupa", 2048, 31, 1.0 / 64)
+
+
+def make_integ(out_dir):
+    name, gen, n, seed, dt = INTEG_CASE
+    x, y, z, vx, vy, vz, m = getattr(ics, gen)(n, seed)
+    pot = oracle.direct(x, y, z, m)["pot"]
+    d = oracle.ref_system_diagnostics(m, x, y, z, vx, vy, vz, pot)
+    diag = np.array([d["kinetic"], d["potential"], d["mass"], *d["cm_pos"], *d["cm_vel"]])
+    st = (x, y, z, np.zeros(n), np.zeros(n), np.zeros(n))
+    for _ in range(3):
+        st = oracle.ref_drift(*st, vx, vy, vz, dt)
+    # block time steps 2^-k (k = 3..9) from the body's speed, so the split has ties with dt
+    speed = np.sqrt(vx * vx + vy * vy + vz * vz)
+    ts = 2.0 ** -np.clip(np.round(3 + 6 * speed / speed.max()), 3, 9)
+    perm, nf = oracle.ref_split(ts, dt)
+    np.savez_compressed(os.path.join(out_dir, name + ".npz"), dt=dt, x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m,
+                        pot=pot, diag=diag, drift_x=st[0], drift_y=st[1], drift_z=st[2], drift_ex=st[3],
+                        drift_ey=st[4], drift_ez=st[5], ts=ts, split_perm=perm, split_nfast=nf)
+    print(name, "kinetic", d["kinetic"], "potential", d["potential"], "fast", nf)
+
+
+EVOLVE_CASE = ("evolve_hold_plummer_kroupa1k", "plummer_kroupa", 1024, 41, 64, 0.4, 2e-7, 0.025, 1.0 / 64)
+
+
+def evolve_initial_state(gen, n, seed):
+    x, y, z, vx, vy, vz, m = getattr(ics, gen)(n, seed)
+    zero = np.zeros(n)
+    return dict(x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m, ex=zero, ey=zero, ez=zero, timestep=zero, pot=zero,
+                id=np.arange(n, dtype=np.int32))
+
+
+def make_evolve(out_dir):
+    name, gen, n, seed, nc, th, fa, dtp, dt = EVOLVE_CASE
+    st0 = evolve_initial_state(gen, n, seed)
+    st, simtime = oracle.ref_evolve_hold(st0, ncrit=nc, theta=th, force_accuracy=fa, dt_param=dtp, dt=dt)
+    np.savez_compressed(os.path.join(out_dir, name + ".npz"), gen=gen, n=n, seed=seed, ncrit=nc, theta=th,
+                        force_accuracy=fa, dt_param=dtp, dt=dt, simtime=simtime,
+                        **{"out_" + k: v for k, v in st.items()})
+    print(name, "simtime", simtime)
+
+
 def main():
     out_dir = os.path.dirname(os.path.abspath(__file__))
+    make_evolve(out_dir)
+    if "--evolve-only" in sys.argv:
+        return
+    make_integ(out_dir)
+    if "--integ-only" in sys.argv:
+        return
     make_emac(out_dir)
     if "--emac-only" in sys.argv:
         return

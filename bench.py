@@ -8,6 +8,7 @@ seeded synthetic data (no dataset is involved) and stay resident in HBM; the sta
 (7 x 32 MiB) is larger than L2, so every step streams from HBM.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+  python bench.py --evolve N [--steps K --warmup W]   # the block-time-step integrator instead
 
 N > 1 (torchrun, one process per GPU): independent replicas, no data-path collective; the
 timed region is bracketed by barriers and the slowest rank's device time is reported.
@@ -51,6 +52,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each evaluation's kernels directly instead of replaying one captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--evolve", type=int, default=0, metavar="N",
+                    help="time one step of the HOLD block-time-step integrator on N bodies instead")
     return ap.parse_args()
 
 
@@ -185,6 +188,58 @@ def run_reference(args, rank):
     print(json.dumps(line))
 
 
+EVOLVE_CPU_SAMPLE_N = 1024
+
+
+def run_evolve(args):
+    """One do_evolve step (evolve_split_hold_dkd, dt = 1/64, dt_param = 0.025) of the
+    reference's block-time-step scheme, device-resident (tc_evolve_hold_dkd), with the top
+    tree's error-controlled MAC (force_accuracy 2e-7) at p = 8, ncrit = 64: particle-steps/s
+    over K steps, CUDA events around them; beside it the reference's own step (its CPU FMM and
+    integrator, oracle/_ref) on a 1,024-body sample."""
+    import torch
+    import taichi_collisional_b200 as tcb
+    n, dt, dtp, fa = args.evolve, 1.0 / 64, 0.025, 2e-7
+    x, y, z, vx, vy, vz, m = make_ics(n, 2027)
+    zero = np.zeros(n)
+    host = dict(x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m, ex=zero, ey=zero, ez=zero, timestep=zero, pot=zero)
+    st = {k: torch.tensor(v, dtype=torch.float64, device="cuda") for k, v in host.items()}
+    st["id"] = torch.arange(n, dtype=torch.int32, device="cuda")
+    g = tcb.Gravity(p=8, ncrit=64, theta=0.4, variant=tcb.VARIANT_TOP, precision=tcb.PREC_FP64)
+    g.set_error_mac(True, fa)
+    for _ in range(args.warmup):
+        g.evolve_hold_dkd(st, dtp, dt)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    e0.record()
+    for _ in range(args.steps):
+        stats.append(g.evolve_hold_dkd(st, dtp, dt))
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    line = {"metric": "particle-steps/s of one HOLD block-time-step step (p=8, error MAC)", "impl": "ours",
+            "value": n / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded Plummer/Kroupa)",
+            "config": {"workload": "hold_dkd_plummer_kroupa_N%d_p8_fa2e-7_dt1/64" % n, "n": n, "p": 8, "ncrit": 64,
+                       "force_accuracy": fa, "dt": dt, "dt_param": dtp},
+            "per_step": {k: [s[k] for s in stats] for k in ("n_evaluations", "n_direct", "max_level")}}
+    import oracle
+    if not args.no_cpu_baseline and oracle.integ_ref_available():
+        xs, ys, zs, vxs, vys, vzs, ms_ = make_ics(EVOLVE_CPU_SAMPLE_N, 2027)
+        z0 = np.zeros(EVOLVE_CPU_SAMPLE_N)
+        s0 = dict(x=xs, y=ys, z=zs, vx=vxs, vy=vys, vz=vzs, m=ms_, ex=z0, ey=z0, ez=z0, timestep=z0, pot=z0,
+                  id=np.arange(EVOLVE_CPU_SAMPLE_N, dtype=np.int32))
+        t0 = time.perf_counter()
+        oracle.ref_evolve_hold(s0, ncrit=64, theta=0.4, force_accuracy=fa, dt_param=dtp, dt=dt)
+        sec = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": EVOLVE_CPU_SAMPLE_N / sec, "unit": UNIT, "cores": os.cpu_count() or 1,
+                                "kind": "reference", "sample": "one HOLD step of a %d-body Plummer/Kroupa sample "
+                                "(the reference's integrator.h and CPU FMM, p = 8)" % EVOLVE_CPU_SAMPLE_N}
+    print(json.dumps(line))
+    g.close()
+
+
 def error_stats(out, idx_t, ref):
     """RMS and 99th percentile of |a - a_ref| / |a_ref| and |j - j_ref| / |j_ref| at the
     targets idx_t (out: device tensors of one evaluation, ref: direct sums at those bodies)."""
@@ -205,6 +260,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.evolve:
+        run_evolve(args)
         return
     import datetime
 

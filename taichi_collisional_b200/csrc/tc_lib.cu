@@ -1462,9 +1462,14 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
     if (ctx->events)
       for (int i = 1; i <= 6; i++) cudaEventRecord(ctx->ev[i], st);
   } else {
+    size_t grow_c = 0;  // cell capacity asked for by a retry after a cell overflow
     for (int attempt = 0; attempt < 4; attempt++) {
-      size_t want_c = ctx->ccap ? ctx->ccap : (size_t)(2 * N / (size_t)(ctx->prm.ncrit > 8 ? 8 : ctx->prm.ncrit) + 1024);
+      // cells for this n (kept at least as large as what the context already holds), or what a
+      // retry asks for; the buffers are grown whenever the capacity grows
+      size_t want_c = (size_t)(2 * N / (size_t)(ctx->prm.ncrit > 8 ? 8 : ctx->prm.ncrit) + 1024);
       if (want_c > 2 * N + 1024) want_c = 2 * N + 1024;
+      if (want_c < ctx->ccap) want_c = ctx->ccap;
+      if (want_c < grow_c) want_c = grow_c;
       if (ctx->ccap < want_c || !ctx->cint.p) {
         TC_CK(ctx->cint.ensure(6 * want_c));
         TC_CK(ctx->cdbl.ensure(7 * want_c));
@@ -1484,7 +1489,7 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
       if (!f) return TC_ERR_UNSUPPORTED;
       rs = f(ctx, n);
       if (rs == TC_ERR_CAPACITY && ctx->ncell == 0) {
-        ctx->ccap = 2 * ctx->ccap + 1024;
+        grow_c = 2 * ctx->ccap + 1024;
         continue;
       }
       break;

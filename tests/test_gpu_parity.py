@@ -173,6 +173,22 @@ def test_runs_are_bitwise_deterministic():
     g.close()
 
 
+@pytest.mark.parametrize("variant", [tcb.VARIANT_TOP, tcb.VARIANT_JERKS])
+def test_context_reused_at_growing_n(variant):
+    """One context evaluating ever larger inputs (its cell, list and frontier capacities were
+    sized by the smaller calls) gives the same results, bit for bit, as a fresh context."""
+    g = tcb.Gravity(p=8, ncrit=64, theta=0.4, variant=variant, direct_below=0)
+    for n in (130, 2000, 8000, 32768, 100000):
+        x, y, z, vx, vy, vz, m = ics.plummer_kroupa(n, seed=50 + n % 7)
+        a = g.evaluate(x, y, z, m, vx, vy, vz)
+        f = tcb.Gravity(p=8, ncrit=64, theta=0.4, variant=variant, direct_below=0)
+        b = f.evaluate(x, y, z, m, vx, vy, vz)
+        f.close()
+        for k in a:
+            assert np.array_equal(a[k], b[k]), (n, k)
+    g.close()
+
+
 def test_large_n_against_direct_sum():
     n = 1 << 20
     x, y, z, vx, vy, vz, m = ics.plummer(n, seed=46)

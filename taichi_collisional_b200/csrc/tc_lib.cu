@@ -61,6 +61,14 @@ struct DBuf {
   }
 };
 
+// Source chunks per target leaf of the FP64 near field: 1 at large n; at small n (few target
+// leaves, ~48 bodies each) enough chunks for ~32 warps per SM, at most 16.  A function of n only,
+// so the direct launches and a captured graph of the same call sum in the same order.
+static inline int p2p_nsplit(int n) {
+  long long k = (148LL * 32 * 48 + n - 1) / (n > 0 ? n : 1);
+  return (int)(k < 1 ? 1 : k > 16 ? 16 : k);
+}
+
 // what a captured evaluation was recorded for (a call must match to replay it)
 struct TcGraphKey {
   int n = -1, mem = -1;
@@ -134,6 +142,7 @@ struct tc_ctx {
   // tc_direct_sums: bodies in caller order, targets, partial and final sums
   DBuf<double> ds_bod, ds_out;
   DBuf<double> diag;  // system diagnostics: block partials + the 9 results
+  DBuf<double> p2p_part;  // near-field partial sums per source chunk (few target leaves)
   // block-time-step integrator: accelerations, potential, 1/tau^4 sums; split counters, pair
   // positions, kick flags
   DBuf<double> ev_d;
@@ -870,8 +879,22 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     if (mixed_p2p)
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b,
                                                        cv, o);
-    else
-      k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o);
+    else {
+      // few target leaves (small n): split each leaf's sources over up to 16 warps, then fold
+      // the chunks in order (k_p2p_join); the split depends on n only, as in the graph path
+      const int ntl = (int)hs[1];
+      int nsplit = p2p_nsplit(n);
+      constexpr int NC = JERK ? 7 : 4;
+      if (nsplit > 1 && ctx->p2p_part.ensure((size_t)nsplit * NC * n) != cudaSuccess) nsplit = 1;
+      if (nsplit > 1) {
+        k_p2p<JERK><<<nblocks(ntl * nsplit, kP2PWarps), kP2PWarps * 32, 0, st>>>(
+            ctx->p2p_tl.p, ntl, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o, nullptr, nsplit, ctx->p2p_part.p, n);
+        k_p2p_join<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ntl, b, cv, o, nsplit, ctx->p2p_part.p, n);
+        ctx->launches++;
+      } else {
+        k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ntl, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o);
+      }
+    }
     ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[5], st);
@@ -999,9 +1022,20 @@ static void run_fmm_graph(tc_ctx* ctx, int n) {
     if (prm.precision != TC_PREC_FP64)
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o,
                                                        ctx->d_small + 1);
-    else
-      k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o,
-                                                 ctx->d_small + 1);
+    else {
+      const int nsplit = p2p_nsplit(n);
+      if (nsplit > 1) {  // the same chunks as the direct launches (p2p_part sized by graph_plan)
+        k_p2p<JERK><<<nblocks(ccap * nsplit, kP2PWarps), kP2PWarps * 32, 0, st>>>(
+            ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o, ctx->d_small + 1, nsplit,
+            ctx->p2p_part.p, n);
+        k_p2p_join<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, b, cv, o, nsplit, ctx->p2p_part.p, n,
+                                                        ctx->d_small + 1);
+        L++;
+      } else {
+        k_p2p<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o,
+                                                   ctx->d_small + 1);
+      }
+    }
   }
   L += 2;
   graph_check(ctx, "P2P");
@@ -1303,7 +1337,7 @@ tc_status tc_destroy(tc_ctx* ctx) {
   ctx->cell_pn.release(); ctx->cls_start.release(); ctx->cls_tl.release(); ctx->mlp_w.release();
   ctx->judge_idx.release(); ctx->judge_out.release();
   ctx->ds_bod.release(); ctx->ds_out.release(); ctx->ds_flags.release(); ctx->ds_idx.release(); ctx->ds_tgt.release();
-  ctx->tsum.release(); ctx->diag.release();
+  ctx->tsum.release(); ctx->diag.release(); ctx->p2p_part.release();
   ctx->ev_d.release(); ctx->ev_u.release(); ctx->ev_i.release(); ctx->ev_f.release();
   if (ctx->d_root) cudaFree(ctx->d_root);
   if (ctx->d_lv) cudaFree(ctx->d_lv);
@@ -1686,7 +1720,8 @@ static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* 
       ctx->hist.ensure(257 * ((mx + kRsTile - 1) / kRsTile + 1) + 1024) || ctx->m2l_start.ensure(ccap + 1) ||
       ctx->p2p_start.ensure(ccap + 1) || ctx->m2l_src.ensure(ctx->mcap + 1) || ctx->p2p_src.ensure(ctx->pcap + 1) ||
       ctx->m2l_tl.ensure(ccap) || ctx->p2p_tl.ensure(ccap) || ctx->leaves.ensure(ccap) ||
-      ctx->expn.ensure(ccap * NT * (jerk ? 4 : 2)) || ctx->bpart.ensure(6 * 148 * 4))
+      ctx->expn.ensure(ccap * NT * (jerk ? 4 : 2)) || ctx->bpart.ensure(6 * 148 * 4) ||
+      (p2p_nsplit(n) > 1 && ctx->p2p_part.ensure((size_t)p2p_nsplit(n) * (jerk ? 7 : 4) * N)))
     return;
   int sb = 1;
   while (((size_t)1 << sb) < ccap) sb++;

@@ -79,14 +79,24 @@ template <bool JERK>
 __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p(const int* __restrict__ tlist, int ntl,
                                                         const int* __restrict__ tstart, const int* __restrict__ src,
                                                         const TcBodies b, const TcCells c, TcOut out,
-    const unsigned* ntldev = nullptr) {
+                                                        const unsigned* ntldev = nullptr, int nsplit = 1,
+                                                        double* __restrict__ part = nullptr, int pstride = 0) {
+  // Work item k: target leaf k / nsplit, chunk k % nsplit of its source-cell list.  With
+  // nsplit == 1 the item adds into out; otherwise it stores its partial sums in
+  // part[(chunk * NC + component) * pstride + body] for k_p2p_join (few target leaves: more
+  // warps than leaves, the chunks folded afterwards in a fixed order).
   if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
+  constexpr int NC = JERK ? 7 : 4;
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
-    int t = tlist[k];
+  const long long nitem = (long long)ntl * nsplit;
+  for (long long k = (long long)blockIdx.x * kP2PWarps + w; k < nitem; k += (long long)gridDim.x * kP2PWarps) {
+    const int kk = (int)(k / nsplit), chunk = (int)(k % nsplit);
+    int t = tlist[kk];
     if (!c.has_sink[t]) continue;
     int tb = c.begin[t], nt = c.nbody[t];
-    int sb = tstart[t], se = tstart[t + 1];
+    const int sb0 = tstart[t], len = tstart[t + 1] - sb0;
+    const int sb = sb0 + (int)((long long)len * chunk / nsplit);
+    const int se = sb0 + (int)((long long)len * (chunk + 1) / nsplit);
     for (int t0 = 0; t0 < nt; t0 += 32) {
       // up to 32 targets per pass; a last pass of r <= 16 targets runs floor(32 / r) lane
       // groups of r lanes, each over every ng-th source
@@ -110,16 +120,67 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p(const int* __restrict__ 
         }
       }
       a.add_groups(gsz, ng, grp);
-      if (vi && grp == 0 && (b.flags[i] & 1)) {
-        out.pot[i] += a.pot;
-        out.ax[i] += a.ax;
-        out.ay[i] += a.ay;
-        out.az[i] += a.az;
-        if (JERK) {
-          out.jx[i] += a.jx;
-          out.jy[i] += a.jy;
-          out.jz[i] += a.jz;
+      if (vi && grp == 0) {
+        if (nsplit > 1) {
+          double* pp = part + (size_t)chunk * NC * pstride + i;
+          pp[0] = a.pot;
+          pp[(size_t)pstride] = a.ax;
+          pp[2 * (size_t)pstride] = a.ay;
+          pp[3 * (size_t)pstride] = a.az;
+          if (JERK) {
+            pp[4 * (size_t)pstride] = a.jx;
+            pp[5 * (size_t)pstride] = a.jy;
+            pp[6 * (size_t)pstride] = a.jz;
+          }
+        } else if (b.flags[i] & 1) {
+          out.pot[i] += a.pot;
+          out.ax[i] += a.ax;
+          out.ay[i] += a.ay;
+          out.az[i] += a.az;
+          if (JERK) {
+            out.jx[i] += a.jx;
+            out.jy[i] += a.jy;
+            out.jz[i] += a.jz;
+          }
         }
+      }
+    }
+  }
+}
+
+// Folds the nsplit chunk partials of k_p2p (chunk 0 first) into the sink bodies of each target
+// leaf: one warp per leaf, one lane per body.
+template <bool JERK>
+__global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_join(const int* __restrict__ tlist, int ntl,
+                                                             const TcBodies b, const TcCells c, TcOut out,
+                                                             int nsplit, const double* __restrict__ part,
+                                                             int pstride, const unsigned* ntldev = nullptr) {
+  if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
+  constexpr int NC = JERK ? 7 : 4;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
+    const int t = tlist[k];
+    if (!c.has_sink[t]) continue;
+    const int tb = c.begin[t], nt = c.nbody[t];
+    for (int u = lane; u < nt; u += 32) {
+      const int i = tb + u;
+      if (!(b.flags[i] & 1)) continue;
+      double v[NC];
+#pragma unroll
+      for (int q = 0; q < NC; q++) v[q] = 0.0;
+      for (int ch = 0; ch < nsplit; ch++) {
+        const double* pp = part + (size_t)ch * NC * pstride + i;
+#pragma unroll
+        for (int q = 0; q < NC; q++) v[q] += pp[(size_t)q * pstride];
+      }
+      out.pot[i] += v[0];
+      out.ax[i] += v[1];
+      out.ay[i] += v[2];
+      out.az[i] += v[3];
+      if (JERK) {
+        out.jx[i] += v[4];
+        out.jy[i] += v[5];
+        out.jz[i] += v[6];
       }
     }
   }

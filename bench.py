@@ -9,6 +9,7 @@ seeded synthetic data (no dataset is involved) and stay resident in HBM; the sta
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
   python bench.py --evolve N [--steps K --warmup W]   # the block-time-step integrator instead
+  python bench.py --diagnostics N [--steps K --warmup W]   # the energy / centre-of-mass sums
 
 N > 1 (torchrun, one process per GPU): independent replicas, no data-path collective; the
 timed region is bracketed by barriers and the slowest rank's device time is reported.
@@ -52,6 +53,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each evaluation's kernels directly instead of replaying one captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--diagnostics", type=int, default=0, metavar="N",
+                    help="time the system diagnostics (energies, centre of mass) over N bodies instead")
     ap.add_argument("--evolve", type=int, default=0, metavar="N",
                     help="time one step of the HOLD block-time-step integrator on N bodies instead")
     return ap.parse_args()
@@ -240,6 +243,47 @@ def run_evolve(args):
     g.close()
 
 
+def run_diagnostics(args):
+    """tc_system_diagnostics over N resident bodies (kinetic and potential energy, mass, centre of
+    mass and its velocity: 64 algorithmic bytes read per body); CUDA events around K calls, the
+    roofline against the measured HBM copy bandwidth."""
+    import torch
+    import taichi_collisional_b200 as tcb
+    n = args.diagnostics
+    x, y, z, vx, vy, vz, m = make_ics(n, 2028)
+    pot = np.random.default_rng(5).random(n)
+    arrs = [torch.tensor(a, dtype=torch.float64, device="cuda") for a in (m, x, y, z, vx, vy, vz, pot)]
+    g = tcb.Gravity(p=8, ncrit=64, theta=0.4, variant=tcb.VARIANT_TOP, precision=tcb.PREC_FP64)
+    for _ in range(args.warmup):
+        d = g.system_diagnostics(*arrs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        d = g.system_diagnostics(*arrs)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    gbs = 64.0 * n / (ms * 1e-3) / 1e9
+    peak = None
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peak = json.load(f).get("hbm_gbs")
+    except (OSError, ValueError):
+        pass
+    line = {"metric": "bodies/s of the system diagnostics (energies, centre of mass)", "impl": "ours",
+            "value": n / (ms * 1e-3), "unit": "bodies/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "dtype": "f64 (double-double sums)",
+            "data": "synthetic (seeded Plummer/Kroupa)",
+            "config": {"workload": "system_diagnostics_plummer_kroupa_N%d" % n, "n": n,
+                       "l2": "inputs larger than L2 (8 x 8 B per body)" if 64 * n > 126e6 else "inputs fit in L2"},
+            "roofline": {"kernel": "k_sys_diag_part", "bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": gbs / peak if peak else None, "work": "64 B read per body (call: both kernels)"},
+            "result": d}
+    print(json.dumps(line))
+    g.close()
+
+
 def error_stats(out, idx_t, ref):
     """RMS and 99th percentile of |a - a_ref| / |a_ref| and |j - j_ref| / |j_ref| at the
     targets idx_t (out: device tensors of one evaluation, ref: direct sums at those bodies)."""
@@ -263,6 +307,9 @@ def main():
         return
     if args.evolve:
         run_evolve(args)
+        return
+    if args.diagnostics:
+        run_diagnostics(args)
         return
     import datetime
 

@@ -70,7 +70,7 @@ __device__ __forceinline__ void tc_diag_block_reduce(TcDD (*sh)[kDiagThreads], T
 }
 
 // One double-double partial per block and quantity: part[(block * kDiagQ + q) * 2 + {0, 1}].
-__global__ void __launch_bounds__(kDiagThreads) k_sys_diag_part(
+__global__ void __launch_bounds__(kDiagThreads, 3) k_sys_diag_part(
     int n, const double* __restrict__ m, const double* __restrict__ x, const double* __restrict__ y,
     const double* __restrict__ z, const double* __restrict__ vx, const double* __restrict__ vy,
     const double* __restrict__ vz, const double* __restrict__ pot, double* __restrict__ part) {
@@ -79,15 +79,22 @@ __global__ void __launch_bounds__(kDiagThreads) k_sys_diag_part(
 #pragma unroll
   for (int q = 0; q < kDiagQ; q++) acc[q] = {0.0, 0.0};
   const int stride = gridDim.x * kDiagThreads;
-  for (int i = blockIdx.x * kDiagThreads + threadIdx.x; i < n; i += stride) {
-    const double mi = m[i], ux = vx[i], uy = vy[i], uz = vz[i];
+  // software-pipelined: the next body's eight values are loaded before this body is folded, so
+  // each thread keeps two bodies' loads in flight (same order of the sums as a plain loop)
+  int i = blockIdx.x * kDiagThreads + threadIdx.x;
+  double cm = 0, cx = 0, cy = 0, cz = 0, cu = 0, cv = 0, cw = 0, cp = 0;
+  if (i < n) { cm = m[i]; cx = x[i]; cy = y[i]; cz = z[i]; cu = vx[i]; cv = vy[i]; cw = vz[i]; cp = pot[i]; }
+  for (; i < n; i += stride) {
+    const double mi = cm, px = cx, py = cy, pz = cz, ux = cu, uy = cv, uz = cw, pi = cp;
+    const int j = i + stride;
+    if (j < n) { cm = m[j]; cx = x[j]; cy = y[j]; cz = z[j]; cu = vx[j]; cv = vy[j]; cw = vz[j]; cp = pot[j]; }
     const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy)), __dmul_rn(uz, uz));
     acc[0] = tc_dd_add(acc[0], __dmul_rn(__dmul_rn(mi, v2), 0.5));
-    acc[1] = tc_dd_add(acc[1], __dmul_rn(__dmul_rn(mi, pot[i]), 0.5));
+    acc[1] = tc_dd_add(acc[1], __dmul_rn(__dmul_rn(mi, pi), 0.5));
     acc[2] = tc_dd_add(acc[2], mi);
-    acc[3] = tc_dd_add(acc[3], tc_dd_prod(mi, x[i]));
-    acc[4] = tc_dd_add(acc[4], tc_dd_prod(mi, y[i]));
-    acc[5] = tc_dd_add(acc[5], tc_dd_prod(mi, z[i]));
+    acc[3] = tc_dd_add(acc[3], tc_dd_prod(mi, px));
+    acc[4] = tc_dd_add(acc[4], tc_dd_prod(mi, py));
+    acc[5] = tc_dd_add(acc[5], tc_dd_prod(mi, pz));
     acc[6] = tc_dd_add(acc[6], tc_dd_prod(mi, ux));
     acc[7] = tc_dd_add(acc[7], tc_dd_prod(mi, uy));
     acc[8] = tc_dd_add(acc[8], tc_dd_prod(mi, uz));

@@ -1961,7 +1961,7 @@ tc_status tc_system_diagnostics(tc_ctx* ctx, int n, const double* m, const doubl
   TC_CK(cudaSetDevice(ctx->prm.device));
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->prm.device);
-  const int nblk = std::max(1, std::min(4 * nsm, (n + kDiagThreads - 1) / kDiagThreads));
+  const int nblk = std::max(1, std::min(3 * nsm, (n + kDiagThreads - 1) / kDiagThreads));  // one wave: 3 CTAs per SM
   TC_CK(ctx->diag.ensure((size_t)nblk * kDiagQ * 2 + kDiagQ));
   double* res = ctx->diag.p + (size_t)nblk * kDiagQ * 2;
   cudaStream_t st = ctx->stream;

@@ -869,9 +869,21 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   }
   if (hs[1] > 0 && ctx->steps) {
     if constexpr (!JERK) {
-      k_p2p_steps<<<nblocks(hs[1], kP2PWarps), kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p,
+      const int ntl = (int)hs[1];
+      int nsplit = p2p_nsplit(n);  // few target leaves: source chunks folded in order, as k_p2p
+      if (nsplit > 1 && ctx->p2p_part.ensure((size_t)nsplit * 5 * n) != cudaSuccess) nsplit = 1;
+      if (nsplit > 1) {
+        k_p2p_steps<<<nblocks(ntl * nsplit, kP2PWarps), kP2PWarps * 32, 0, st>>>(
+            ctx->p2p_tl.p, ntl, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o, ctx->dt_param, ctx->tsum.p, nsplit,
+            ctx->p2p_part.p, n);
+        k_p2p_steps_join<<<nblocks(ntl, kP2PWarps), kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ntl, b, cv, o,
+                                                                             ctx->tsum.p, nsplit, ctx->p2p_part.p, n);
+        ctx->launches++;
+      } else {
+        k_p2p_steps<<<nblocks(ntl, kP2PWarps), kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ntl, ctx->p2p_start.p,
                                                                         ctx->p2p_src.p, b, cv, o, ctx->dt_param,
                                                                         ctx->tsum.p);
+      }
       ctx->launches++;
     }
   } else if (hs[1] > 0) {

@@ -307,14 +307,23 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_steps(const int* __restr
                                                               const int* __restrict__ tstart,
                                                               const int* __restrict__ src, const TcBodies b,
                                                               const TcCells c, TcOut out, double dtp,
-                                                              double* __restrict__ tsum) {
+                                                              double* __restrict__ tsum, int nsplit = 1,
+                                                              double* __restrict__ part = nullptr,
+                                                              int pstride = 0) {
+  // work item k: target leaf k / nsplit, chunk k % nsplit of its source cells (whole cells, so
+  // the per-cell time-step terms are unchanged); with nsplit > 1 the chunk's pot, acc and
+  // 1/tau^4 sums go to part[(chunk * 5 + component) * pstride + body] for k_p2p_steps_join
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double dts = dtp / 1.41421356237309504880;  // dt_param / M_SQRT2
-  for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
+  const long long nitem = (long long)ntl * nsplit;
+  for (long long kw = (long long)blockIdx.x * kP2PWarps + w; kw < nitem; kw += (long long)gridDim.x * kP2PWarps) {
+    const int k = (int)(kw / nsplit), chunk = (int)(kw % nsplit);
     const int t = tlist[k];
     if (!c.has_sink[t]) continue;
     const int tb = c.begin[t], nt = c.nbody[t];
-    const int sb = tstart[t], se = tstart[t + 1];
+    const int sb0 = tstart[t], len = tstart[t + 1] - sb0;
+    const int sb = sb0 + (int)((long long)len * chunk / nsplit);
+    const int se = sb0 + (int)((long long)len * (chunk + 1) / nsplit);
     for (int t0 = 0; t0 < nt; t0 += 32) {
       const bool vi = t0 + lane < nt;
       const int i = tb + (vi ? t0 + lane : 0);
@@ -361,13 +370,48 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_steps(const int* __restr
         tmin *= tmin;
         ts += 1.0 / tmin;
       }
-      if (vi && (b.flags[i] & 1)) {
+      if (vi && nsplit > 1) {
+        double* pp = part + (size_t)chunk * 5 * pstride + i;
+        pp[0] = pot;
+        pp[(size_t)pstride] = ax;
+        pp[2 * (size_t)pstride] = ay;
+        pp[3 * (size_t)pstride] = az;
+        pp[4 * (size_t)pstride] = ts;
+      } else if (vi && (b.flags[i] & 1)) {
         out.pot[i] += pot;
         out.ax[i] += ax;
         out.ay[i] += ay;
         out.az[i] += az;
         tsum[i] += ts;
       }
+    }
+  }
+}
+
+// Folds the chunks of k_p2p_steps (chunk 0 first) into the sink bodies of each target leaf.
+__global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_steps_join(const int* __restrict__ tlist, int ntl,
+                                                                   const TcBodies b, const TcCells c, TcOut out,
+                                                                   double* __restrict__ tsum, int nsplit,
+                                                                   const double* __restrict__ part, int pstride) {
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
+    const int t = tlist[k];
+    if (!c.has_sink[t]) continue;
+    const int tb = c.begin[t], nt = c.nbody[t];
+    for (int u = lane; u < nt; u += 32) {
+      const int i = tb + u;
+      if (!(b.flags[i] & 1)) continue;
+      double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      for (int ch = 0; ch < nsplit; ch++) {
+        const double* pp = part + (size_t)ch * 5 * pstride + i;
+#pragma unroll
+        for (int q = 0; q < 5; q++) v[q] += pp[(size_t)q * pstride];
+      }
+      out.pot[i] += v[0];
+      out.ax[i] += v[1];
+      out.ay[i] += v[2];
+      out.az[i] += v[3];
+      tsum[i] += v[4];
     }
   }
 }

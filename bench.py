@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true",
                     help="launch each evaluation's kernels directly instead of replaying one captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget", type=float, default=1500.0,
+                    help="--impl reference: stop timing further steps once this many seconds have passed")
     ap.add_argument("--diagnostics", type=int, default=0, metavar="N",
                     help="time the system diagnostics (energies, centre of mass) over N bodies instead")
     ap.add_argument("--evolve", type=int, default=0, metavar="N",
@@ -141,54 +143,125 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------
 # CPU baseline: the reference's own code (oracle/_ref) or the oracle port
 # ---------------------------------------------------------------------------------------
-def cpu_baseline(n_sample, p, theta, ncrit, steps=1, warmup=0):
+def cpu_runner(x, y, z, vx, vy, vz, m, p, theta, ncrit):
+    """One force evaluation (acc + pot + jerk, theta MAC) by the reference's own OpenMP +
+    vectorclass build on all host cores (oracle/_ref), or by the oracle port when that build is
+    absent.  Returns (run() -> dict of outputs, kind, cores)."""
     import oracle
     cores = os.cpu_count() or 1
-    x, y, z, vx, vy, vz, m = make_ics(n_sample, 2026)
     if oracle.ref_available(oracle.VARIANT_JERKS, p):
-        kind = "reference"
         os.environ.setdefault("OMP_PROC_BIND", "close")
 
         def run():
-            oracle.ref_evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, variant=oracle.VARIANT_JERKS,
-                                seed=1, nthreads=cores)
-    else:
-        kind = "port"
-        cores = 1
+            return oracle.ref_evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit,
+                                       variant=oracle.VARIANT_JERKS, seed=1, nthreads=cores)
+        return run, "reference", cores
 
-        def run():
-            oracle.evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, variant=oracle.VARIANT_JERKS,
-                            direct_below=0)
-    for _ in range(warmup):
-        run()
+    def run_port():
+        return oracle.evaluate(x, y, z, m, vx, vy, vz, p=p, theta=theta, ncrit=ncrit, variant=oracle.VARIANT_JERKS,
+                               direct_below=0)
+    return run_port, "port", 1
+
+
+def cpu_baseline(n_sample, p, theta, ncrit, gpu_check=None):
+    """The CPU build on a bounded sample of the workload (one evaluation of n_sample bodies).
+    With gpu_check(x, y, z, vx, vy, vz, m, shift_u) -> outputs, also states how far this
+    library's FP64 form is from the reference's own output on the same sample (max over
+    particles of the relative acceleration, potential and jerk differences)."""
+    import oracle
+    x, y, z, vx, vy, vz, m = make_ics(n_sample, 2026)
+    run, kind, cores = cpu_runner(x, y, z, vx, vy, vz, m, p, theta, ncrit)
     t0 = time.perf_counter()
-    for _ in range(steps):
-        run()
+    ref = run()
     dt = time.perf_counter() - t0
-    sample = ("%d force evaluation(s) (acc+pot+jerk, theta-MAC) of a N=%d Plummer/Kroupa sample, p=%d, theta=%g, "
-              "ncrit=%d; the per-particle cost grows ~log N, so the N=4M rate is lower" %
-              (steps, n_sample, p, theta, ncrit))
-    return {"value": n_sample * steps / dt, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
-            "seconds": dt}
+    sample = ("1 force evaluation (acc+pot+jerk, theta-MAC) of a N=%d Plummer/Kroupa sample, p=%d, theta=%g, "
+              "ncrit=%d; the per-particle cost grows ~log N, so the N=4M rate is lower (bench.py --impl reference "
+              "times the full N)" % (n_sample, p, theta, ncrit))
+    res = {"value": n_sample / dt, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+    if gpu_check is not None and kind == "reference":
+        su = oracle.ref_shift_uniforms(oracle.VARIANT_JERKS, p, 1)
+        got = gpu_check(x, y, z, vx, vy, vz, m, su)
+        par = {"n": n_sample, "form": "fp64", "against": "the reference's own evaluation (oracle/_ref)"}
+        for key, comps in (("acc", ("ax", "ay", "az")), ("jerk", ("jx", "jy", "jz"))):
+            a = np.stack([got[c] for c in comps], 1)
+            b = np.stack([ref[c] for c in comps], 1)
+            e = np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+            par[key + "_max_rel"] = float(e.max())
+        par["pot_max_rel"] = float(np.max(np.abs(got["pot"] - ref["pot"]) / np.abs(ref["pot"])))
+        res["parity"] = par
+    return res
 
 
 def run_reference(args, rank):
+    """The reference arm: the reference's own CPU build (oracle/_ref, compiled from its sources)
+    on the full workload -- the same N, distribution, p, theta, ncrit and step (kick-drift, one
+    force evaluation with jerks, kick) as the GPU arm -- on every host core.  Each step is one
+    full evaluation at N; steps beyond the time budget are not run, and the line states the
+    number actually timed."""
     if rank != 0:
         return
     try:
-        cb = cpu_baseline(CPU_SAMPLE_N, args.p, WORKLOAD["theta"], WORKLOAD["ncrit"], steps=args.steps,
-                          warmup=args.warmup)
+        n, p = args.n, args.p
+        x, y, z, vx, vy, vz, m = make_ics(n, 2026)
+        run, kind, cores = cpu_runner(x, y, z, vx, vy, vz, m, p, WORKLOAD["theta"], WORKLOAD["ncrit"])
+        dt = 1.0 / 4096
+        acc = {"ax": np.zeros(n), "ay": np.zeros(n), "az": np.zeros(n)}
+
+        def step():
+            for c in "xyz":
+                vel = {"x": vx, "y": vy, "z": vz}[c]
+                pos = {"x": x, "y": y, "z": z}[c]
+                vel += 0.5 * dt * acc["a" + c]
+                pos += dt * vel
+            out = run()
+            for c in "xyz":
+                acc["a" + c][:] = out["a" + c]
+                vel = {"x": vx, "y": vy, "z": vz}[c]
+                vel += 0.5 * dt * acc["a" + c]
+
+        out = run()
+        for c in "xyz":
+            acc["a" + c][:] = out["a" + c]
+        t_start = time.perf_counter()
+        warm = 0
+        for _ in range(min(args.warmup, 1)):
+            step()
+            warm += 1
+        times = []
+        while len(times) < args.steps:
+            t0 = time.perf_counter()
+            step()
+            times.append(time.perf_counter() - t0)
+            if time.perf_counter() - t_start + times[-1] > args.ref_budget:
+                break
     except Exception as e:  # pragma: no cover - reported, not hidden
         print(json.dumps({"impl": "reference", "unavailable": "reference CPU build failed: %s" % e}))
         return
-    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * cb["seconds"] / args.steps,
+    k = len(times)
+    sec = sum(times)
+    value = n * k / sec
+    note = ("%d of the %d requested steps timed (time budget %.0f s; one untimed warm-up step of the %d requested)"
+            % (k, args.steps, args.ref_budget, args.warmup)) if k < args.steps or warm < args.warmup else None
+    sample = ("%d full step(s) at N=%d (kick-drift, one force evaluation acc+pot+jerk with the theta MAC, kick), "
+              "p=%d, theta=%g, ncrit=%d, %s" % (k, n, p, WORKLOAD["theta"], WORKLOAD["ncrit"],
+                                                "the reference's OpenMP + vectorclass build" if kind == "reference"
+                                                else "the oracle port"))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": k, "warmup": warm, "ms_per_step": 1e3 * sec / k,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Plummer/Kroupa sample)",
-            "config": dict(WORKLOAD, n_sample=CPU_SAMPLE_N),
-            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
-            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "data": "synthetic (seeded Plummer sphere, Kroupa IMF masses)",
+            "config": workload_config(n, p, args.gpus),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "seconds_per_step": times}
+    if note:
+        line["note"] = note
     print(json.dumps(line))
+
+
+def workload_config(n, p, world):
+    """The workload both arms are timed on (identical for the reference arm and this one)."""
+    return dict(WORKLOAD, n=n, p=p, parallelism="replicas" if world > 1 else "single")
 
 
 EVOLVE_CPU_SAMPLE_N = 1024
@@ -462,8 +535,13 @@ def main():
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb = cpu_baseline(CPU_SAMPLE_N, p, WORKLOAD["theta"], WORKLOAD["ncrit"])
-            cb.pop("seconds", None)
+            def gpu_fp64(xs, ys, zs, vxs, vys, vzs, ms_, su):
+                gs = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
+                                 precision=tcb.PREC_FP64, device=local, shift_u=su, direct_below=0)
+                o = gs.evaluate(xs, ys, zs, ms_, vxs, vys, vzs)
+                gs.close()
+                return o
+            cb = cpu_baseline(CPU_SAMPLE_N, p, WORKLOAD["theta"], WORKLOAD["ncrit"], gpu_check=gpu_fp64)
         except Exception as e:
             cb = {"value": None, "error": str(e)}
     if rank == 0:
@@ -471,9 +549,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded Plummer sphere, Kroupa IMF masses)",
-                "config": dict(WORKLOAD, n=n, p=p, precision=args.precision,
-                               parallelism="replicas" if world > 1 else "single",
-                               evaluation="one CUDA graph replay" if g.graph_ready() else "direct launches"),
+                "config": workload_config(n, p, world),
+                "form": {"precision": args.precision,
+                         "evaluation": "one CUDA graph replay" if g.graph_ready() else "direct launches"},
                 "e2e": e2e, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cb, "clocks": clocks,
                 "accuracy": accuracy,
                 "fp64_form": fp64,

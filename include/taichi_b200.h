@@ -100,16 +100,21 @@ tc_status tc_destroy(tc_ctx* ctx);
 /* Run work on this CUDA stream (cudaStream_t passed as void*; NULL = legacy default). */
 tc_status tc_set_stream(tc_ctx* ctx, void* stream);
 
-/* The top tree's own traversal: the error-controlled MAC of horizontalPassHigh
- * (traverse_eager.h:61-148), which get_force_and_potential uses (integrator.h:459-562:
- * horizontalPass(cells, cells, 1, get_steps)), preceded by the reference's low-order pre-pass
- * (integrator.h:476-493, kernel_fast_lean.h:1358-1647) that estimates each body's acceleration
- * (acc_old) for the cells' min_acc.  force_accuracy is the reference's global (exafmm.h:95,
- * default 2e-7).  With on != 0, tc_evaluate and tc_evaluate_steps of this context build their
- * lists with it instead of the theta MAC.  The top tree only (TC_ERR_UNSUPPORTED for the jerks
- * tree, whose traversal is theta only); not captured by tc_set_graph.  As the reference's
- * first call: acc_old starts at zero every evaluation (the reference's global body array
- * carries it from call to call). */
+/* Each tree's own traversal: the error-controlled MAC that get_force_and_potential uses
+ * (horizontalPass(cells, cells, 1, get_steps)), preceded by the reference's low-order pre-pass
+ * that estimates each body's acceleration (acc_old) for the cells' min_acc.
+ *   top tree:   integrator.h:459-562; pre-pass integrator.h:476-493, kernel_fast_lean.h:1358-1647
+ *               (acc_old = sum of scalar estimates); MAC horizontalPassHigh, traverse_eager.h:
+ *               61-148 (both f1 and f2, pre-test |d| > Ra + Rb, small cells to P2P);
+ *   jerks tree: taichi_with_jerks/integrator.h:308-432; pre-pass integrator.h:326-360,
+ *               kernel_fast_lean.h:1446-1780 (acc_old = |F| of the order-2 FMM, its near field
+ *               in FP32); MAC taichi_with_jerks/traverse_eager.h:59-122 (one-sided f2 only,
+ *               pre-test 0.4 |d|^2 > (Ra + Rb)^2).
+ * force_accuracy is the reference's global (top exafmm.h:95, default 2e-7; jerks
+ * taichi_with_jerks/exafmm.h:99, default 2e-8).  With on != 0, tc_evaluate and
+ * tc_evaluate_steps of this context build their lists with it instead of the theta MAC.  Not
+ * captured by tc_set_graph.  As the reference's first call: acc_old starts at zero every
+ * evaluation (the reference's global body array carries it from call to call). */
 tc_status tc_set_error_mac(tc_ctx* ctx, int on, double force_accuracy);
 /* The pre-pass's acc_old of the last evaluation with the error MAC, per body (caller order, host). */
 tc_status tc_get_acc_old(tc_ctx* ctx, double* acc_old);
@@ -276,10 +281,13 @@ double tc_probe_peak(tc_ctx* ctx, int kind);
  * Its working storage is one fixed static device array per GPU that loads the library
  * (held until the process exits), sized for TC_NOALLOC_MAX_N bodies; larger n returns
  * TC_ERR_CAPACITY without doing any work.  The first call on a device looks that array
- * up (cudaGetSymbolAddress) with the caller's current device; make that first call before
- * any stream capture.  Every call reuses the same array, and every entry a call reads is
- * written earlier in that same call, so nothing has to be cleared between calls; calls that
- * overlap on the GPU (different streams, or another host thread) race on the array. */
+ * up (cudaGetSymbolAddress) with the caller's current device, under a lock, and keeps the
+ * address for the life of the process; make that first call before any stream capture, and
+ * do not call this entry point again on a device after cudaDeviceReset there (the kept
+ * address belongs to the reset context).  Every call reuses the same array, and every entry a
+ * call reads is written earlier in that same call, so nothing has to be cleared between
+ * calls; calls that overlap on the GPU (different streams, or another host thread) race on
+ * the array.  The library's own code never uses this array: contexts keep their own storage. */
 #define TC_NOALLOC_MAX_N 16384
 tc_status tc_evaluate_direct_noalloc(int n, const double* x, const double* y, const double* z,
                                      const double* vx, const double* vy, const double* vz,

@@ -49,11 +49,22 @@ def _f64(a):
     return None if a is None else np.ascontiguousarray(a, dtype=np.float64)
 
 
+def reference_dir():
+    """The reference source tree: $TC_REFERENCE, else a `reference` directory beside the
+    repository checkout; None when neither holds the reference's exafmm.h (the GPU host has
+    only the prebuilt oracle/_ref libraries)."""
+    cands = [os.environ.get("TC_REFERENCE"), os.path.join(HERE, "..", "..", "reference")]
+    for c in cands:
+        if c and os.path.isfile(os.path.join(c, "exafmm.h")):
+            return os.path.abspath(c)
+    return None
+
+
 def build():
     """Compile liboracle.so (and, when the reference tree is present, oracle/_ref)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "oracle"])
-    if os.path.isdir(os.environ.get("TC_REFERENCE", "/root/reference")):
-        ref = "REF=" + os.environ.get("TC_REFERENCE", "/root/reference")
+    if reference_dir():
+        ref = "REF=" + reference_dir()
         subprocess.check_call(["make", "-s", "-j8", "-C", HERE, "ref", ref])
         # the reference's integrator over this repository's force evaluation needs the CUDA library
         if os.path.exists(os.path.join(HERE, "..", "taichi_collisional_b200", "libtaichi_b200.so")):
@@ -259,6 +270,12 @@ def ref_lib(variant, p):
         L.tcr_list.argtypes = [C.c_int, _ip, _ip]
         L.tcr_list.restype = C.c_longlong
         L.tcr_shift_uniforms.argtypes = [C.c_long, _dp]
+        if hasattr(L, "tcr_evaluate_high_jerks"):
+            L.tcr_evaluate_high_jerks.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_long,
+                                                                          C.c_int] + [_dp] * 7
+            L.tcr_evaluate_high_jerks.restype = C.c_int
+            L.tcr_acc_old.argtypes = [_dp]
+            L.tcr_min_acc.argtypes = [_dp, _dp]
         if hasattr(L, "tcr_evaluate_high"):
             L.tcr_evaluate_high.argtypes = [C.c_int] + [_dp] * 7 + [_u8p, C.c_double, C.c_int, C.c_int] + [_dp] * 4
             L.tcr_evaluate_high.restype = C.c_int
@@ -326,6 +343,28 @@ def ref_evaluate_high(x, y, z, m, *, p, ncrit, force_accuracy, nthreads=1, flags
     nc = L.tcr_evaluate_high(n, _d(x), _d(y), _d(z), None, None, None, _d(m),
                              None if fl is None else fl.ctypes.data_as(_u8p), force_accuracy, ncrit, nthreads,
                              *[_d(out[k]) for k in ("ax", "ay", "az", "pot")])
+    out["ncell"] = nc
+    out["acc_old"] = np.zeros(n)
+    L.tcr_acc_old(_d(out["acc_old"]))
+    out["min_acc"] = np.zeros(nc)
+    out["pn"] = np.zeros((nc, p + 1))
+    L.tcr_min_acc(_d(out["min_acc"]), _d(out["pn"]))
+    return out
+
+
+def ref_evaluate_high_jerks(x, y, z, m, vx, vy, vz, *, p, ncrit, force_accuracy, seed=1, nthreads=1, flags=None):
+    """The jerks tree's own get_force_and_potential (taichi_with_jerks/integrator.h:308-432,
+    without its direct branch): low-order pre-pass, then its one-sided error-controlled MAC.
+    Returns the outputs, acc_old (caller order), per-cell min_acc and Pn."""
+    L = ref_lib(VARIANT_JERKS, p)
+    n = len(x)
+    x, y, z, m = map(_f64, (x, y, z, m))
+    vx, vy, vz = map(_f64, (vx, vy, vz))
+    out = {k: np.zeros(n) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
+    fl = None if flags is None else np.ascontiguousarray(flags, dtype=np.uint8)
+    nc = L.tcr_evaluate_high_jerks(n, _d(x), _d(y), _d(z), _d(vx), _d(vy), _d(vz), _d(m),
+                                   None if fl is None else fl.ctypes.data_as(_u8p), force_accuracy, ncrit, seed,
+                                   nthreads, *[_d(out[k]) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")])
     out["ncell"] = nc
     out["acc_old"] = np.zeros(n)
     L.tcr_acc_old(_d(out["acc_old"]))

@@ -31,7 +31,7 @@ static const int kJerks = 0;
 static Cells g_cells;
 static std::vector<int> g_list_t[2], g_list_s[2];
 static int g_init = 0;
-static int g_high = 0;  // last evaluation used the error-controlled MAC (top tree)
+static int g_high = 0;  // last evaluation used the error-controlled MAC
 
 static double now_s() {
   struct timeval tv;
@@ -93,6 +93,40 @@ static void record_high(Cell* Ci, Cell* Cj) {
     int k = ((Ci->NBODY <= 2 && Cj->NBODY <= 8) || (Cj->NBODY <= 2 && Ci->NBODY <= 8)) ? 1 : 0;
     g_list_t[k].push_back(ci);
     g_list_s[k].push_back(cj);
+  } else if (Ci->NCHILD == 0 && Cj->NCHILD == 0) {
+    g_list_t[1].push_back(ci);
+    g_list_s[1].push_back(cj);
+  } else if (Cj->NCHILD == 0 || (Ci->R >= Cj->R && Ci->NCHILD != 0)) {
+    for (Cell* c = Ci->CHILD; c != Ci->CHILD + Ci->NCHILD; c++) record_high(c, Cj);
+  } else {
+    for (Cell* c = Cj->CHILD; c != Cj->CHILD + Cj->NCHILD; c++) record_high(Ci, c);
+  }
+}
+#else
+// same decisions as the jerks tree's horizontalPassHigh (taichi_with_jerks/traverse_eager.h:
+// 59-122) on the reference's own cells: the one-sided test f2 only, its pre-test
+// |d|^2 0.4 > (Ra + Rb)^2, and no small-cell P2P rule
+static void record_high(Cell* Ci, Cell* Cj) {
+  real_t d[3];
+  for (int k = 0; k < 3; k++) d[k] = Ci->X[k] - Cj->X[k];
+  real_t R2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+  real_t f2 = 10;
+  real_t Ra = Ci->R, Rb = Cj->R, Ra_p_Rb = Ra + Rb;
+  if (R2 * 0.4 > Ra_p_Rb * Ra_p_Rb) {
+    real_t R = sqrt(R2), Rp = std::pow(R, -(P + 1)), pa = 1, Eba = 0;
+    for (int k = 0; k <= P; k++) {
+      real_t fac = combinator_coef[P][k];
+      Eba += Cj->Pn[P - k] * pa * fac;
+      pa *= Ra;
+    }
+    real_t fac = 8 * fmax(Ra, Rb) * Rp;
+    Eba *= fac;
+    f2 = Eba / (force_accuracy * Ci->min_acc);
+  }
+  int ci = (int)(Ci - &g_cells[0]), cj = (int)(Cj - &g_cells[0]);
+  if (f2 < 1) {
+    g_list_t[0].push_back(ci);
+    g_list_s[0].push_back(cj);
   } else if (Ci->NCHILD == 0 && Cj->NCHILD == 0) {
     g_list_t[1].push_back(ci);
     g_list_s[1].push_back(cj);
@@ -164,6 +198,19 @@ int tcr_evaluate_high_steps(int n, const double* x, const double* y, const doubl
   return run(n, x, y, z, vx, vy, vz, m, flags, 0.4, nc, 0, nthreads, ax, ay, az, pot, nullptr, nullptr, nullptr,
              nullptr, true, timestep, true);
 }
+#else
+// The jerks tree's own get_force_and_potential (taichi_with_jerks/integrator.h:308-432) without
+// its direct-sum branch for small N: low-order pre-pass (acc_old = |F| of the order-2 FMM),
+// then the error-controlled MAC (horizontalPass(cells, cells, 1, false)) with force_accuracy.
+// seed feeds srand48 before buildTree (the root shift's draws).
+int tcr_evaluate_high_jerks(int n, const double* x, const double* y, const double* z, const double* vx,
+                            const double* vy, const double* vz, const double* m, const unsigned char* flags,
+                            double fa, int nc, long seed, int nthreads, double* ax, double* ay, double* az,
+                            double* pot, double* jx, double* jy, double* jz) {
+  force_accuracy = fa;
+  return run(n, x, y, z, vx, vy, vz, m, flags, 0.4, nc, seed, nthreads, ax, ay, az, pot, jx, jy, jz, nullptr,
+             false, nullptr, true);
+}
 #endif
 }  // extern "C"
 
@@ -221,6 +268,40 @@ static int run(int n, const double* x, const double* y, const double* z, const d
         g_cells[i].min_acc = HUGE;
         g_cells[i].has_sink = false;
       }
+    upwardPass(g_cells);
+    for (size_t i = 0; i < g_cells.size(); i++)
+      for (int nn = 0; nn <= P; nn++) {
+        for (int mm = -nn; mm <= nn; mm++) {
+          int index = nn * nn + nn + mm;
+          g_cells[i].Pn[nn] += g_cells[i].M[index] * g_cells[i].M[index] * factorial_table[nn + mm] *
+                               factorial_table[nn - mm];
+        }
+        g_cells[i].Pn[nn] = sqrt(g_cells[i].Pn[nn]);
+      }
+  } else
+#else
+  if (high) {
+    // taichi_with_jerks/integrator.h:326-398, in order
+    g_high = 1;
+    upwardPass_low(g_cells);
+    horizontalPass_low(g_cells, g_cells);
+    downwardPass_low(g_cells);
+    for (size_t b = 0; b < bodies.size(); b++) {
+      Body& B = bodies[b];
+      B.acc_old = sqrt(B.F[0] * B.F[0] + B.F[1] * B.F[1] + B.F[2] * B.F[2]);
+      B.F[0] = B.F[1] = B.F[2] = 0;
+      B.J[0] = B.J[1] = B.J[2] = 0;
+      B.p = 0;
+      B.timestep = HUGE;
+    }
+    for (size_t i = 0; i < g_cells.size(); i++) {
+      for (int term = 0; term < NTERM; term++) {
+        g_cells[i].L[term] = 0;
+        g_cells[i].M[term] = 0;
+      }
+      g_cells[i].min_acc = HUGE;
+      g_cells[i].has_sink = false;
+    }
     upwardPass(g_cells);
     for (size_t i = 0; i < g_cells.size(); i++)
       for (int nn = 0; nn <= P; nn++) {
@@ -299,9 +380,7 @@ void tcr_expansions(double* M, double* L) {
 
 // kind 0 = M2L, 1 = P2P.  First call with tgt == NULL walks the tree and returns the count.
 long long tcr_list(int kind, int* tgt, int* src) {
-#ifndef TCR_JERKS
   if (g_list_t[0].empty() && g_list_t[1].empty() && g_high) record_high(&g_cells[0], &g_cells[0]);
-#endif
   if (g_list_t[0].empty() && g_list_t[1].empty()) record(&g_cells[0], &g_cells[0]);
   long long n = (long long)g_list_t[kind].size();
   if (tgt) memcpy(tgt, g_list_t[kind].data(), n * sizeof(int));

@@ -1,5 +1,7 @@
-// The top tree's error-controlled MAC (tc_set_error_mac): the low-order pre-pass that the
-// reference runs before it (integrator.h:476-493) and the per-cell inputs of the MAC.
+// The error-controlled MAC (tc_set_error_mac): the low-order pre-pass that the reference runs
+// before it (top tree integrator.h:476-493; jerks tree taichi_with_jerks/integrator.h:326-360)
+// and the per-cell inputs of the MAC.  The top tree's pre-pass is described first; the jerks
+// tree's differs in its near field and output (k_low_p2p_jerks below).
 //
 // Pre-pass (traverse_eager.h:36-52, :220-258, :306-322; kernel_fast_lean.h:1358-1647): an
 // order-2 FMM on the geometric cells (centre and radius of the octree, before any enclosing
@@ -231,6 +233,73 @@ __global__ void k_low_l2p(int n, const TcBodies b, const TcCells c, const int* _
             Phi[ind] += cl[(nn + kk) * (nn + kk) + (nn + kk) + (m + ll)] * G[kk * kk + kk + ll];
       }
     acc_old[i] += sqrt(Phi[3].x * Phi[3].x + Phi[3].y * Phi[3].y + Phi[2].x * Phi[2].x);
+  }
+}
+
+// ---------------------------------------------------------------------------------------
+// The jerks tree's pre-pass (taichi_with_jerks/integrator.h:326-360) differs from the top
+// tree's in its near field and its output: P2P_low (taichi_with_jerks/kernel_fast_lean.h:
+// 1567-1688, the SIMD_P2P branch the reference is built with) sums the acceleration VECTOR of
+// every source body of a low-order P2P source cell in FP32 (16 targets per SIMD vector, one
+// FP32 sum per source cell, added to the body's FP64 F), L2P_low (:1742-1780) subtracts the
+// order-2 local's gradient from F, and acc_old = |F| (integrator.h:350-356).  The FP32
+// arithmetic follows the reference's x86-64-v4 build operation by operation: positions and
+// masses rounded to FP32, dx = xj + (-xi), r2 = fma(dz, dz, fma(dy, dy, dx dx)), IEEE sqrt
+// and division, f = ((m / r) / r) / r as three products, a = fma(dx, f, a).
+// ---------------------------------------------------------------------------------------
+__global__ void k_low_p2p_jerks(int n, const TcBodies b, const TcCells c, const int* __restrict__ cell_of,
+                                const int* __restrict__ start, const int* __restrict__ src,
+                                double* __restrict__ F) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int t = cell_of[i];
+    const float xi = -(float)b.x[i], yi = -(float)b.y[i], zi = -(float)b.z[i];
+    double Fx = 0.0, Fy = 0.0, Fz = 0.0;
+    for (int q = start[t]; q < start[t + 1]; q++) {
+      const int s = src[q];
+      float ax = 0.f, ay = 0.f, az = 0.f;
+      for (int j = c.begin[s]; j < c.begin[s] + c.nbody[s]; j++) {
+        const float dx = __fadd_rn(xi, (float)b.x[j]);
+        const float dy = __fadd_rn(yi, (float)b.y[j]);
+        const float dz = __fadd_rn(zi, (float)b.z[j]);
+        const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+        const float mj = r2 > 0.f ? (float)b.m[j] : 0.f;
+        const float rr = r2 > 0.f ? r2 : __int_as_float(0x7f800000);
+        const float inv = __fdiv_rn(1.f, __fsqrt_rn(rr));
+        const float f = __fmul_rn(__fmul_rn(__fmul_rn(mj, inv), inv), inv);
+        ax = __fmaf_rn(dx, f, ax);
+        ay = __fmaf_rn(dy, f, ay);
+        az = __fmaf_rn(dz, f, az);
+      }
+      Fx += (double)ax;
+      Fy += (double)ay;
+      Fz += (double)az;
+    }
+    F[i] = Fx;
+    F[(size_t)n + i] = Fy;
+    F[2 * (size_t)n + i] = Fz;
+  }
+}
+
+// L2P_low of the jerks tree: F -= grad of the order-2 local at the body, acc_old = |F|
+__global__ void k_low_l2p_jerks(int n, const TcBodies b, const TcCells c, const int* __restrict__ cell_of,
+                                const double* __restrict__ L9, const double* __restrict__ F,
+                                double* __restrict__ acc_old) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int ci = cell_of[i];
+    cd cl[kLowNT], G[kLowNT], Phi[4];
+    tc_low_r2c(L9 + (size_t)ci * kLowNT, cl);
+    tc_low_gnm(c.gx[ci] - b.x[i], c.gy[ci] - b.y[i], c.gz[ci] - b.z[i], G);
+    for (int q = 0; q < kLowNT; q++) G[q] = conj(G[q]);
+    for (int q = 0; q < 4; q++) Phi[q] = mk(0, 0);
+    for (int nn = 0; nn <= 1; nn++)
+      for (int m = 0; m <= nn; m++) {
+        const int ind = nn * nn + nn + m;
+        for (int kk = 0; kk <= 2 - nn; kk++)
+          for (int ll = -kk; ll <= kk; ll++)
+            Phi[ind] += cl[(nn + kk) * (nn + kk) + (nn + kk) + (m + ll)] * G[kk * kk + kk + ll];
+      }
+    const double fx = F[i] - Phi[3].x, fy = F[(size_t)n + i] - Phi[3].y, fz = F[2 * (size_t)n + i] - Phi[2].x;
+    acc_old[i] = sqrt(__fma_rn(fz, fz, __fma_rn(fx, fx, __dmul_rn(fy, fy))));
   }
 }
 

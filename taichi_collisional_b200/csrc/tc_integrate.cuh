@@ -4,7 +4,7 @@
 //   split by time step (integrator.h:591-640)                      -> k_split_* below,
 //   kick_naive with update_timestep (integrator.h:182-311)        -> tc_evaluate_steps + k_ev_naive,
 //   kick of sinks by sources (integrator.h:378-457)                -> tc_evaluate with flags + k_ev_kick,
-//   kick_cpu, the direct kick of small systems (integrator.h:65-96) -> tc_evaluate_direct_noalloc + k_ev_kick,
+//   kick_cpu, the direct kick of small systems (integrator.h:65-96) -> direct sums + k_ev_kick,
 //   drift with COMPSUM (integrator.h:42, :642-656)                 -> k_drift_compsum.
 // The particles stay in the caller's device arrays, which are permuted in place exactly as the
 // reference's split swaps its particles, so after a step the arrays hold the reference's order
@@ -137,8 +137,15 @@ struct TcEvolve {
     const cudaStream_t s = ctx->stream;
     tc_status r;
     if (direct) {
-      r = tc_evaluate_direct_noalloc(ns, X(0, off), X(1, off), X(2, off), nullptr, nullptr, nullptr, X(9, off), fl,
-                                     ax, ay, az, apot, nullptr, nullptr, nullptr, 0, (void*)s);
+      // the context's own storage (never the library-wide static array of
+      // tc_evaluate_direct_noalloc, which contexts stepping at once would share)
+      const size_t S = ctx->kd_cap;
+      r = (size_t)ns <= S && direct_with_scratch(ns, X(0, off), X(1, off), X(2, off), nullptr, nullptr, nullptr,
+                                                 X(9, off), fl, ax, ay, az, apot, nullptr, nullptr, nullptr, 0, s,
+                                                 ctx->kd_scratch.p, ctx->kd_index.p, ctx->kd_flags.p,
+                                                 S) == cudaSuccess
+              ? TC_OK
+              : TC_ERR_CUDA;
       st.n_direct++;
     } else {
       r = tc_evaluate(ctx, ns, X(0, off), X(1, off), X(2, off), nullptr, nullptr, nullptr, X(9, off), fl, ax, ay, az,
@@ -276,6 +283,12 @@ extern "C" tc_status tc_evolve_hold_dkd(tc_ctx* ctx, int n, double* x, double* y
   TC_CK(ctx->ev_u.ensure((size_t)n + (size_t)n / 4096 + 2));
   TC_CK(ctx->ev_i.ensure(2 * (size_t)n + 2));
   TC_CK(ctx->ev_f.ensure((size_t)n));
+  // systems of at most kDirectMax bodies are kicked by direct sums (kick_cpu)
+  constexpr size_t kDirectMax = 128;
+  TC_CK(ctx->kd_scratch.ensure(14 * kDirectMax));
+  TC_CK(ctx->kd_index.ensure(kDirectMax));
+  TC_CK(ctx->kd_flags.ensure(kDirectMax));
+  ctx->kd_cap = kDirectMax;
   TcEvolve E;
   E.ctx = ctx;
   double* arr[12] = {x, y, z, ex, ey, ez, vx, vy, vz, m, timestep, pot};

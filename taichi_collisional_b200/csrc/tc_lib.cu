@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include <random>
 #include <string>
 #include <vector>
@@ -151,6 +152,10 @@ struct tc_ctx {
   DBuf<uint8_t> ev_f;
   DBuf<uint8_t> ds_flags;
   DBuf<int> ds_idx, ds_tgt;
+  DBuf<double> kd_scratch;  // direct kicks of small systems: 14 arrays of kd_cap entries
+  DBuf<int> kd_index;
+  DBuf<uint8_t> kd_flags;
+  size_t kd_cap = 0;
   size_t fcap = 0, mcap = 0, pcap = 0;
   // small device structs
   TcRootInfo* d_root = nullptr;
@@ -186,10 +191,11 @@ struct tc_ctx {
   long long glaunches = 0;
   int gsbits = 1;
   std::string gfail;  // why the last capture was abandoned (empty: captured)
+  std::vector<const void*> gsig;  // buffers and capacities baked into the captured graph
   // error-controlled MAC of the top tree (tc_set_error_mac) and its low-order pre-pass
   bool emac = false;
   double emac_fa = 2.0e-7;
-  DBuf<double> low_rgeo, low_m9, low_l9, acc_old, min_acc, pn_ref;
+  DBuf<double> low_rgeo, low_m9, low_l9, acc_old, min_acc, pn_ref, low_f;
   DBuf<int> cell_of;
 };
 
@@ -778,8 +784,9 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     return TC_OK;
   };
   TcMac mac;  // theta
-  if (ctx->emac && prm.variant == TC_VARIANT_TOP) {
-    // ---- low-order pre-pass on the geometric cells -> acc_old (integrator.h:476-493)
+  if (ctx->emac) {
+    // ---- low-order pre-pass on the geometric cells -> acc_old (integrator.h:476-493;
+    // taichi_with_jerks/integrator.h:326-360)
     const int nc = ctx->ncell;
     TC_CK(ctx->low_rgeo.ensure(nc));
     TC_CK(ctx->low_m9.ensure((size_t)nc * kLowNT));
@@ -802,15 +809,23 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     TC_CK(cudaMemsetAsync(ctx->low_l9.p, 0, sizeof(double) * (size_t)nc * kLowNT, st));
     k_low_m2l<<<gc, 128, 0, st>>>(nc, cv, ctx->m2l_start.p, ctx->m2l_src.p, ctx->low_m9.p, ctx->low_l9.p);
     k_low_cell_of<<<gc, 128, 0, st>>>(nc, cv, ctx->cell_of.p);
-    k_low_p2p<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->p2p_start.p, ctx->p2p_src.p, ctx->acc_old.p);
+    if (JERK) {
+      TC_CK(ctx->low_f.ensure(3 * (size_t)n));
+      k_low_p2p_jerks<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->p2p_start.p, ctx->p2p_src.p, ctx->low_f.p);
+    } else {
+      k_low_p2p<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->p2p_start.p, ctx->p2p_src.p, ctx->acc_old.p);
+    }
     for (int l = 0; l < maxl; l++) k_low_l2l<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->low_l9.p);
-    k_low_l2p<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->low_l9.p, ctx->acc_old.p);
+    if (JERK)
+      k_low_l2p_jerks<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->low_l9.p, ctx->low_f.p, ctx->acc_old.p);
+    else
+      k_low_l2p<<<gb, 128, 0, st>>>(n, b, cv, ctx->cell_of.p, ctx->low_l9.p, ctx->acc_old.p);
     // ---- MAC inputs: min_acc (bottom-up) and Pn of the reference's form
     for (int l = maxl; l >= 0; l--)
       k_min_acc<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->acc_old.p, ctx->min_acc.p);
     k_cell_pn_ref<P><<<gc, 128, 0, st>>>(nc, cv.M, ctx->pn_ref.p);
     ctx->launches += 7 + 3 * (maxl + 1);
-    mac.mode = 2;
+    mac.mode = JERK ? 3 : 2;
     mac.p = P;
     mac.fa = ctx->emac_fa;
     mac.pn = ctx->pn_ref.p;
@@ -1245,6 +1260,36 @@ struct TcNoallocDev {
   uint8_t* flags = nullptr;
 };
 static TcNoallocDev g_noalloc_dev[64];
+static std::mutex g_noalloc_mu;  // guards the one-time fill of g_noalloc_dev
+
+// Direct-sum evaluation over working storage the caller provides: S entries per array in
+// `scratch` (14 arrays: x y z m vx vy vz | pot ax ay az jx jy jz), `index` and `flags`
+// (n <= S).  Shared by tc_evaluate_direct_noalloc (the static array) and the block-time-step
+// integrator's direct kicks (the context's own buffers, so contexts never share storage).
+static cudaError_t direct_with_scratch(int n, const double* x, const double* y, const double* z, const double* vx,
+                                       const double* vy, const double* vz, const double* m,
+                                       const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
+                                       double* jx, double* jy, double* jz, int jerk, cudaStream_t st,
+                                       double* scratch, int* index, uint8_t* fl, size_t S) {
+  TcBodies b;
+  b.x = scratch; b.y = scratch + S; b.z = scratch + 2 * S; b.m = scratch + 3 * S;
+  b.vx = jerk ? scratch + 4 * S : nullptr; b.vy = jerk ? scratch + 5 * S : nullptr;
+  b.vz = jerk ? scratch + 6 * S : nullptr;
+  b.flags = fl;
+  b.perm = index;
+  TcOut o;
+  o.pot = scratch + 7 * S; o.ax = scratch + 8 * S; o.ay = scratch + 9 * S; o.az = scratch + 10 * S;
+  o.jx = jerk ? scratch + 11 * S : nullptr; o.jy = jerk ? scratch + 12 * S : nullptr;
+  o.jz = jerk ? scratch + 13 * S : nullptr;
+  k_identity<<<nblocks(n, 256), 256, 0, st>>>(n, index);
+  k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, index, x, y, z, m, vx, vy, vz, flags, b);
+  if (jerk)
+    k_direct<true><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
+  else
+    k_direct<false><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
+  k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, index, o, pot, ax, ay, az, jerk ? jx : nullptr, jy, jz);
+  return cudaGetLastError();
+}
 
 // ----------------------------------------------------------------------------------------
 // C ABI
@@ -1614,6 +1659,24 @@ static void graph_drop(tc_ctx* ctx) {
   ctx->gvalid = false;
 }
 
+// Every device buffer and capacity a captured graph has baked into its launches.  Any other
+// call on the context (tc_evaluate_steps, tc_direct_sums, tc_train_selector, an evaluation of
+// another n) may grow, and so free and reallocate, one of them; a replay is only valid while
+// the signature is unchanged.
+static void graph_signature(const tc_ctx* c, std::vector<const void*>& s) {
+  s.clear();
+  const void* bufs[] = {c->in_d.p,     c->in_f.p,      c->out_d.p,     c->keys.p,      c->keys_alt.p,
+                        c->vals.p,     c->vals_alt.p,  c->hist.p,      c->bod.p,       c->bflags.p,
+                        c->perm.p,     c->outs.p,      c->cint.p,      c->cdbl.p,      c->csink.p,
+                        c->split_off.p, c->expn.p,     c->front[0].p,  c->front[1].p,  c->m2l.p,
+                        c->m2l_alt.p,  c->p2p.p,       c->p2p_alt.p,   c->m2l_start.p, c->m2l_src.p,
+                        c->p2p_start.p, c->p2p_src.p,  c->m2l_tl.p,    c->p2p_tl.p,    c->leaves.p,
+                        c->judge_idx.p, c->judge_out.p, c->p2p_part.p, c->bpart.p,     c->tc_bins.p};
+  s.assign(bufs, bufs + sizeof(bufs) / sizeof(bufs[0]));
+  const size_t caps[] = {c->ccap, c->mcap, c->pcap, c->fcap, c->expn.n, c->p2p_part.n};
+  for (size_t v : caps) s.push_back((const void*)(uintptr_t)v);
+}
+
 static bool graph_key_equal(const TcGraphKey& a, const TcGraphKey& b) {
   if (a.n != b.n || a.mem != b.mem) return false;
   for (int i = 0; i < 15; i++)
@@ -1799,6 +1862,7 @@ static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* 
   }
   ctx->graph = g;
   ctx->gkey = key;
+  graph_signature(ctx, ctx->gsig);
   ctx->gvalid = true;
   graph_check(ctx, "instantiate");
   if (!ctx->gfail.empty()) graph_drop(ctx);
@@ -1815,6 +1879,11 @@ static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const doubl
   for (int i = 0; i < 15; i++) key.ptr[i] = ptrs[i];
   key.prm = ctx->prm;
   const bool jerk = ctx->prm.variant == TC_VARIANT_JERKS;
+  if (ctx->gvalid) {
+    std::vector<const void*> sig;
+    graph_signature(ctx, sig);
+    if (sig != ctx->gsig) graph_drop(ctx);  // a buffer it launches on was reallocated since the capture
+  }
   if (ctx->gvalid && graph_key_equal(key, ctx->gkey)) {
     TC_CK(cudaSetDevice(ctx->prm.device));
     TC_CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
@@ -1869,7 +1938,6 @@ static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const doubl
 
 tc_status tc_set_error_mac(tc_ctx* ctx, int on, double force_accuracy) {
   if (!ctx || (on && !(force_accuracy > 0.0))) return TC_ERR_ARG;
-  if (on && ctx->prm.variant != TC_VARIANT_TOP) return TC_ERR_UNSUPPORTED;
   ctx->emac = on != 0;
   ctx->emac_fa = force_accuracy;
   graph_drop(ctx);  // a captured graph used the theta MAC
@@ -2059,38 +2127,23 @@ tc_status tc_evaluate_direct_noalloc(int n, const double* x, const double* y, co
   if (n > TC_NOALLOC_MAX_N) return TC_ERR_CAPACITY;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return TC_ERR_CUDA;
-  TcNoallocDev& D = g_noalloc_dev[dev];
-  if (!D.scratch) {  // once per device: device addresses of the static arrays
-    double* ps = nullptr;
-    int* pi = nullptr;
-    uint8_t* pf = nullptr;
-    if (cudaGetSymbolAddress((void**)&ps, g_noalloc_scratch) != cudaSuccess) return TC_ERR_CUDA;
-    if (cudaGetSymbolAddress((void**)&pi, g_noalloc_index) != cudaSuccess) return TC_ERR_CUDA;
-    if (cudaGetSymbolAddress((void**)&pf, g_noalloc_flags) != cudaSuccess) return TC_ERR_CUDA;
-    D.index = pi;
-    D.flags = pf;
-    D.scratch = ps;
+  TcNoallocDev D;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_dev[dev].scratch) {  // once per device: device addresses of the static arrays
+      TcNoallocDev f;
+      if (cudaGetSymbolAddress((void**)&f.scratch, g_noalloc_scratch) != cudaSuccess ||
+          cudaGetSymbolAddress((void**)&f.index, g_noalloc_index) != cudaSuccess ||
+          cudaGetSymbolAddress((void**)&f.flags, g_noalloc_flags) != cudaSuccess)
+        return TC_ERR_CUDA;
+      g_noalloc_dev[dev] = f;
+    }
+    D = g_noalloc_dev[dev];
   }
-  cudaStream_t st = (cudaStream_t)stream;
-  const size_t S = TC_NOALLOC_MAX_N;
-  TcBodies b;
-  b.x = D.scratch; b.y = D.scratch + S; b.z = D.scratch + 2 * S; b.m = D.scratch + 3 * S;
-  b.vx = jerk ? D.scratch + 4 * S : nullptr; b.vy = jerk ? D.scratch + 5 * S : nullptr;
-  b.vz = jerk ? D.scratch + 6 * S : nullptr;
-  b.flags = D.flags;
-  b.perm = D.index;
-  TcOut o;
-  o.pot = D.scratch + 7 * S; o.ax = D.scratch + 8 * S; o.ay = D.scratch + 9 * S; o.az = D.scratch + 10 * S;
-  o.jx = jerk ? D.scratch + 11 * S : nullptr; o.jy = jerk ? D.scratch + 12 * S : nullptr;
-  o.jz = jerk ? D.scratch + 13 * S : nullptr;
-  k_identity<<<nblocks(n, 256), 256, 0, st>>>(n, D.index);
-  k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, D.index, x, y, z, m, vx, vy, vz, flags, b);
-  if (jerk)
-    k_direct<true><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
-  else
-    k_direct<false><<<nblocks(n, 128), 128, 0, st>>>(n, b, o);
-  k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, D.index, o, pot, ax, ay, az, jerk ? jx : nullptr, jy, jz);
-  return cudaGetLastError() == cudaSuccess ? TC_OK : TC_ERR_CUDA;
+  return direct_with_scratch(n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, jerk,
+                             (cudaStream_t)stream, D.scratch, D.index, D.flags, TC_NOALLOC_MAX_N) == cudaSuccess
+             ? TC_OK
+             : TC_ERR_CUDA;
 }
 
 tc_status tc_train_selector(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,

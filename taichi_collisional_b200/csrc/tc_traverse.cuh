@@ -14,8 +14,10 @@
 namespace tc {
 
 // acceptance test of a traversal (mode 0: theta, traverse_eager.h:151-203; 1: the low-order
-// pre-pass, |d|^2 > 3 (Ri + Rj)^2 on geometric cells, :220-245; 2: the error-controlled MAC of
-// horizontalPassHigh, :61-148, with the reference's binomials comb[k] = combinator_coef[P][k])
+// pre-pass, |d|^2 > 3 (Ri + Rj)^2 on geometric cells, :220-245; 2: the top tree's error-
+// controlled MAC of horizontalPassHigh, :61-148, with the reference's binomials comb[k] =
+// combinator_coef[P][k]; 3: the jerks tree's one-sided horizontalPassHigh,
+// taichi_with_jerks/traverse_eager.h:59-122)
 struct TcMac {
   int mode = 0;
   int p = 0;
@@ -24,6 +26,25 @@ struct TcMac {
   const double* min_acc = nullptr;  // per cell
   double comb[TC_PMAX_DEV + 1];
 };
+
+// x^-k correctly rounded (k >= 1): x^k in double-double by repeated products, then the
+// reciprocal's leading term refined by one Newton step on the pair
+__device__ __forceinline__ double tc_pow_neg_int(double x, int k) {
+  double h = x, l = 0.0;
+  for (int i = 1; i < k; i++) {
+    const double p = h * x;
+    const double e = __fma_rn(h, x, -p);
+    h = p;
+    l = __fma_rn(l, x, e);
+    const double s = h + l;
+    l = l - (s - h);
+    h = s;
+  }
+  const double y = 1.0 / h;
+  // residual of y (h + l) - 1 in extended precision
+  const double r = __fma_rn(-y, h, 1.0) - y * l;
+  return __fma_rn(y, r, y);
+}
 
 struct TcTravCounters {
   unsigned long long frontier[3];  // rotating frontier sizes
@@ -79,6 +100,25 @@ __global__ void k_trav_step(int s, const int2* __restrict__ fin, int2* __restric
         accept = R2 > rs * rs;
       } else if (mac.mode == 1) {
         accept = dx * dx + dy * dy + dz * dz > rs * rs * 3;
+      } else if (mac.mode == 3) {
+        // f2 only, pre-test |d|^2 0.4 > (Ra + Rb)^2; operation order and contractions of the
+        // reference's x86-64 build (norm(): fma(dz, dz, fma(dx, dx, dy dy)); Eba += (Pn pa) comb
+        // as one fma; R^-(P+1) correctly rounded)
+        const double R2 = __fma_rn(dz, dz, __fma_rn(dx, dx, __dmul_rn(dy, dy)));
+        double f2 = 10;
+        const double Ra = c.R[i], Rb = c.R[j];
+        if (__dmul_rn(R2, 0.4) > __dmul_rn(rs, rs)) {
+          const int P = mac.p;
+          const double Rp = tc_pow_neg_int(__dsqrt_rn(R2), P + 1);
+          double pa = 1, Eba = 0;
+          for (int k = 0; k <= P; k++) {
+            Eba = __fma_rn(__dmul_rn(mac.pn[(size_t)j * (P + 1) + P - k], pa), mac.comb[k], Eba);
+            pa = __dmul_rn(pa, Ra);
+          }
+          const double fac = __dmul_rn(__dmul_rn(8.0, fmax(Ra, Rb)), Rp);
+          f2 = __ddiv_rn(__dmul_rn(fac, Eba), __dmul_rn(mac.min_acc[i], mac.fa));
+        }
+        accept = f2 < 1;
       } else {
         const double R2 = dx * dx + dy * dy + dz * dz;
         double f1 = 10, f2 = 10;

@@ -13,15 +13,21 @@
 // Unlike the reference, `bodies` keeps its order (results are written in place, so the
 // Body::index round trip still works but is no longer needed).
 //
+// Traversal: the jerks tree's get_force_and_potential always runs its low-order pre-pass and
+// its one-sided error-controlled MAC (taichi_with_jerks/integrator.h:326-403,
+// horizontalPass(cells, cells, 1, get_steps)), and so does the jerks shim, with the global
+// force_accuracy (define TC_SHIM_THETA to use the theta MAC instead).  For the top-level tree
+// the shim uses the theta MAC unless TC_SHIM_ERROR_MAC is defined, which selects the top
+// tree's own pre-pass and error-controlled MAC (integrator.h:476-539).  With the error MAC,
+// Body::acc_old receives the pre-pass's estimate as in the reference; otherwise (and on the
+// direct-sum branch of small N) it is left unchanged.
+//
 // get_steps == true: for the top-level tree, the time-step pass of the reference
 // (tc_evaluate_steps: no M2L, near-field F and p, Body::timestep = sum of 1/tau^4 from the
-// pairwise criterion of kernel_fast_lean.h:462-548, with the global dt_param); for the jerks
-// tree the reference's theta path ignores get_steps (taichi_with_jerks/traverse_eager.h:
-// 125-155), and so does the shim.  Body::timestep is otherwise reset as the reference does
-// (0 for the top-level tree, integrator.h:500-507; HUGE for the jerks tree,
-// taichi_with_jerks/integrator.h:352-364).  Body::acc_old is left unchanged: the reference
-// fills it from its low-order pre-pass, which belongs to the error-controlled MAC path, not to
-// the theta path implemented here.
+// pairwise criterion of kernel_fast_lean.h:462-548, with the global dt_param); the jerks
+// tree's traversal ignores get_steps (taichi_with_jerks/traverse_eager.h:59-155), and so does
+// the shim.  Body::timestep is otherwise reset as the reference does (0 for the top-level
+// tree, integrator.h:500-507; HUGE for the jerks tree, taichi_with_jerks/integrator.h:352-364).
 #pragma once
 #include <vector>
 
@@ -65,9 +71,11 @@ inline void get_force_and_potential(Bodies& bodies, bool get_steps) {
     flags[i] = (unsigned char)((b.issink ? 1 : 0) | (b.issource ? 2 : 0));
   }
   tc_status s;
-#if defined(TC_SHIM_ERROR_MAC) && !defined(TC_SHIM_JERKS)
-  // the top tree's own traversal: low-order pre-pass + error-controlled MAC with the current
-  // global force_accuracy (integrator.h:459-562; main.cxx changes force_accuracy for a while)
+#if (defined(TC_SHIM_ERROR_MAC) && !defined(TC_SHIM_JERKS)) || (defined(TC_SHIM_JERKS) && !defined(TC_SHIM_THETA))
+#define TC_SHIM_USES_ERROR_MAC 1
+  // the tree's own traversal: low-order pre-pass + error-controlled MAC with the current
+  // global force_accuracy (integrator.h:459-562, taichi_with_jerks/integrator.h:308-432;
+  // main.cxx changes force_accuracy for a while)
   s = tc_set_error_mac(tc_shim_context(), 1, force_accuracy);
   if (s != TC_OK) ENDRUN("tc_set_error_mac: %s\n", tc_status_string(s));
 #endif
@@ -82,12 +90,20 @@ inline void get_force_and_potential(Bodies& bodies, bool get_steps) {
                     flags.data(), ax.data(), ay.data(), az.data(), pot.data(), jx.data(), jy.data(), jz.data(),
                     TC_MEM_HOST);
   if (s != TC_OK) ENDRUN("taichi_b200 force evaluation: %s\n", tc_status_string(s));
+#ifdef TC_SHIM_USES_ERROR_MAC
+  std::vector<double> acc_old(n);
+  // TC_ERR_UNSUPPORTED on the direct-sum branch, which has no pre-pass: acc_old stays
+  const bool have_acc_old = tc_get_acc_old(tc_shim_context(), acc_old.data()) == TC_OK;
+#endif
   for (int i = 0; i < n; i++) {
     Body& b = bodies[i];
     // the reference's FMM branch resets F, p (and J) before accumulating
     // (integrator.h:500-507, taichi_with_jerks/integrator.h:352-364)
     b.F[0] = ax[i]; b.F[1] = ay[i]; b.F[2] = az[i];
     b.p = pot[i];
+#ifdef TC_SHIM_USES_ERROR_MAC
+    if (have_acc_old) b.acc_old = acc_old[i];
+#endif
 #ifdef TC_SHIM_JERKS
     b.J[0] = jx[i]; b.J[1] = jy[i]; b.J[2] = jz[i];
     b.timestep = HUGE;

@@ -12,12 +12,15 @@ radius) and its M2L / P2P lists as visited by the reference recursion.  The step
 store the time-step pass of the top-level tree (get_steps = true): near-field pot / acc and
 each body's accumulated 1 / tau^4, with a sink / source subset.  The emac_* cases store the
 top tree's own get_force_and_potential: the low-order pre-pass (acc_old per body, min_acc per
-cell) and the error-controlled MAC's lists and forces.  The integ_* case stores the
+cell) and the error-controlled MAC's lists and forces; the emac_jerks_* cases the same for the
+jerks tree (its order-2 pre-pass with the FP32 vector near field, its one-sided MAC, and the
+jerks).  The integ_* case stores the
 reference integrator's diagnostics (kinetic / potential energy, centre of mass), three
 compensated drifts and one split by time step.  The evolve_* case stores one do_evolve step
 of the reference's HOLD block-time-step scheme with its own force evaluation (p = 8).
 
-    python tests/golden/make_golden.py [--evolve-only | --integ-only | --emac-only | --steps-only]
+    python tests/golden/make_golden.py [--emac-jerks-only | --evolve-only | --integ-only | --emac-only |
+                                        --steps-only]
 """
 import os
 import sys
@@ -51,6 +54,31 @@ EMAC_CASES = [
     ("emac_top_kroupa3k_p8", "plummer_kroupa", 3000, 31, 8, 32, 2.0e-7),
     ("emac_top_plummer2k_p12", "plummer", 2000, 32, 12, 64, 1.0e-8),
 ]
+
+
+EMAC_JERKS_CASES = [
+    # name, generator, n, seed, p, ncrit, force_accuracy, shift seed  (jerks tree, error-controlled MAC)
+    ("emac_jerks_kroupa3k_p8", "plummer_kroupa", 3000, 51, 8, 32, 2.0e-8, 9),
+    ("emac_jerks_plummer2k_p12", "plummer", 2000, 52, 12, 64, 2.0e-8, 10),
+]
+
+
+def make_emac_jerks(out_dir):
+    """The jerks tree's own get_force_and_potential (low-order pre-pass, one-sided error MAC)."""
+    for name, gen, n, seed, p, ncrit, fa, sseed in EMAC_JERKS_CASES:
+        x, y, z, vx, vy, vz, m = getattr(ics, gen)(n, seed)
+        r = oracle.ref_evaluate_high_jerks(x, y, z, m, vx, vy, vz, p=p, ncrit=ncrit, force_accuracy=fa, seed=sseed)
+        cells = oracle.ref_cells(oracle.VARIANT_JERKS, p, r["ncell"], n)
+        lists = oracle.ref_lists(oracle.VARIANT_JERKS, p)
+        shift = oracle.ref_shift_uniforms(oracle.VARIANT_JERKS, p, sseed)
+        np.savez_compressed(
+            os.path.join(out_dir, name + ".npz"), p=p, ncrit=ncrit, force_accuracy=fa, shift_u=shift,
+            x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, m=m, ax=r["ax"], ay=r["ay"], az=r["az"], pot=r["pot"],
+            jx=r["jx"], jy=r["jy"], jz=r["jz"], acc_old=r["acc_old"], min_acc=r["min_acc"],
+            cell_begin=cells["begin"], cell_nbody=cells["nbody"], cell_nchild=cells["nchild"],
+            cell_child=cells["child"], cell_X=cells["X"], cell_R=cells["R"],
+            m2l_t=lists["m2l"][0], m2l_s=lists["m2l"][1], p2p_t=lists["p2p"][0], p2p_s=lists["p2p"][1])
+        print(name, "cells", r["ncell"], "m2l", len(lists["m2l"][0]), "p2p", len(lists["p2p"][0]))
 
 
 def make_emac(out_dir):
@@ -144,6 +172,9 @@ def make_evolve(out_dir):
 
 def main():
     out_dir = os.path.dirname(os.path.abspath(__file__))
+    make_emac_jerks(out_dir)
+    if "--emac-jerks-only" in sys.argv:
+        return
     make_evolve(out_dir)
     if "--evolve-only" in sys.argv:
         return

@@ -111,3 +111,36 @@ def test_graph_with_pinned_host_buffers():
         assert g.graph_ready()
         for k in ref:
             np.testing.assert_array_equal(hout[k].numpy(), ref[k], err_msg=k)
+
+
+def test_graph_survives_buffer_reallocation_by_other_calls():
+    """A captured graph bakes in the context's buffers.  tc_evaluate_steps on the same context
+    (top tree, small n) needs a larger near-field chunk buffer than tc_evaluate planned, so it
+    frees and reallocates it; the next matching tc_evaluate must not replay into the freed
+    memory.  Its results must equal a context that never used a graph."""
+    import taichi_collisional_b200 as t
+    from taichi_collisional_b200 import ics
+    n = 20000
+    x, y, z, vx, vy, vz, m = ics.plummer_kroupa(n, 21)
+    d = {k: torch.tensor(a, device="cuda") for k, a in zip(("x", "y", "z", "vx", "vy", "vz", "m"),
+                                                           (x, y, z, vx, vy, vz, m))}
+    out = {k: torch.empty(n, dtype=torch.float64, device="cuda") for k in ("ax", "ay", "az", "pot")}
+    g = t.Gravity(p=8, ncrit=64, theta=0.5, variant=t.VARIANT_TOP, precision=t.PREC_FP64, direct_below=0)
+    gd = t.Gravity(p=8, ncrit=64, theta=0.5, variant=t.VARIANT_TOP, precision=t.PREC_FP64, direct_below=0)
+    g.set_graph(True)
+
+    def run(gg, o):
+        gg.evaluate(d["x"], d["y"], d["z"], d["m"], out=o)
+        torch.cuda.synchronize()
+        return {k: v.cpu().numpy().copy() for k, v in o.items()}
+
+    run(g, out)
+    assert g.graph_ready(), g.graph_note()
+    ref = run(gd, {k: torch.empty_like(v) for k, v in out.items()})
+    g.evaluate_steps(d["x"], d["y"], d["z"], d["m"], d["vx"], d["vy"], d["vz"], 0.025)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        got = run(g, out)
+        for k in ref:
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+    assert g.graph_ready()

@@ -307,3 +307,33 @@ def test_error_mac_time_step_pass_matches_reference():
     acc_old = g.acc_old()
     assert np.max(np.abs(acc_old - d["acc_old"]) / np.abs(d["acc_old"])) < 1e-12
     g.close()
+
+
+def test_jerks_error_mac_matches_reference():
+    """The jerks tree's own get_force_and_potential (taichi_with_jerks/integrator.h:308-432):
+    the order-2 pre-pass with its FP32 vector near field (acc_old = |F|), the one-sided error
+    MAC of taichi_with_jerks/traverse_eager.h:59-122 (lists identical), and the forces and jerks
+    within 1e-12 -- against the reference run by tests/golden/make_golden.py (emac_jerks_*)."""
+    import glob
+    files = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "emac_jerks_*.npz")))
+    assert files
+    for f in files:
+        d = dict(np.load(f))
+        name = os.path.basename(f)
+        g = tcb.Gravity(p=int(d["p"]), ncrit=int(d["ncrit"]), theta=0.4, variant=tcb.VARIANT_JERKS,
+                        precision=tcb.PREC_FP64, shift_u=d["shift_u"], direct_below=0)
+        g.set_error_mac(True, float(d["force_accuracy"]))
+        out = g.evaluate(d["x"], d["y"], d["z"], d["m"], d["vx"], d["vy"], d["vz"])
+        acc_old = g.acc_old()
+        # FP32 sums in the reference's operation order; FP64 sums over source cells in another order
+        assert np.max(np.abs(acc_old - d["acc_old"]) / np.abs(d["acc_old"])) < 1e-9, name
+        c = g.cells()
+        ref_lev = ref_cell_levels(d["cell_nchild"], d["cell_child"])
+        rkeys = cell_keys(d["cell_begin"], d["cell_nbody"], ref_lev)
+        gkeys = cell_keys(c["begin"], c["nbody"], c["level"])
+        assert sorted(rkeys) == sorted(gkeys), name
+        lists = g.lists()
+        for k in ("m2l", "p2p"):
+            assert pair_set(lists[k][0], lists[k][1], gkeys) == pair_set(d[k + "_t"], d[k + "_s"], rkeys), (name, k)
+        _check_forces(out, d, True)
+        g.close()

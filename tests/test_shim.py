@@ -6,7 +6,9 @@ import subprocess
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = os.environ.get("TC_REFERENCE", "/root/reference")
+import oracle  # noqa: E402
+
+REF = oracle.reference_dir() or ""
 
 PROGRAM = r"""
 #include <cmath>
@@ -26,7 +28,8 @@ int main(int argc, char**) {
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "exafmm.h")), reason="reference tree not present")
 @pytest.mark.parametrize("tree,defs", [("", []), ("", ["-DTC_SHIM_ERROR_MAC"]),
-                                       ("taichi_with_jerks", ["-DTC_SHIM_JERKS"])])
+                                       ("taichi_with_jerks", ["-DTC_SHIM_JERKS"]),
+                                       ("taichi_with_jerks", ["-DTC_SHIM_JERKS", "-DTC_SHIM_THETA"])])
 def test_shim_compiles_and_links_against_reference_types(tmp_path, tree, defs):
     src = tmp_path / "shim_main.cpp"
     src.write_text(PROGRAM)

@@ -12,7 +12,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(HERE, "..", "taichi_collisional_b200", "csrc"))
 import gen_swap_tables as g  # noqa: E402
 
-REF = os.environ.get("TC_REFERENCE", "/root/reference")
+import oracle  # noqa: E402
+
+REF = oracle.reference_dir() or ""
 MATS = g.derive(30)
 
 

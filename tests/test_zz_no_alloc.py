@@ -4,8 +4,10 @@ Some callers cannot allocate device memory (their own allocator owns the GPU mem
 may touch, or their time step must not stall on cudaMalloc's implicit synchronisation).
 For them the library keeps its working storage in one fixed static device array.  These
 checks call that entry point through the C ABI, twice in a row with different inputs, and
-compare each result with the allocating entry point (tc_evaluate on its direct branch).
-This file is collected last on purpose; it must pass alone and after the other tests."""
+compare each result with the allocating entry point (tc_evaluate on its direct branch) and
+with the CPU oracle's FP64 direct sum, also with sink-only, source-only and sink+source
+bodies mixed.  This file is collected last on purpose; it must pass alone and after the
+other tests."""
 import ctypes as C
 
 import numpy as np
@@ -28,7 +30,20 @@ def _reference_result(arrays, jerk):
     return out
 
 
-def _noalloc(arrays, jerk):
+def _oracle_result(arrays, jerk, flags=None):
+    """FP64 direct sums of the CPU oracle; with flags, only bit-1 bodies act as sources and
+    bodies without bit 0 (not sinks) get zeros, as the library defines them."""
+    import oracle
+    x, y, z, vx, vy, vz, m = arrays
+    msrc = m if flags is None else np.where(flags & 2, m, 0.0)
+    ref = oracle.direct(x, y, z, msrc, *((vx, vy, vz) if jerk else (None, None, None)))
+    if flags is not None:
+        for k in ref:
+            ref[k] = np.where(flags & 1, ref[k], 0.0)
+    return ref
+
+
+def _noalloc(arrays, jerk, flags=None):
     import torch
     L = tcb.load_library()
     t = [torch.tensor(a, dtype=torch.float64, device="cuda") for a in arrays]
@@ -36,9 +51,10 @@ def _noalloc(arrays, jerk):
     n = len(arrays[0])
     keys = ("ax", "ay", "az", "pot", "jx", "jy", "jz")
     out = {k: torch.full((n,), np.nan, dtype=torch.float64, device="cuda") for k in keys}
+    fl = None if flags is None else torch.tensor(flags, dtype=torch.uint8, device="cuda")
     P = lambda a: C.c_void_p(a.data_ptr()) if a is not None else None  # noqa: E731
     rc = L.tc_evaluate_direct_noalloc(n, P(x), P(y), P(z), P(vx) if jerk else None, P(vy) if jerk else None,
-                                      P(vz) if jerk else None, P(m), None, P(out["ax"]), P(out["ay"]),
+                                      P(vz) if jerk else None, P(m), P(fl), P(out["ax"]), P(out["ay"]),
                                       P(out["az"]), P(out["pot"]), P(out["jx"]) if jerk else None,
                                       P(out["jy"]) if jerk else None, P(out["jz"]) if jerk else None,
                                       int(jerk), None)
@@ -62,6 +78,20 @@ def test_noalloc_matches_allocating_entry_point_twice(jerk):
         got = _noalloc(arrays, jerk)
         ref = _reference_result(arrays, jerk)
         _compare(got, ref, keys)
+        _compare(got, _oracle_result(arrays, jerk), keys)
+
+
+@pytest.mark.parametrize("jerk", [True, False])
+def test_noalloc_sink_and_source_flags_match_the_oracle(jerk):
+    """The flags the block-time-step integrator's direct kicks pass: 1 sink only, 2 source
+    only, 3 both; two calls in a row with different flag patterns."""
+    keys = ("ax", "ay", "az", "pot", "jx", "jy", "jz") if jerk else ("ax", "ay", "az", "pot")
+    rng = np.random.default_rng(7)
+    for n, seed in ((2000, 201), (700, 202)):
+        arrays = ics.plummer_kroupa(n, seed=seed)
+        flags = rng.integers(1, 4, n).astype(np.uint8)
+        got = _noalloc(arrays, jerk, flags)
+        _compare(got, _oracle_result(arrays, jerk, flags), keys)
 
 
 def test_noalloc_rejects_sizes_above_its_fixed_array():

@@ -70,6 +70,12 @@ typedef struct {
                          makes the call redo the far field at the fixed order p             */
   double judge_tol;
   unsigned long long judge_seed;
+  double softening;   /* Plummer softening eps of the pair interactions (near field, direct sums,
+                         tc_direct_sums): 1/r -> 1/sqrt(r^2 + eps^2); r = 0 pairs stay skipped.
+                         0 = the reference's Newtonian kernel (it has no softening).  The far
+                         field keeps the Newtonian multipoles, whose difference is O(eps^2/r^2)
+                         at the far-field separations; the time-step pass and the error MAC's
+                         pre-pass estimate stay Newtonian.  No counterpart in the reference.   */
 } tc_params;
 
 typedef struct {
@@ -79,9 +85,10 @@ typedef struct {
   long long n_launches; /* kernels launched by the last tc_evaluate */
   long long flags;      /* diagnostic bits of the last evaluation (1 M2L, 2 P2P, 4 frontier capacity
                            retries; 8 depth limit; 16 an enclosing ball hit its iteration cap) */
-  int n_classes;                /* far-field order classes used by the last evaluation     */
-  int class_order[6];           /* their orders                                            */
-  long long class_pairs[6];     /* M2L pairs evaluated at each order                       */
+  int n_classes;                /* distinct M2L orders the last evaluation's pairs got     */
+  int class_order[16];          /* those orders, lowest first                              */
+  long long class_pairs[16];    /* M2L pairs selected at each order (a batch of 32 pairs runs
+                                   at the largest order among them)                        */
   double m2l_flop_fraction;     /* sum over pairs of (q+1)^3 / (p+1)^3, divided by pairs   */
   double judge_rms;             /* RMS relative acceleration error at the judge's bodies   */
   int judge_redo;               /* 1 if the judge rejected the selector's step             */
@@ -199,6 +206,27 @@ tc_status tc_mlp_predict(int ns, int n_out, const float* feat, const float* w, c
 tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy,
                         double* vz, const double* ax, const double* ay, const double* az,
                         double dt_kick, double dt_drift);
+
+/* Limit, in GPU clock cycles, of every bounded device-side wait of this context's kernels (the
+ * tensor-core far field's waits for its products); cycles <= 0 restores the default (4e9, about
+ * two seconds).  A wait that runs out stops the kernel's work, waits (with the default limit)
+ * for the products already in flight, frees its tensor memory and makes the call return
+ * TC_ERR_TIMEOUT; the context stays usable.  Meant for testing that path.  No counterpart in
+ * the reference. */
+tc_status tc_set_wait_limit(tc_ctx* ctx, long long cycles);
+
+/* One shared-time-step leapfrog step (kick-drift-kick) around a force evaluation, on device
+ * arrays: v += a dt/2; x += v dt; (a, pot, j) <- tc_evaluate(x, v, m); v += a dt/2.
+ * a (ax, ay, az) holds the previous step's accelerations on entry (zero before the first step)
+ * and the new ones on return; jx..jz may be NULL (jerks tree only).  The reference's kick
+ * (integrator.h:378-457) and drift (integrator.h:642-670) for one shared step.  With
+ * tc_set_graph on, the whole step -- both kicks, the evaluation and the judge -- is one CUDA
+ * graph replay (captured on the first call, as tc_evaluate's graph; a step and a plain
+ * evaluation never share a graph).  No counterpart in the reference, whose integrators are
+ * host code.  Asynchronous on the context's stream. */
+tc_status tc_step_leapfrog(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                           const double* m, double* ax, double* ay, double* az, double* pot, double* jx, double* jy,
+                           double* jz, double dt);
 
 /* System diagnostics on device arrays (n bodies; pot in the positive convention p = +sum m/r
  * that tc_evaluate writes).  Replaces system_kinetic_energy (integrator.h:887-895),

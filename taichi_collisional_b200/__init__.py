@@ -36,7 +36,7 @@ class Params(C.Structure):
                 ("precision", C.c_int), ("use_shift", C.c_int), ("shift_u", C.c_double * 3),
                 ("direct_below", C.c_int), ("device", C.c_int), ("selector", C.c_int),
                 ("selector_tol", C.c_double), ("judge_n", C.c_int), ("judge_tol", C.c_double),
-                ("judge_seed", C.c_ulonglong)]
+                ("judge_seed", C.c_ulonglong), ("softening", C.c_double)]
 
 
 class Stats(C.Structure):
@@ -45,8 +45,8 @@ class Stats(C.Structure):
                 ("max_level", C.c_int), ("ms_total", C.c_double), ("ms_tree", C.c_double),
                 ("ms_upward", C.c_double), ("ms_traverse", C.c_double), ("ms_m2l", C.c_double),
                 ("ms_p2p", C.c_double), ("ms_downward", C.c_double), ("n_launches", C.c_longlong),
-                ("flags", C.c_longlong), ("n_classes", C.c_int), ("class_order", C.c_int * 6),
-                ("class_pairs", C.c_longlong * 6), ("m2l_flop_fraction", C.c_double), ("judge_rms", C.c_double),
+                ("flags", C.c_longlong), ("n_classes", C.c_int), ("class_order", C.c_int * 16),
+                ("class_pairs", C.c_longlong * 16), ("m2l_flop_fraction", C.c_double), ("judge_rms", C.c_double),
                 ("judge_redo", C.c_int)]
 
 
@@ -60,7 +60,8 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
            "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note", "tc_set_error_mac", "tc_get_acc_old", "tc_hermite_predict", "tc_hermite_correct",
-           "tc_system_diagnostics", "tc_drift_compensated", "tc_split_order", "tc_evolve_hold_dkd"]
+           "tc_system_diagnostics", "tc_drift_compensated", "tc_split_order", "tc_evolve_hold_dkd", "tc_step_leapfrog",
+           "tc_set_wait_limit"]
 NOALLOC_MAX_N = 16384
 
 _lib = None
@@ -95,6 +96,10 @@ def load_library(path=LIB_PATH):
     L.tc_hermite_predict.restype = C.c_int
     L.tc_hermite_correct.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 13 + [C.c_double]
     L.tc_hermite_correct.restype = C.c_int
+    L.tc_set_wait_limit.argtypes = [C.c_void_p, C.c_longlong]
+    L.tc_set_wait_limit.restype = C.c_int
+    L.tc_step_leapfrog.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 14 + [C.c_double]
+    L.tc_step_leapfrog.restype = C.c_int
     L.tc_set_error_mac.argtypes = [C.c_void_p, C.c_int, C.c_double]
     L.tc_set_error_mac.restype = C.c_int
     L.tc_get_acc_old.argtypes = [C.c_void_p, _dp]
@@ -202,12 +207,12 @@ class Gravity:
 
     def __init__(self, p=12, ncrit=64, theta=0.4, variant=VARIANT_JERKS, precision=PREC_FP64, shift_u=None,
                  direct_below=-1, device=0, selector=0, selector_tol=1e-9, judge_n=0, judge_tol=0.0,
-                 judge_seed=12345):
+                 judge_seed=12345, softening=0.0):
         self._L = load_library()
         self.params = default_params(p=p, ncrit=ncrit, theta=theta, variant=variant, precision=precision,
                                      shift_u=shift_u, direct_below=direct_below, device=device, selector=selector,
                                      selector_tol=selector_tol, judge_n=judge_n, judge_tol=judge_tol,
-                                     judge_seed=judge_seed)
+                                     judge_seed=judge_seed, softening=softening)
         h = C.c_void_p()
         rc = self._L.tc_create(C.byref(self.params), C.byref(h))
         if rc != 0:
@@ -324,6 +329,20 @@ class Gravity:
                                     MEM_DEVICE if dev else MEM_HOST)
         self._check(rc, "tc_direct_sums")
         return {k: out[:, i].copy() for i, k in enumerate(("pot", "ax", "ay", "az", "jx", "jy", "jz"))}
+
+    def set_wait_limit(self, cycles):
+        """Clock-cycle limit of the bounded device waits (tc_set_wait_limit; <= 0: default)."""
+        self._check(self._L.tc_set_wait_limit(self._h, int(cycles)), "tc_set_wait_limit")
+
+    def step_leapfrog(self, st, out, dt):
+        """One kick-drift-kick step on CUDA tensors (tc_step_leapfrog): st holds x, y, z, vx, vy,
+        vz, m; out holds ax, ay, az (the previous accelerations on entry), pot (and jx, jy, jz).
+        With set_graph(True) the whole step replays as one CUDA graph."""
+        rc = self._L.tc_step_leapfrog(self._h, len(st["x"]), *[_ptr(st[k]) for k in ("x", "y", "z", "vx", "vy", "vz",
+                                                                                      "m")],
+                                      *[_ptr(out.get(k)) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")],
+                                      float(dt))
+        self._check(rc, "tc_step_leapfrog")
 
     def kick_drift(self, x, y, z, vx, vy, vz, ax, ay, az, dt_kick, dt_drift):
         """FP64 leapfrog update on CUDA tensors: v += a dt_kick; x += v dt_drift."""

@@ -25,6 +25,7 @@ struct TcBodies {
   double *x, *y, *z, *m, *vx, *vy, *vz;
   uint8_t* flags;  // bit0 sink, bit1 source
   int* perm;       // sorted position -> caller index
+  double eps2 = 0.0;  // Plummer softening squared of the pair interactions (0: Newtonian)
 };
 
 // Cells in breadth-first order; level l occupies [lvl_start[l], lvl_start[l+1]).

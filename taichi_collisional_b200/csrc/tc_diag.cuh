@@ -78,15 +78,16 @@ __global__ void __launch_bounds__(kDiagThreads, 3) k_sys_diag_part(
   TcDD acc[kDiagQ];
 #pragma unroll
   for (int q = 0; q < kDiagQ; q++) acc[q] = {0.0, 0.0};
-  const int stride = gridDim.x * kDiagThreads;
+  // 64-bit indices: i + stride must not wrap for n within one grid stride of INT_MAX
+  const long long stride = (long long)gridDim.x * kDiagThreads;
   // software-pipelined: the next body's eight values are loaded before this body is folded, so
   // each thread keeps two bodies' loads in flight (same order of the sums as a plain loop)
-  int i = blockIdx.x * kDiagThreads + threadIdx.x;
+  long long i = (long long)blockIdx.x * kDiagThreads + threadIdx.x;
   double cm = 0, cx = 0, cy = 0, cz = 0, cu = 0, cv = 0, cw = 0, cp = 0;
   if (i < n) { cm = m[i]; cx = x[i]; cy = y[i]; cz = z[i]; cu = vx[i]; cv = vy[i]; cw = vz[i]; cp = pot[i]; }
   for (; i < n; i += stride) {
     const double mi = cm, px = cx, py = cy, pz = cz, ux = cu, uy = cv, uz = cw, pi = cp;
-    const int j = i + stride;
+    const long long j = i + stride;
     if (j < n) { cm = m[j]; cx = x[j]; cy = y[j]; cz = z[j]; cu = vx[j]; cv = vy[j]; cw = vz[j]; cp = pot[j]; }
     const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(ux, ux), __dmul_rn(uy, uy)), __dmul_rn(uz, uz));
     acc[0] = tc_dd_add(acc[0], __dmul_rn(__dmul_rn(mi, v2), 0.5));

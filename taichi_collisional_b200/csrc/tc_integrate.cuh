@@ -142,8 +142,8 @@ struct TcEvolve {
       const size_t S = ctx->kd_cap;
       r = (size_t)ns <= S && direct_with_scratch(ns, X(0, off), X(1, off), X(2, off), nullptr, nullptr, nullptr,
                                                  X(9, off), fl, ax, ay, az, apot, nullptr, nullptr, nullptr, 0, s,
-                                                 ctx->kd_scratch.p, ctx->kd_index.p, ctx->kd_flags.p,
-                                                 S) == cudaSuccess
+                                                 ctx->kd_scratch.p, ctx->kd_index.p, ctx->kd_flags.p, S,
+                                                 ctx->prm.softening * ctx->prm.softening) == cudaSuccess
               ? TC_OK
               : TC_ERR_CUDA;
       st.n_direct++;

@@ -34,6 +34,7 @@
 #include "tc_select.cuh"
 #include "tc_mlp.cuh"
 #include "tc_train.cuh"
+#include "tc_order.cuh"
 #include "tc_diag.cuh"
 #include "tdesign.h"
 
@@ -75,12 +76,14 @@ struct TcGraphKey {
   int n = -1, mem = -1;
   const void* ptr[15] = {};
   tc_params prm;
+  double step_dt = 0.0;  // != 0: the whole leapfrog step (tc_step_leapfrog) around the evaluation
 };
 
 // read back after a replay (small device structs, copied by the graph into pinned memory)
 struct TcGraphStatus {
   unsigned err;
   unsigned small[4];
+  unsigned hist[32];  // pairs per order (order selection)
   TcLevels lv;
   TcTravCounters cnt;
 };
@@ -122,9 +125,16 @@ struct tc_ctx {
   DBuf<int> m2l_start, m2l_src, p2p_start, p2p_src, m2l_tl, p2p_tl, leaves;
   DBuf<double> cell_pn;
   DBuf<int> cls_start, cls_tl;  // per order class: per-target offsets and target lists
-  int n_classes = 0, class_order[TC_MAX_CLASSES];
-  long long class_pairs[TC_MAX_CLASSES];
+  int n_classes = 0, class_order[16];
+  long long class_pairs[16];
   double flop_frac = 1.0;
+  // per-pair orders with a per-target budget: |a| of the last evaluation (caller order, valid for
+  // amag_n bodies), per-body and per-cell budget scales, the regrouped source lists and orders
+  DBuf<double> amag, body_scale, cell_scale;
+  int amag_n = -1;
+  DBuf<int> m2l_src2;
+  DBuf<uint8_t> m2l_off;
+  unsigned* d_hist = nullptr;  // 32 counters
   // learned selector
   bool mlp_ready = false;
   int mlp_nout = 0;
@@ -166,6 +176,7 @@ struct tc_ctx {
                                     // [10] target counter of the persistent FP64 M2L (graph)
   DBuf<float> tc_bins;  // tensor-core M2L bin matrices (hi, lo) of order tc_bins_q
   int tc_bins_q = -1;
+  long long wait_limit = kTcWaitLimit;  // clock cycles a bounded device wait may take (tc_set_wait_limit)
   int nsm = 0;
   DBuf<double> bpart;
   // last evaluation
@@ -192,6 +203,8 @@ struct tc_ctx {
   int gsbits = 1;
   std::string gfail;  // why the last capture was abandoned (empty: captured)
   std::vector<const void*> gsig;  // buffers and capacities baked into the captured graph
+  double gstep_dt = 0.0;          // the graph being planned holds a leapfrog step of this dt
+  bool gselect = false;           // the captured graph selects per-pair orders
   // error-controlled MAC of the top tree (tc_set_error_mac) and its low-order pre-pass
   bool emac = false;
   double emac_fa = 2.0e-7;
@@ -359,6 +372,7 @@ static TcBodies bodies_view(tc_ctx* c, int n, bool jerk) {
   b.vx = vel ? d + 4 * N : nullptr; b.vy = vel ? d + 5 * N : nullptr; b.vz = vel ? d + 6 * N : nullptr;
   b.flags = c->bflags.p;
   b.perm = c->perm.p;
+  b.eps2 = c->prm.softening * c->prm.softening;
   return b;
 }
 
@@ -409,87 +423,54 @@ __global__ void k_p2p_count(const unsigned long long* __restrict__ keys, unsigne
 }
 
 // ----------------------------------------------------------------------------------------
-// far field with a per-pair order (tc_select.cuh): classify, re-sort by class, one launch per
-// class
+// per-pair orders with a per-target error budget (tc_order.cuh): the target scale of every cell
+// from the previous evaluation's accelerations, then each target's list regrouped by order
 // ----------------------------------------------------------------------------------------
-template <int P, int I, bool JERK>
-struct TcClassLaunch {
-  static void run(int cls, int ntl, const int* tl, const int* tstart, const int* src, TcCells cv, cudaStream_t st) {
-    if constexpr (I < TcOrderClasses<P>::n) {
-      if (cls == I) {
-        constexpr int Q = TcOrderClasses<P>::q[I];
-        size_t smem = (size_t)TcM2LSmem<Q>::TOTAL * sizeof(double);
-        k_m2l<P, Q, JERK><<<ntl, tc_m2l_threads<Q>(), smem, st>>>(tl, ntl, tstart, src, cv);
-      } else {
-        TcClassLaunch<P, I + 1, JERK>::run(cls, ntl, tl, tstart, src, cv, st);
-      }
-    }
+// the orders used by an evaluation (h[o]: pairs at order p - o), lowest first
+static void order_stats(tc_ctx* ctx, int p, const unsigned* h) {
+  ctx->n_classes = 0;
+  double tot = 0.0, ff = 0.0;
+  for (int o = p; o >= 0; o--) {
+    if (!h[o]) continue;
+    const int q = p - o;
+    ctx->class_order[ctx->n_classes] = q;
+    ctx->class_pairs[ctx->n_classes] = h[o];
+    ctx->n_classes++;
+    tot += h[o];
+    ff += h[o] * std::pow((q + 1.0) / (p + 1.0), 3);
   }
-  static void attrs() {
-    if constexpr (I < TcOrderClasses<P>::n) {
-      constexpr int Q = TcOrderClasses<P>::q[I];
-      size_t smem = (size_t)TcM2LSmem<Q>::TOTAL * sizeof(double);
-      cudaFuncSetAttribute(k_m2l<P, Q, JERK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      TcClassLaunch<P, I + 1, JERK>::attrs();
-    }
-  }
-};
+  ctx->flop_frac = tot > 0 ? ff / tot : 1.0;
+}
 
-template <int P, bool JERK>
-static cudaError_t run_m2l_classes(tc_ctx* ctx, TcCells cv) {
-  using OC = TcOrderClasses<P>;
+template <int P>
+static cudaError_t select_orders(tc_ctx* ctx, TcCells cv, int n, int ntl, const unsigned* ntldev, bool capture) {
   cudaStream_t st = ctx->stream;
-  const int nc = ctx->ncell, sbits = ctx->sbits;
-  const unsigned long long nm = ctx->n_m2l;
+  const int nc = capture ? (int)ctx->ccap : ctx->ncell;
   cudaError_t e;
   if ((e = ctx->cell_pn.ensure((size_t)nc * (P + 1))) != cudaSuccess) return e;
-  if ((e = ctx->cls_start.ensure((size_t)OC::n * (nc + 1))) != cudaSuccess) return e;
-  if ((e = ctx->cls_tl.ensure((size_t)OC::n * nc)) != cudaSuccess) return e;
-  k_cell_pn<P><<<nblocks(nc, 128), 128, 0, st>>>(nc, cv.M, ctx->cell_pn.p);
-  if ((e = cudaMemsetAsync(ctx->d_small, 0, 4 * sizeof(unsigned) * 2, st)) != cudaSuccess) return e;
-  unsigned* d_hist = ctx->d_small;  // TC_MAX_CLASSES counters (d_small holds 8)
-  if (ctx->prm.selector == 2) {
-    if (!ctx->mlp_ready || ctx->mlp_nout != OC::n) return cudaErrorInvalidValue;
-    k_select_mlp<P><<<148 * 8, 256, 0, st>>>(ctx->m2l.p, nm, sbits, cv, ctx->cell_pn.p, ctx->mlp_w.p, ctx->mlp_norm,
-                                             (float)log10(ctx->prm.selector_tol), ctx->m2l_alt.p, d_hist);
-  } else {
-    k_select_analytic<P><<<148 * 8, 256, 0, st>>>(ctx->m2l.p, nm, sbits, cv, ctx->cell_pn.p, ctx->prm.selector_tol,
-                                                  ctx->m2l_alt.p, d_hist);
-  }
-  // stable sort by class: one radix pass over the class bits keeps (target, source) order
-  ctx->launches += 2 + radix_sort(ctx->m2l_alt.p, nullptr, ctx->m2l.p, nullptr, (int)nm, 2 * sbits + 8,
-                                  ctx->hist.p, st, 2 * sbits);
-  unsigned hcnt[8];
-  if ((e = cudaMemcpyAsync(hcnt, d_hist, sizeof(hcnt), cudaMemcpyDeviceToHost, st)) != cudaSuccess) return e;
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-  k_strip_class<<<148 * 8, 256, 0, st>>>(ctx->m2l_alt.p, nm, sbits);
-  ctx->n_classes = OC::n;
-  unsigned long long off = 0;
-  double ff = 0.0;
-  for (int i = 0; i < OC::n; i++) {
-    ctx->class_order[i] = OC::q[i];
-    ctx->class_pairs[i] = hcnt[i];
-    double q1 = OC::q[i] + 1.0, p1 = P + 1.0;
-    ff += hcnt[i] * (q1 * q1 * q1) / (p1 * p1 * p1);
-    int* cs = ctx->cls_start.p + (size_t)i * (nc + 1);
-    int* tl = ctx->cls_tl.p + (size_t)i * nc;
-    if (hcnt[i] == 0) {
-      off += hcnt[i];
-      continue;
-    }
-    k_list_csr<<<148 * 8, 256, 0, st>>>(ctx->m2l_alt.p + off, hcnt[i], nc, sbits, cs, ctx->m2l_src.p + off);
-    if ((e = cudaMemsetAsync(ctx->d_small + 7, 0, sizeof(unsigned), st)) != cudaSuccess) return e;
-    k_list_targets<<<nblocks(nc, 256), 256, 0, st>>>(cs, nc, tl, ctx->d_small + 7);
-    unsigned ntl = 0;
-    if ((e = cudaMemcpyAsync(&ntl, ctx->d_small + 7, sizeof(unsigned), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
-      return e;
-    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
-    if (ntl) TcClassLaunch<P, 0, JERK>::run(i, (int)ntl, tl, cs, ctx->m2l_src.p + off, cv, st);
-    ctx->launches += 3;
-    off += hcnt[i];
-  }
-  ctx->flop_frac = nm ? ff / (double)nm : 1.0;
-  // the class-ordered list stays in m2l_alt; restore the (target, source) order for inspection
+  if ((e = ctx->cell_scale.ensure((size_t)nc)) != cudaSuccess) return e;
+  if ((e = ctx->body_scale.ensure((size_t)n)) != cudaSuccess) return e;
+  if ((e = ctx->m2l_src2.ensure(ctx->m2l_src.n)) != cudaSuccess) return e;
+  if ((e = ctx->m2l_off.ensure(ctx->m2l_src.n)) != cudaSuccess) return e;
+  const int* d_ncell = capture ? &((TcLevels*)ctx->d_lv)->ncell : nullptr;
+  k_cell_pn<P><<<std::min(nblocks(nc, 128), 148 * 16), 128, 0, st>>>(nc, cv.M, ctx->cell_pn.p, d_ncell);
+  k_gather_scale<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, ctx->amag.p, ctx->body_scale.p);
+  int* d_start = &((TcLevels*)ctx->d_lv)->start[0];
+  int* d_count = &((TcLevels*)ctx->d_lv)->count[0];
+  const int maxl = capture ? TC_MAX_LEVEL : ctx->max_level;
+  const int gc = std::min(nblocks(nc, 128), 148 * 16);
+  for (int l = maxl; l >= 0; l--)
+    k_min_acc<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->body_scale.p, ctx->cell_scale.p);
+  if ((e = cudaMemsetAsync(ctx->d_hist, 0, 32 * sizeof(unsigned), st)) != cudaSuccess) return e;
+  TcClassOrders cls;
+  for (int i = 0; i < TC_MAX_CLASSES; i++) cls.q[i] = i < TcOrderClasses<P>::n ? TcOrderClasses<P>::q[i] : P;
+  const int mode = ctx->prm.selector == 2 ? 2 : 1;
+  const int grid = capture ? 148 * 8 : std::max(1, std::min(nblocks(ntl, 4), 148 * 8));
+  k_select_order<P><<<grid, 128, 0, st>>>(ctx->m2l_tl.p, ntl, ctx->m2l_start.p, ctx->m2l_src.p, ctx->m2l_src2.p,
+                                          ctx->m2l_off.p, cv, ctx->cell_pn.p, ctx->cell_scale.p,
+                                          ctx->prm.selector_tol, mode, ctx->mlp_w.p, ctx->mlp_norm,
+                                          TcOrderClasses<P>::n, cls, ctx->d_hist, ntldev);
+  ctx->launches += 4 + maxl;
   return cudaGetLastError();
 }
 
@@ -853,10 +834,17 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
   ctx->flop_frac = 1.0;
   if (ctx->steps) {
     // time-step pass: no far field (the reference skips M2L when get_steps is set)
-  } else if (hs[0] > 0 && prm.selector > 0 && !mixed && TcOrderClasses<P>::n > 1) {
-    cudaError_t ce = run_m2l_classes<P, JERK>(ctx, cv);
-    if (ce != cudaSuccess) return cuda_fail(ctx, ce, "far field by order class");
   } else if (hs[0] > 0) {
+    const int* m2l_src = ctx->m2l_src.p;
+    if (prm.selector > 0 && !mixed && ctx->amag_n == n && (prm.selector == 1 || ctx->mlp_ready)) {
+      cudaError_t ce = select_orders<P>(ctx, cv, n, (int)hs[0], nullptr, false);
+      if (ce != cudaSuccess) return cuda_fail(ctx, ce, "order selection");
+      m2l_src = ctx->m2l_src2.p;
+      unsigned h[32];
+      TC_CK(cudaMemcpyAsync(h, ctx->d_hist, sizeof(h), cudaMemcpyDeviceToHost, st));
+      TC_CK(cudaStreamSynchronize(st));
+      order_stats(ctx, P, h);
+    }
     if (mixed && P <= TC_TC_QMAX) {
       if constexpr (P <= TC_TC_QMAX) {
         TC_CK(tc_ensure_bins<P>(ctx));
@@ -864,7 +852,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
         int grid = std::min((int)hs[0], ctx->nsm);
         k_m2l_tc<P, P, JERK><<<grid, 128, TcTcSmem<P>::TOTAL, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
                                                                      ctx->m2l_src.p, cv, ctx->tc_bins.p,
-                                                                     ctx->d_small + 9, ctx->d_err);
+                                                                     ctx->d_small + 9, ctx->d_err, ctx->wait_limit);
       }
     } else if (mixed) {
       size_t smem = (size_t)TcM2LMixSmem<P>::BYTES;
@@ -873,11 +861,28 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     } else {
       size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
       k_m2l<P, P, JERK><<<hs[0], tc_m2l_threads<P>(), smem, st>>>(ctx->m2l_tl.p, (int)hs[0], ctx->m2l_start.p,
-                                                                     ctx->m2l_src.p, cv);
+                                                                     m2l_src, cv);
     }
     ctx->launches++;
   }
   if (ctx->events) cudaEventRecord(ctx->ev[4], st);
+  // ---- downward, before the near field (the mixed near field reads the far-field
+  // acceleration); nothing to add in the time-step pass, where every local expansion is zero
+  if (!ctx->steps) {
+    ctx->launches += maxl + (ctx->nleaf > 0);
+    for (int l = 1; l <= maxl; l++) {
+      int cnt = ctx->lv.count[l];
+      int g = nblocks(cnt, TcTransW<P>::W);
+      if (g > 148 * 16) g = 148 * 16;
+      k_l2l_level<P, JERK><<<g, TcTransW<P>::W * 32, 0, st>>>(l, cv, d_start, d_count);
+    }
+    if (ctx->nleaf > 0) {
+      int g = nblocks(ctx->nleaf, kUpWarps);
+      if (g > 148 * 32) g = 148 * 32;
+      k_l2p<P, JERK><<<g, kUpWarps * 32, 0, st>>>(ctx->leaves.p, ctx->nleaf, b, cv, o);
+    }
+  }
+  if (ctx->events) cudaEventRecord(ctx->ev[5], st);
   if (ctx->steps) {
     TC_CK(ctx->tsum.ensure((size_t)n));
     TC_CK(cudaMemsetAsync(ctx->tsum.p, 0, sizeof(double) * (size_t)n, st));
@@ -905,7 +910,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     int g = nblocks(hs[1], kP2PWarps);
     if (mixed_p2p)
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b,
-                                                       cv, o);
+                                                       cv, o, kP2PExclFrac);
     else {
       // few target leaves (small n): split each leaf's sources over up to 16 warps, then fold
       // the chunks in order (k_p2p_join); the split depends on n only, as in the graph path
@@ -923,24 +928,6 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
       }
     }
     ctx->launches++;
-  }
-  if (ctx->events) cudaEventRecord(ctx->ev[5], st);
-  // ---- downward (nothing to add in the time-step pass: every local expansion is zero)
-  if (ctx->steps) {
-    if (ctx->events) cudaEventRecord(ctx->ev[6], st);
-    return TC_OK;
-  }
-  ctx->launches += maxl + (ctx->nleaf > 0);
-  for (int l = 1; l <= maxl; l++) {
-    int cnt = ctx->lv.count[l];
-    int g = nblocks(cnt, TcTransW<P>::W);
-    if (g > 148 * 16) g = 148 * 16;
-    k_l2l_level<P, JERK><<<g, TcTransW<P>::W * 32, 0, st>>>(l, cv, d_start, d_count);
-  }
-  if (ctx->nleaf > 0) {
-    int g = nblocks(ctx->nleaf, kUpWarps);
-    if (g > 148 * 32) g = 148 * 32;
-    k_l2p<P, JERK><<<g, kUpWarps * 32, 0, st>>>(ctx->leaves.p, ctx->nleaf, b, cv, o);
   }
   if (ctx->events) cudaEventRecord(ctx->ev[6], st);
   return TC_OK;
@@ -1040,15 +1027,32 @@ static void run_fmm_graph(tc_ctx* ctx, int n) {
   TcOut o = out_view(ctx, n, JERK);
   cudaMemsetAsync(ctx->outs.p, 0, sizeof(double) * (size_t)n * (JERK ? 7 : 4), st);
   cudaMemsetAsync(ctx->d_small + 10, 0, sizeof(unsigned), st);
+  const int* m2l_src = ctx->m2l_src.p;
+  if (ctx->gselect) {  // per-pair orders (the previous replay left |a| in ctx->amag)
+    select_orders<P>(ctx, cv, n, ccap, ctx->d_small, true);
+    m2l_src = ctx->m2l_src2.p;
+    L += 4 + TC_MAX_LEVEL;
+    graph_check(ctx, "order selection");
+  }
   k_m2l<P, P, JERK><<<ctx->nsm, tc_m2l_threads<P>(), (size_t)TcM2LSmem<P>::TOTAL * sizeof(double), st>>>(
-      ctx->m2l_tl.p, ccap, ctx->m2l_start.p, ctx->m2l_src.p, cv, ctx->d_small, ctx->d_small + 10);
+      ctx->m2l_tl.p, ccap, ctx->m2l_start.p, m2l_src, cv, ctx->d_small, ctx->d_small + 10);
   graph_check(ctx, "M2L");
   graph_event(ctx, 4, st);
+  // ---- downward (before the near field: the mixed near field reads the far-field acceleration)
+  for (int l = 1; l <= TC_MAX_LEVEL; l++)
+    k_l2l_level<P, JERK><<<148 * 16, TcTransW<P>::W * 32, 0, st>>>(l, cv, d_start, d_count);
+  {
+    const int g = std::min(nblocks(ccap, kUpWarps), 148 * 32);
+    k_l2p<P, JERK><<<g, kUpWarps * 32, 0, st>>>(ctx->leaves.p, ccap, b, cv, o, ctx->d_small + 2);
+  }
+  L += TC_MAX_LEVEL + 1;
+  graph_check(ctx, "downward pass");
+  graph_event(ctx, 5, st);
   {
     const int g = nblocks(ccap, kP2PWarps);  // a warp per target slot; warps past the count exit
     if (prm.precision != TC_PREC_FP64)
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o,
-                                                       ctx->d_small + 1);
+                                                       kP2PExclFrac, ctx->d_small + 1);
     else {
       const int nsplit = p2p_nsplit(n);
       if (nsplit > 1) {  // the same chunks as the direct launches (p2p_part sized by graph_plan)
@@ -1066,16 +1070,6 @@ static void run_fmm_graph(tc_ctx* ctx, int n) {
   }
   L += 2;
   graph_check(ctx, "P2P");
-  graph_event(ctx, 5, st);
-  // ---- downward
-  for (int l = 1; l <= TC_MAX_LEVEL; l++)
-    k_l2l_level<P, JERK><<<148 * 16, TcTransW<P>::W * 32, 0, st>>>(l, cv, d_start, d_count);
-  {
-    const int g = std::min(nblocks(ccap, kUpWarps), 148 * 32);
-    k_l2p<P, JERK><<<g, kUpWarps * 32, 0, st>>>(ctx->leaves.p, ccap, b, cv, o, ctx->d_small + 2);
-  }
-  L += TC_MAX_LEVEL + 1;
-  graph_check(ctx, "downward pass");
   graph_event(ctx, 6, st);
   ctx->glaunches += L;
 }
@@ -1119,8 +1113,6 @@ static tc_status judge(tc_ctx* ctx, int n, int nt, bool jerk, double* rms) {
 
 template <int P>
 static void set_m2l_attrs() {
-  TcClassLaunch<P, 0, true>::attrs();
-  TcClassLaunch<P, 0, false>::attrs();
   size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
   cudaFuncSetAttribute(k_m2l<P, P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_m2l<P, P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1181,6 +1173,18 @@ __global__ void k_kick_drift(int n, double* x, double* y, double* z, double* vx,
   if (dd != 0.0) {
     x[i] += u * dd; y[i] += v * dd; z[i] += w * dd;
   }
+}
+
+// the closing kick of a captured leapfrog step: skipped when the evaluation before it overflowed a
+// capacity (its accelerations are invalid; the host re-runs the evaluation and this kick)
+__global__ void k_kick_guarded(int n, double* vx, double* vy, double* vz, const double* ax, const double* ay,
+                               const double* az, double dk, const unsigned* err, unsigned mask) {
+  if (*err & mask) return;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vx[i] += ax[i] * dk;
+  vy[i] += ay[i] * dk;
+  vz[i] += az[i] * dk;
 }
 
 // Hermite 4th-order predictor (Makino & Aarseth 1992) in FP64: saves x0, v0, a0, j0 into
@@ -1270,13 +1274,14 @@ static cudaError_t direct_with_scratch(int n, const double* x, const double* y, 
                                        const double* vy, const double* vz, const double* m,
                                        const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
                                        double* jx, double* jy, double* jz, int jerk, cudaStream_t st,
-                                       double* scratch, int* index, uint8_t* fl, size_t S) {
+                                       double* scratch, int* index, uint8_t* fl, size_t S, double eps2 = 0.0) {
   TcBodies b;
   b.x = scratch; b.y = scratch + S; b.z = scratch + 2 * S; b.m = scratch + 3 * S;
   b.vx = jerk ? scratch + 4 * S : nullptr; b.vy = jerk ? scratch + 5 * S : nullptr;
   b.vz = jerk ? scratch + 6 * S : nullptr;
   b.flags = fl;
   b.perm = index;
+  b.eps2 = eps2;
   TcOut o;
   o.pot = scratch + 7 * S; o.ax = scratch + 8 * S; o.ay = scratch + 9 * S; o.az = scratch + 10 * S;
   o.jx = jerk ? scratch + 11 * S : nullptr; o.jy = jerk ? scratch + 12 * S : nullptr;
@@ -1354,6 +1359,7 @@ tc_status tc_create(const tc_params* prm, tc_ctx** out) {
     return TC_ERR_ARG;
   if (prm->precision != TC_PREC_FP64 && prm->precision != TC_PREC_MIXED && prm->precision != TC_PREC_MIXED_M2L)
     return TC_ERR_ARG;
+  if (!(prm->softening >= 0.0) || !std::isfinite(prm->softening)) return TC_ERR_ARG;
   tc_ctx* ctx = new tc_ctx();
   ctx->prm = *prm;
   memset(&ctx->stats, 0, sizeof(ctx->stats));
@@ -1364,6 +1370,7 @@ tc_status tc_create(const tc_params* prm, tc_ctx** out) {
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_cnt, sizeof(TcTravCounters));
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_err, sizeof(unsigned));
   if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_small, 16 * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaMalloc((void**)&ctx->d_hist, 32 * sizeof(unsigned));
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, ctx->prm.device);
   if (e == cudaSuccess) {
     for (int i = 0; i < 8 && e == cudaSuccess; i++) e = cudaEventCreate(&ctx->ev[i]);
@@ -1396,11 +1403,15 @@ tc_status tc_destroy(tc_ctx* ctx) {
   ctx->ds_bod.release(); ctx->ds_out.release(); ctx->ds_flags.release(); ctx->ds_idx.release(); ctx->ds_tgt.release();
   ctx->tsum.release(); ctx->diag.release(); ctx->p2p_part.release();
   ctx->ev_d.release(); ctx->ev_u.release(); ctx->ev_i.release(); ctx->ev_f.release();
+  ctx->amag.release(); ctx->body_scale.release(); ctx->cell_scale.release(); ctx->m2l_src2.release();
+  ctx->m2l_off.release(); ctx->kd_scratch.release(); ctx->kd_index.release(); ctx->kd_flags.release();
+  ctx->low_f.release();
   if (ctx->d_root) cudaFree(ctx->d_root);
   if (ctx->d_lv) cudaFree(ctx->d_lv);
   if (ctx->d_cnt) cudaFree(ctx->d_cnt);
   if (ctx->d_err) cudaFree(ctx->d_err);
   if (ctx->d_small) cudaFree(ctx->d_small);
+  if (ctx->d_hist) cudaFree(ctx->d_hist);
   if (ctx->events)
     for (int i = 0; i < 8; i++) cudaEventDestroy(ctx->ev[i]);
   graph_drop(ctx);
@@ -1430,7 +1441,7 @@ static tc_status finish_stats(tc_ctx* ctx, int n, unsigned herr) {
   S.n_launches = ctx->launches;
   S.flags = herr | ctx->tree_flags;
   S.n_classes = ctx->n_classes;
-  for (int i = 0; i < 6; i++) {
+  for (int i = 0; i < 16; i++) {
     S.class_order[i] = i < ctx->n_classes ? ctx->class_order[i] : 0;
     S.class_pairs[i] = i < ctx->n_classes ? ctx->class_pairs[i] : 0;
   }
@@ -1447,7 +1458,7 @@ static tc_status finish_stats(tc_ctx* ctx, int n, unsigned herr) {
       for (int i = 0; i < 8; i++) t[i] = 0.f;
     }
     S.ms_total = t[0]; S.ms_tree = t[1]; S.ms_upward = t[2]; S.ms_traverse = t[3]; S.ms_m2l = t[4];
-    S.ms_p2p = t[5]; S.ms_downward = t[6];
+    S.ms_downward = t[5]; S.ms_p2p = t[6];  // the downward pass runs before the near field
   }
   if (herr & TC_EBIT_TIMEOUT) {
     ctx->err = "a device-side wait of the tensor-core far field gave up";
@@ -1467,7 +1478,7 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
 static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
                                 const double* vx, const double* vy, const double* vz, const double* m,
                                 const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
-                                double* jx, double* jy, double* jz, int mem);
+                                double* jx, double* jy, double* jz, int mem, double step_dt = 0.0);
 
 tc_status tc_evaluate(tc_ctx* ctx, int n, const double* x, const double* y, const double* z, const double* vx,
                       const double* vy, const double* vz, const double* m, const unsigned char* flags, double* ax,
@@ -1621,6 +1632,12 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
   }
   k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, o, opot, oax, oay, oaz, ojx, ojy, ojz);
   ctx->launches++;
+  const bool keep_amag = ctx->prm.selector > 0 && !timestep && !ctx->direct;
+  if (keep_amag) {  // the next evaluation's per-target error budget
+    TC_CK(ctx->amag.ensure(N));
+    k_amag<<<nblocks(n, 256), 256, 0, st>>>(n, oax, oay, oaz, ctx->amag.p);
+    ctx->launches++;
+  }
   if (timestep) {
     k_scatter_one<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, ctx->tsum.p, ots);
     ctx->launches++;
@@ -1639,6 +1656,7 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
   }
   TC_CK(cudaStreamSynchronize(st));
   TC_CK(cudaGetLastError());
+  ctx->amag_n = keep_amag ? n : -1;
   return finish_stats(ctx, n, herr);
 }
 
@@ -1671,14 +1689,18 @@ static void graph_signature(const tc_ctx* c, std::vector<const void*>& s) {
                         c->split_off.p, c->expn.p,     c->front[0].p,  c->front[1].p,  c->m2l.p,
                         c->m2l_alt.p,  c->p2p.p,       c->p2p_alt.p,   c->m2l_start.p, c->m2l_src.p,
                         c->p2p_start.p, c->p2p_src.p,  c->m2l_tl.p,    c->p2p_tl.p,    c->leaves.p,
-                        c->judge_idx.p, c->judge_out.p, c->p2p_part.p, c->bpart.p,     c->tc_bins.p};
+                        c->judge_idx.p, c->judge_out.p, c->p2p_part.p, c->bpart.p,     c->tc_bins.p,
+                        c->amag.p,      c->body_scale.p, c->cell_scale.p, c->m2l_src2.p, c->m2l_off.p,
+                        c->cell_pn.p,   c->mlp_w.p};
   s.assign(bufs, bufs + sizeof(bufs) / sizeof(bufs[0]));
   const size_t caps[] = {c->ccap, c->mcap, c->pcap, c->fcap, c->expn.n, c->p2p_part.n};
   for (size_t v : caps) s.push_back((const void*)(uintptr_t)v);
 }
 
+constexpr unsigned kGraphCapBits = TC_EBIT_CELL_CAP | TC_EBIT_M2L_CAP | TC_EBIT_P2P_CAP | TC_EBIT_FRONTIER_CAP;
+
 static bool graph_key_equal(const TcGraphKey& a, const TcGraphKey& b) {
-  if (a.n != b.n || a.mem != b.mem) return false;
+  if (a.n != b.n || a.mem != b.mem || a.step_dt != b.step_dt) return false;
   for (int i = 0; i < 15; i++)
     if (a.ptr[i] != b.ptr[i]) return false;
   return memcmp(&a.prm, &b.prm, sizeof(tc_params)) == 0;
@@ -1714,6 +1736,13 @@ static void graph_issue(tc_ctx* ctx, int n, const double* const* in, const unsig
       df = ctx->in_f.p;
     }
   }
+  const double sdt = ctx->gstep_dt;
+  if (sdt != 0.0) {  // leapfrog step: kick by the previous accelerations and drift, in place
+    k_kick_drift<<<nblocks(n, 256), 256, 0, st>>>(n, (double*)in[0], (double*)in[1], (double*)in[2], (double*)in[4],
+                                                  (double*)in[5], (double*)in[6], outp[0], outp[1], outp[2],
+                                                  0.5 * sdt, sdt);
+    L++;
+  }
   cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st);
   TcBodies b = bodies_view(ctx, n, jerk);
   const int nb = 148 * 4;
@@ -1746,6 +1775,15 @@ static void graph_issue(tc_ctx* ctx, int n, const double* const* in, const unsig
   }
   k_scatter_out<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, o, opot, oax, oay, oaz, ojx, ojy, ojz);
   L += 1;
+  if (ctx->prm.selector > 0) {  // the next replay's per-target error budget
+    k_amag<<<nblocks(n, 256), 256, 0, st>>>(n, oax, oay, oaz, ctx->amag.p);
+    L++;
+  }
+  if (sdt != 0.0) {  // closing kick by the new accelerations (not after a capacity overflow)
+    k_kick_guarded<<<nblocks(n, 256), 256, 0, st>>>(n, (double*)in[4], (double*)in[5], (double*)in[6], outp[0],
+                                                    outp[1], outp[2], 0.5 * sdt, ctx->d_err, kGraphCapBits);
+    L++;
+  }
   graph_event(ctx, 7, st);
   if (mem == TC_MEM_HOST) {
     double* s = ctx->out_d.p;
@@ -1756,6 +1794,7 @@ static void graph_issue(tc_ctx* ctx, int n, const double* const* in, const unsig
   TcGraphStatus* h = ctx->hstat;
   cudaMemcpyAsync(&h->err, ctx->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(h->small, ctx->d_small, 4 * sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+  if (ctx->gselect) cudaMemcpyAsync(h->hist, ctx->d_hist, 32 * sizeof(unsigned), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(&h->lv, ctx->d_lv, sizeof(TcLevels), cudaMemcpyDeviceToHost, st);
   cudaMemcpyAsync(&h->cnt, ctx->d_cnt, sizeof(TcTravCounters), cudaMemcpyDeviceToHost, st);
   graph_check(ctx, "judge, outputs and status");
@@ -1766,7 +1805,8 @@ static void graph_issue(tc_ctx* ctx, int n, const double* const* in, const unsig
 static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* const* in, const unsigned char* flags,
                        double* const* outp, int mem, bool jerk) {
   graph_drop(ctx);
-  if (ctx->direct || ctx->prm.selector > 0 || ctx->prm.precision == TC_PREC_MIXED_M2L || ctx->emac) return;
+  if (ctx->direct || ctx->prm.precision == TC_PREC_MIXED_M2L || ctx->emac) return;
+  if (ctx->prm.selector == 2 && !ctx->mlp_ready) return;
   graph_fn f = pick_graph(ctx->prm.p, jerk);
   if (!f) return;
   if (mem == TC_MEM_HOST) {
@@ -1798,6 +1838,12 @@ static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* 
       ctx->expn.ensure(ccap * NT * (jerk ? 4 : 2)) || ctx->bpart.ensure(6 * 148 * 4) ||
       (p2p_nsplit(n) > 1 && ctx->p2p_part.ensure((size_t)p2p_nsplit(n) * (jerk ? 7 : 4) * N)))
     return;
+  if (ctx->prm.selector > 0 &&
+      (ctx->cell_pn.ensure(ccap * (ctx->prm.p + 1)) || ctx->cell_scale.ensure(ccap) || ctx->body_scale.ensure(N) ||
+       ctx->amag.ensure(N) || ctx->m2l_src2.ensure(ctx->m2l_src.n) || ctx->m2l_off.ensure(ctx->m2l_src.n)))
+    return;
+  // orders are selected in the graph once an evaluation of these bodies left its |a| behind
+  ctx->gselect = ctx->prm.selector > 0 && ctx->amag_n == n;
   int sb = 1;
   while (((size_t)1 << sb) < ccap) sb++;
   ctx->gsbits = sb;
@@ -1871,10 +1917,11 @@ static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* 
 static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const double* y, const double* z,
                                 const double* vx, const double* vy, const double* vz, const double* m,
                                 const unsigned char* flags, double* ax, double* ay, double* az, double* pot,
-                                double* jx, double* jy, double* jz, int mem) {
+                                double* jx, double* jy, double* jz, int mem, double step_dt) {
   TcGraphKey key;
   key.n = n;
   key.mem = mem;
+  key.step_dt = step_dt;
   const void* ptrs[15] = {x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz};
   for (int i = 0; i < 15; i++) key.ptr[i] = ptrs[i];
   key.prm = ctx->prm;
@@ -1889,8 +1936,7 @@ static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const doubl
     TC_CK(cudaGraphLaunch(ctx->gexec, ctx->stream));
     TC_CK(cudaStreamSynchronize(ctx->stream));
     const TcGraphStatus& h = *ctx->hstat;
-    const unsigned cap_bits = TC_EBIT_CELL_CAP | TC_EBIT_M2L_CAP | TC_EBIT_P2P_CAP | TC_EBIT_FRONTIER_CAP;
-    if (!(h.err & cap_bits)) {
+    if (!(h.err & kGraphCapBits)) {
       ctx->n = n;
       ctx->direct = 0;
       ctx->ncell = h.lv.ncell;
@@ -1911,6 +1957,8 @@ static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const doubl
       ctx->class_order[0] = ctx->prm.p;
       ctx->class_pairs[0] = (long long)ctx->n_m2l;
       ctx->flop_frac = 1.0;
+      if (ctx->gselect) order_stats(ctx, ctx->prm.p, h.hist);
+      if (ctx->prm.selector > 0) ctx->amag_n = n;  // the replay left its |a| for the next one
       ctx->judge_redo = 0;
       ctx->judge_rms = 0.0;
       if (ctx->gjudge_nt > 0) {
@@ -1923,15 +1971,50 @@ static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const doubl
         }
         ctx->judge_rms = sqrt(sacc / ctx->gjudge_nt);
       }
+      if (ctx->gselect && step_dt == 0.0 && ctx->prm.judge_tol > 0 && ctx->judge_rms > ctx->prm.judge_tol) {
+        // the judge rejected the selected orders: redo this evaluation at the fixed order (a
+        // step's kicks are already applied, so a captured step only reports judge_rms)
+        const int sel = ctx->prm.selector;
+        ctx->prm.selector = 0;
+        tc_status rr = evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, mem, nullptr);
+        ctx->prm.selector = sel;
+        ctx->amag_n = n;
+        if (rr == TC_OK) ctx->judge_redo = 1;
+        return rr;
+      }
       return finish_stats(ctx, n, h.err);
     }
     ctx->gvalid = false;  // a capacity overflowed: re-run on the normal path and re-plan
+    if (step_dt != 0.0) {
+      // the replay already kicked and drifted (and skipped its closing kick): redo the
+      // evaluation and the closing kick only
+      tc_status rs = evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, mem, nullptr);
+      if (rs != TC_OK) return rs;
+      k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, (double*)x, (double*)y, (double*)z, (double*)vx,
+                                                             (double*)vy, (double*)vz, ax, ay, az, 0.5 * step_dt,
+                                                             0.0);
+      const double* in[7] = {x, y, z, m, vx, vy, vz};
+      double* outp[7] = {ax, ay, az, pot, jx, jy, jz};
+      ctx->gstep_dt = step_dt;
+      graph_plan(ctx, n, key, in, flags, outp, mem, jerk);
+      ctx->gstep_dt = 0.0;
+      return TC_OK;
+    }
   }
+  if (step_dt != 0.0)
+    k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, (double*)x, (double*)y, (double*)z, (double*)vx,
+                                                           (double*)vy, (double*)vz, ax, ay, az, 0.5 * step_dt,
+                                                           step_dt);
   tc_status rs = evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, flags, ax, ay, az, pot, jx, jy, jz, mem, nullptr);
+  if (rs == TC_OK && step_dt != 0.0)
+    k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, (double*)x, (double*)y, (double*)z, (double*)vx,
+                                                           (double*)vy, (double*)vz, ax, ay, az, 0.5 * step_dt, 0.0);
   if (rs == TC_OK) {
     const double* in[7] = {x, y, z, m, vx, vy, vz};
     double* outp[7] = {ax, ay, az, pot, jx, jy, jz};
+    ctx->gstep_dt = step_dt;
     graph_plan(ctx, n, key, in, flags, outp, mem, jerk);
+    ctx->gstep_dt = 0.0;
   }
   return rs;
 }
@@ -2006,6 +2089,7 @@ tc_status tc_direct_sums(tc_ctx* ctx, int n, const double* x, const double* y, c
   b.vx = bb + 4 * N; b.vy = bb + 5 * N; b.vz = bb + 6 * N;
   b.flags = ctx->ds_flags.p;
   b.perm = ctx->ds_idx.p;
+  b.eps2 = ctx->prm.softening * ctx->prm.softening;
   k_identity<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->ds_idx.p);
   k_gather_bodies<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->ds_idx.p, dx, dy, dz, dm, dvx, dvy, dvz, df, b);
   const int nchunk = std::max(1, std::min(4 * ctx->nsm, n / 1024));
@@ -2030,6 +2114,33 @@ tc_status tc_kick_drift(tc_ctx* ctx, int n, double* x, double* y, double* z, dou
   if (!ctx || n <= 0 || !x || !y || !z || !vx || !vy || !vz || !ax || !ay || !az) return TC_ERR_ARG;
   TC_CK(cudaSetDevice(ctx->prm.device));
   k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, vx, vy, vz, ax, ay, az, dt_kick, dt_drift);
+  TC_CK(cudaGetLastError());
+  return TC_OK;
+}
+
+tc_status tc_set_wait_limit(tc_ctx* ctx, long long cycles) {
+  if (!ctx) return TC_ERR_ARG;
+  ctx->wait_limit = cycles > 0 ? cycles : kTcWaitLimit;
+  graph_drop(ctx);
+  return TC_OK;
+}
+
+tc_status tc_step_leapfrog(tc_ctx* ctx, int n, double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                           const double* m, double* ax, double* ay, double* az, double* pot, double* jx, double* jy,
+                           double* jz, double dt) {
+  if (!ctx || n <= 0 || !x || !y || !z || !vx || !vy || !vz || !m || !ax || !ay || !az || !pot ||
+      !(dt != 0.0) || !std::isfinite(dt))
+    return TC_ERR_ARG;
+  TC_CK(cudaSetDevice(ctx->prm.device));
+  ctx->steps = false;
+  if (ctx->graph_on)
+    return evaluate_graph(ctx, n, x, y, z, vx, vy, vz, m, nullptr, ax, ay, az, pot, jx, jy, jz, TC_MEM_DEVICE, dt);
+  k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, vx, vy, vz, ax, ay, az, 0.5 * dt, dt);
+  TC_CK(cudaGetLastError());
+  tc_status r = evaluate_impl(ctx, n, x, y, z, vx, vy, vz, m, nullptr, ax, ay, az, pot, jx, jy, jz, TC_MEM_DEVICE,
+                              nullptr);
+  if (r != TC_OK) return r;
+  k_kick_drift<<<nblocks(n, 256), 256, 0, ctx->stream>>>(n, x, y, z, vx, vy, vz, ax, ay, az, 0.5 * dt, 0.0);
   TC_CK(cudaGetLastError());
   return TC_OK;
 }

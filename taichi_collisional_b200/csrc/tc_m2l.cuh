@@ -26,6 +26,11 @@
 
 namespace tc {
 
+// M2L source lists: bits 0-26 the source cell, bits 27-31 how many orders below the kernel's
+// order the pair may be evaluated at (0 = full order; written by the order selectors)
+constexpr int kM2LOrderShift = 27;
+constexpr int kM2LSrcMask = (1 << kM2LOrderShift) - 1;
+
 __constant__ double c_fc[TC_NTERM(TC_PMAX_DEV)];
 __constant__ double c_fcinv[TC_NTERM(TC_PMAX_DEV)];
 
@@ -234,9 +239,11 @@ __device__ __forceinline__ void tc_tm_to_f64(uint32_t* r, double* v) {
   }
 }
 
+// qb (<= P): the batch's expansion order -- translation terms with n + k > qb are left out, as an
+// order-qb M2L does (the caller skips output degrees N > qb)
 template <int P, int N>
 __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int lane, cd ez1, cd ex1,
-                                            uint32_t tacc, bool valid) {
+                                            uint32_t tacc, bool valid, int qb) {
   double l[2 * N + 1], o[2 * N + 1];
 #pragma unroll
   for (int k = 0; k < 2 * N + 1; k++) l[k] = 0.0;
@@ -247,7 +254,7 @@ __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int 
   {
     double s = 0.0, pr = pn;
 #pragma unroll 1
-    for (int k = 0; k <= P - N; k++) {
+    for (int k = 0; k <= qb - N; k++) {
       s += buf[(k * k + k) * 32 + lane] * (c_fact[N + k] * pr);
       pr *= rinv;
     }
@@ -259,7 +266,7 @@ __device__ __forceinline__ void tc_m2l_back(const double* buf, double rinv, int 
   for (int m = 1; m <= MMAX; m++) {
     double sn = 0.0, sp = 0.0, pr = pn * pm;
 #pragma unroll 1
-    for (int k = m; k <= P - N; k++) {
+    for (int k = m; k <= qb - N; k++) {
       const double f = c_fact[N + k] * pr;
       const int b = (k * k + k) * 32 + lane;
       sn += buf[b - m * 32] * f;
@@ -310,18 +317,18 @@ struct TcM2LSmem {
 template <int Q, bool QUIRK, int W, int I>
 struct TcDegSeq {
   static constexpr int D = TcDegSets<Q>::d[W][I];
-  static __device__ __forceinline__ void fwd(const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
+  static __device__ __forceinline__ void fwd(const double* Ms, cd ez1, cd ex1, double* buf, int lane, int qb) {
     if constexpr (D >= 0) {
-      tc_m2l_fwd<Q, D, QUIRK>(Ms, ez1, ex1, buf, lane);
-      TcDegSeq<Q, QUIRK, W, I + 1>::fwd(Ms, ez1, ex1, buf, lane);
+      if (D <= qb) tc_m2l_fwd<Q, D, QUIRK>(Ms, ez1, ex1, buf, lane);
+      TcDegSeq<Q, QUIRK, W, I + 1>::fwd(Ms, ez1, ex1, buf, lane, qb);
     }
   }
   static constexpr int COL = TcM2LTmem<Q>::cols_before(W, I);
   static __device__ __forceinline__ void back(const double* buf, double rinv, int lane, cd ez1, cd ex1,
-                                              uint32_t twarp, bool valid) {
+                                              uint32_t twarp, bool valid, int qb) {
     if constexpr (D >= 0) {
-      tc_m2l_back<Q, D>(buf, rinv, lane, ez1, ex1, twarp + COL, valid);
-      TcDegSeq<Q, QUIRK, W, I + 1>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
+      if (D <= qb) tc_m2l_back<Q, D>(buf, rinv, lane, ez1, ex1, twarp + COL, valid, qb);
+      TcDegSeq<Q, QUIRK, W, I + 1>::back(buf, rinv, lane, ez1, ex1, twarp, valid, qb);
     }
   }
   // zero this warp's accumulator columns
@@ -350,20 +357,21 @@ struct TcDegSeq {
 };
 
 template <int Q, bool QUIRK>
-__device__ __forceinline__ void tc_m2l_fwd_warp(int w, const double* Ms, cd ez1, cd ex1, double* buf, int lane) {
-  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::fwd(Ms, ez1, ex1, buf, lane);
-  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::fwd(Ms, ez1, ex1, buf, lane);
-  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::fwd(Ms, ez1, ex1, buf, lane);
-  else TcDegSeq<Q, QUIRK, 3, 0>::fwd(Ms, ez1, ex1, buf, lane);
+__device__ __forceinline__ void tc_m2l_fwd_warp(int w, const double* Ms, cd ez1, cd ex1, double* buf, int lane,
+                                                int qb) {
+  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::fwd(Ms, ez1, ex1, buf, lane, qb);
+  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::fwd(Ms, ez1, ex1, buf, lane, qb);
+  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::fwd(Ms, ez1, ex1, buf, lane, qb);
+  else TcDegSeq<Q, QUIRK, 3, 0>::fwd(Ms, ez1, ex1, buf, lane, qb);
 }
 template <int Q, bool QUIRK>
 __device__ __forceinline__ void tc_m2l_back_warp(int w, const double* buf, double rinv, int lane, cd ez1, cd ex1,
-                                                 uint32_t twarp, bool valid) {
+                                                 uint32_t twarp, bool valid, int qb) {
   tc_tm_wait_st();  // the previous batch's accumulator stores
-  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
-  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
-  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
-  else TcDegSeq<Q, QUIRK, 3, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid);
+  if (w == 0) TcDegSeq<Q, QUIRK, 0, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid, qb);
+  else if (w == 1) TcDegSeq<Q, QUIRK, 1, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid, qb);
+  else if (w == 2) TcDegSeq<Q, QUIRK, 2, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid, qb);
+  else TcDegSeq<Q, QUIRK, 3, 0>::back(buf, rinv, lane, ez1, ex1, twarp, valid, qb);
 }
 template <int Q, bool QUIRK>
 __device__ __forceinline__ void tc_m2l_zero_warp(int w, uint32_t twarp) {
@@ -440,11 +448,15 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
     for (int b0 = s_beg + grp * 32; b0 < s_end; b0 += 32 * G) {
       int idx = b0 + lane;
       bool valid = idx < s_end;
-      int s = src[valid ? idx : s_beg];
+      // a source entry carries its pair's order below Q in its top bits (tc_m2l_src_order); the
+      // batch runs at the largest order of its pairs, a lower order never applied to a pair
+      const int sv = src[valid ? idx : s_beg];
+      const int s = sv & kM2LSrcMask;
+      const int qb = Q - (int)__reduce_min_sync(0xffffffffu, valid ? (unsigned)sv >> kM2LOrderShift : 31u);
       TcPairGeo pg = tc_pair_geo(Xt - c.X[s], Yt - c.Y[s], Zt - c.Z[s]);
-      tc_m2l_fwd_warp<Q, QUIRK>(w, Mbase + (size_t)s * NTP, pg.ez1, pg.ex1, buf, lane);
+      tc_m2l_fwd_warp<Q, QUIRK>(w, Mbase + (size_t)s * NTP, pg.ez1, pg.ex1, buf, lane, qb);
       tc_bar_group(grp);
-      tc_m2l_back_warp<Q, QUIRK>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, twarp, valid);
+      tc_m2l_back_warp<Q, QUIRK>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, twarp, valid, qb);
       tc_bar_group(grp);
     }
     tc_bar_cta();  // every group is done with its buffer

@@ -67,10 +67,14 @@ __device__ __forceinline__ void tc_mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
 
-// bounded wait for the phase with the given parity; false after ~2 s of device clock
-__device__ __forceinline__ bool tc_mbar_wait(uint32_t mbar, uint32_t parity) {
+// default limit of a bounded wait: ~2 s of device clock
+constexpr long long kTcWaitLimit = 4000000000ll;
+
+// bounded wait for the phase with the given parity; false after `limit` cycles of device clock
+__device__ __forceinline__ bool tc_mbar_wait(uint32_t mbar, uint32_t parity, long long limit = kTcWaitLimit) {
   long long t0 = clock64();
   for (;;) {
+    if (clock64() - t0 > limit) return false;  // checked first: a limit of a few cycles always runs out
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
@@ -79,7 +83,6 @@ __device__ __forceinline__ bool tc_mbar_wait(uint32_t mbar, uint32_t parity) {
         : "r"(mbar), "r"(parity)
         : "memory");
     if (done) return true;
-    if (clock64() - t0 > 4000000000ll) return false;
   }
 }
 
@@ -438,15 +441,19 @@ __device__ __forceinline__ void tc_tc_mma_half(uint32_t tmem, uint32_t ahi, uint
   }
 }
 
-// CTA barrier after every thread wrote its row, then one thread issues the products
+// CTA barrier after every thread wrote its row, then one thread issues the products.  The
+// barrier also makes `ok` CTA-uniform: once any thread's wait gave up, nothing more is issued
+// (`issued` counts the commits, the same on every thread).
 template <int Q, bool TRANS>
-__device__ __forceinline__ void tc_tc_issue(char* smem, uint32_t tmem, uint32_t mbar) {
+__device__ __forceinline__ void tc_tc_issue(char* smem, uint32_t tmem, uint32_t mbar, bool& ok, int& issued) {
   using SM = TcTcSmem<Q>;
   using PL = TcTcPlan<Q>;
   tc_tmem_wait_st();
   tc_fence_async_smem();
   tc_fence_before_sync();
-  __syncthreads();
+  ok = __syncthreads_and(ok) != 0;
+  if (!ok) return;
+  issued++;
   if (threadIdx.x == 0) {
     tc_fence_after_sync();
     const uint32_t ahi = tc_smem_u32(smem + SM::OFF_AHI), amid = tc_smem_u32(smem + SM::OFF_AMID);
@@ -464,7 +471,8 @@ template <int P, int Q, bool JERK>
 __global__ void __launch_bounds__(128, 1) k_m2l_tc(const int* __restrict__ tlist, int ntl,
                                                    const int* __restrict__ tstart, const int* __restrict__ src,
                                                    TcCells c, const float* __restrict__ bins,
-                                                   unsigned int* __restrict__ counter, unsigned int* __restrict__ err) {
+                                                   unsigned int* __restrict__ counter, unsigned int* __restrict__ err,
+                                                   long long wait_limit = kTcWaitLimit) {
   using PL = TcTcPlan<Q>;
   using SM = TcTcSmem<Q>;
   constexpr int NTP = (P + 1) * (P + 1);  // storage stride of M and L (order P)
@@ -503,6 +511,7 @@ __global__ void __launch_bounds__(128, 1) k_m2l_tc(const int* __restrict__ tlist
   const uint32_t tl = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's lane quarter
   uint32_t phase = 0;
   bool ok = true;
+  int issued = 0;  // commits issued (CTA-uniform)
 
   for (;;) {
     if (tid == 0) *next_slot = (int)atomicAdd(counter, 1u);
@@ -560,7 +569,7 @@ __global__ void __launch_bounds__(128, 1) k_m2l_tc(const int* __restrict__ tlist
         const double* Ms = (arr ? c.Md : c.M) + (size_t)s * NTP;
         // ---- scale, rotate about z, swap
         tc_tc_f0<Q>(Ms, valid, Q == P, tl, ah, am);
-        tc_tc_issue<Q, false>(smem, tmem, mbar);
+        tc_tc_issue<Q, false>(smem, tmem, mbar, ok, issued);
         if (arr == 0) {
           rref = fmax(fmax(wmax[0], wmax[1]), fmax(wmax[2], wmax[3]));
           const float q = rref > 0.0 ? (float)(rinv / rref) : 0.f;
@@ -572,31 +581,31 @@ __global__ void __launch_bounds__(128, 1) k_m2l_tc(const int* __restrict__ tlist
           tc_tmem_wait_st();
         }
         // ---- rotate about x, swap
-        ok = tc_mbar_wait(mbar, phase);
+        ok = ok && tc_mbar_wait(mbar, phase, wait_limit);
         phase ^= 1u;
         tc_fence_after_sync();
         tc_tc_rot_stage<Q, false>(1, tl, ah, am);
-        tc_tc_issue<Q, false>(smem, tmem, mbar);
+        tc_tc_issue<Q, false>(smem, tmem, mbar, ok, issued);
         // ---- translate along z
-        ok = ok && tc_mbar_wait(mbar, phase);
+        ok = ok && tc_mbar_wait(mbar, phase, wait_limit);
         phase ^= 1u;
         tc_fence_after_sync();
         tc_tc_f2<Q>(tl, ah, am);
-        tc_tc_issue<Q, true>(smem, tmem, mbar);
+        tc_tc_issue<Q, true>(smem, tmem, mbar, ok, issued);
         // ---- back: swap
-        ok = ok && tc_mbar_wait(mbar, phase);
+        ok = ok && tc_mbar_wait(mbar, phase, wait_limit);
         phase ^= 1u;
         tc_fence_after_sync();
         tc_tc_b0<Q>(tl, ah, am);
-        tc_tc_issue<Q, false>(smem, tmem, mbar);
+        tc_tc_issue<Q, false>(smem, tmem, mbar, ok, issued);
         // ---- rotate back about x, swap
-        ok = ok && tc_mbar_wait(mbar, phase);
+        ok = ok && tc_mbar_wait(mbar, phase, wait_limit);
         phase ^= 1u;
         tc_fence_after_sync();
         tc_tc_rot_stage<Q, true>(1, tl, ah, am);
-        tc_tc_issue<Q, false>(smem, tmem, mbar);
+        tc_tc_issue<Q, false>(smem, tmem, mbar, ok, issued);
         // ---- rotate back about z, scale relative to the tile's 1/r, sum the tile's rows
-        ok = ok && tc_mbar_wait(mbar, phase);
+        ok = ok && tc_mbar_wait(mbar, phase, wait_limit);
         phase ^= 1u;
         tc_fence_after_sync();
         tc_tc_b2<Q>(tl, red + warp * PL::AW, lane);
@@ -638,7 +647,13 @@ __global__ void __launch_bounds__(128, 1) k_m2l_tc(const int* __restrict__ tlist
     }
     if (!ok) break;
   }
-  if (!ok && tid == 0) atomicOr(err, TC_EBIT_TIMEOUT);
+  ok = __syncthreads_and(ok) != 0;
+  if (!ok) {
+    // a wait gave up: nothing was issued after it, so at most the last commit is outstanding;
+    // wait for it with the default limit before the tensor memory it writes is freed
+    if (issued > 0) tc_mbar_wait(mbar, (uint32_t)((issued - 1) & 1), kTcWaitLimit);
+    if (tid == 0) atomicOr(err, TC_EBIT_TIMEOUT);
+  }
   tc_fence_before_sync();
   __syncthreads();
   if (warp == 0)

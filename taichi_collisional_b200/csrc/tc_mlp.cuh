@@ -177,38 +177,4 @@ __global__ void k_mlp_adam(int np, float* __restrict__ w, float* __restrict__ g,
   g[i] = 0.f;
 }
 
-// learned selector: features -> predicted log10 errors -> smallest class under log10(tol)
-template <int P>
-__global__ void k_select_mlp(const unsigned long long* __restrict__ keys, unsigned long long n, int sbits, TcCells c,
-                             const double* __restrict__ pn, const float* __restrict__ w, TcMlpNorm norm,
-                             float log10_tol, unsigned long long* __restrict__ out, unsigned int* __restrict__ hist) {
-  using OC = TcOrderClasses<P>;
-  __shared__ float sw[kMlpParamMax];
-  __shared__ unsigned int h[TC_MAX_CLASSES];
-  const int nout = OC::n;
-  for (int i = threadIdx.x; i < tc_mlp_nparam(nout); i += blockDim.x) sw[i] = w[i];
-  if (threadIdx.x < TC_MAX_CLASSES) h[threadIdx.x] = 0;
-  __syncthreads();
-  const unsigned long long mask = (1ull << sbits) - 1ull;
-  for (unsigned long long k = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; k < n;
-       k += (unsigned long long)gridDim.x * blockDim.x) {
-    unsigned long long key = keys[k];
-    int t = (int)(key >> sbits), s = (int)(key & mask);
-    float x[kMlpIn], a1[kMlpH], a2[kMlpH], a3[kMlpH], y[kMlpOutMax];
-    tc_pair_features(c, t, s, pn, P, x);
-    for (int i = 0; i < kMlpIn; i++) x[i] = (x[i] - norm.mean[i]) * norm.inv_std[i];
-    tc_mlp_forward<true>(sw, nout, x, a1, a2, a3, y);
-    int cls = nout - 1;
-    for (int i = 0; i < nout - 1; i++)
-      if (y[i] + norm.out_mean <= log10_tol) {
-        cls = i;
-        break;
-      }
-    out[k] = ((unsigned long long)cls << (2 * sbits)) | key;
-    atomicAdd(&h[cls], 1u);
-  }
-  __syncthreads();
-  if (threadIdx.x < TC_MAX_CLASSES && h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], h[threadIdx.x]);
-}
-
 }  // namespace tc

@@ -53,7 +53,7 @@ __device__ __forceinline__ void tc_p2p_one(double xi, double yi, double zi, doub
   double dx = b.x[j] - xi, dy = b.y[j] - yi, dz = b.z[j] - zi;
   double r2 = dx * dx + dy * dy + dz * dz;
   if (!(r2 > 0.0)) return;
-  double invr = rsqrt(r2), invr2 = invr * invr;
+  double invr = rsqrt(r2 + b.eps2), invr2 = invr * invr;
   double f = b.m[j] * invr;
   a.pot += f;
   f *= invr2;
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kJudgeTile) k_direct_targets(int n, int nt, in
       const double dx = sx[q] - xi, dy = sy[q] - yi, dz = sz[q] - zi;
       const double r2 = dx * dx + dy * dy + dz * dz;
       if (r2 > 0.0) {
-        const double invr = rsqrt(r2), invr2 = invr * invr;
+        const double invr = rsqrt(r2 + b.eps2), invr2 = invr * invr;
         const double f = sm[q] * invr;
         pot += f;
         const double f3 = f * invr2;
@@ -508,134 +508,227 @@ __device__ __forceinline__ void tc_split(double x, double c, float& h, float& l)
   l = (float)(d - (double)h);
 }
 
+// ---------------------------------------------------------------------------------------
+// k_p2p_mixed: the mixed-precision near field.
+//
+// One warp per target leaf, one target per lane; a last pass of r <= 16 targets runs
+// floor(32 / r) lane groups, each over every ng-th source of each 32-source tile (so small
+// leaves still fill the warp).
+//
+// Accuracy.  The FP32 pair terms carry a few units of 2^-24 each, and so does their per-tile
+// FP32 sum -- relative to the largest term in the sum.  A term far larger than the target's
+// acceleration would leave an error far larger than the FMM's own.  So every pair whose
+// strength m / r^2 exceeds tau = excl_frac |a_far| (the target's far-field acceleration,
+// which the downward pass has already written into out) is left out of the FP32 sums and
+// recorded; after the loop the recorded pairs are added in FP64.  For a target with more than
+// kP2PRec strong pairs (a zero far field makes every pair strong) the whole warp runs a second
+// pass over its sources that adds every strong pair in FP64 (the same FP32 test decides).
+// Sources are staged per tile as FP32 (hi, lo) pairs of positions relative to the target
+// cell's centre and of masses, so dx = (xj_hi - xi_hi) + (xj_lo - xi_lo) has one rounding even
+// for close pairs; 1/r is the hardware estimate refined by one Newton step; each tile's FP32
+// sums are folded into (hi, lo) accumulators by a two-sum; the final sums are FP64.
+// ---------------------------------------------------------------------------------------
+constexpr int kP2PRec = 16;
+// strong-pair threshold: pairs with m / r^2 above this fraction of the far-field acceleration
+// are summed in FP64
+constexpr float kP2PExclFrac = 1e-2f;
+
 template <bool JERK>
-__global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
+struct TcMix2 {  // one target's FP32 state
+  float xh, yh, zh, xl, yl, zl, vx, vy, vz, tau, eps2;
+  float sp, sx, sy, sz, qx, qy, qz;  // this tile's sums
+  TcF2 pot, ax, ay, az, jx, jy, jz;  // compensated totals
+};
+
+// the FP32 geometry of one pair: difference, 1/r, m/r, and whether m/r^2 exceeds the target's
+// threshold.  The only definition of "strong": the main loop and the overflow pass both call it.
+template <bool JERK>
+__device__ __forceinline__ bool tc_mix2_geom(const TcMix2<JERK>& T, const float4 s0, const float4 s1, float2& dxy,
+                                             float& dz, float& ri, float& f0) {
+  dxy = __fadd2_rn(__fadd2_rn(make_float2(s0.x, s0.y), make_float2(-T.xh, -T.yh)),
+                   __fadd2_rn(make_float2(s0.z, s0.w), make_float2(-T.xl, -T.yl)));
+  dz = __fadd_rn(__fsub_rn(s1.x, T.zh), __fsub_rn(s1.y, T.zl));
+  const float r2 = __fmaf_rn(dxy.x, dxy.x, __fmaf_rn(dxy.y, dxy.y, __fmul_rn(dz, dz)));
+  ri = 0.f;
+  if (r2 > 0.f) {
+    const float rs = __fadd_rn(r2, T.eps2);  // softened (eps2 = 0: unchanged)
+    const float y = rsqrtf(rs);
+    const float e = __fmaf_rn(-__fmul_rn(rs, y), y, 1.f);
+    ri = __fmaf_rn(__fmul_rn(0.5f, y), e, y);
+  }
+  f0 = __fmaf_rn(s1.w, ri, __fmul_rn(s1.z, ri));
+  return __fmul_rn(f0, ri) > T.tau;  // m / r^2 above the target's threshold: FP64 instead
+}
+
+// a source body as the tile stages it: (xh, yh, xl, yl) (zh, zl, mh, ml) relative to the target
+// cell's centre
+__device__ __forceinline__ void tc_mix2_source(const TcBodies& b, int j, double Xc, double Yc, double Zc, float4& s0,
+                                               float4& s1) {
+  tc_split(b.x[j], Xc, s0.x, s0.z);
+  tc_split(b.y[j], Yc, s0.y, s0.w);
+  tc_split(b.z[j], Zc, s1.x, s1.y);
+  tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, s1.z, s1.w);
+}
+
+template <bool JERK>
+__device__ __forceinline__ void tc_mix2_pair(TcMix2<JERK>& T, const float4 s0, const float4 s1, const float4 s2,
+                                             bool& strong) {
+  float2 dxy;
+  float dz, ri, f0;
+  strong = tc_mix2_geom<JERK>(T, s0, s1, dxy, dz, ri, f0);
+  if (strong) f0 = 0.f;
+  const float ri2 = __fmul_rn(ri, ri);
+  const float f = __fmul_rn(f0, ri2);
+  T.sp = __fadd_rn(T.sp, f0);
+  T.sx = __fmaf_rn(dxy.x, f, T.sx);
+  T.sy = __fmaf_rn(dxy.y, f, T.sy);
+  T.sz = __fmaf_rn(dz, f, T.sz);
+  if (JERK) {
+    const float dvx = __fsub_rn(s2.x, T.vx), dvy = __fsub_rn(s2.y, T.vy), dvz = __fsub_rn(s2.z, T.vz);
+    const float vr = __fmul_rn(3.f, __fmaf_rn(dxy.x, dvx, __fmaf_rn(dxy.y, dvy, __fmul_rn(dz, dvz))));
+    const float g = __fmul_rn(__fmul_rn(-f, ri2), vr);
+    T.qx = __fmaf_rn(dxy.x, g, __fmaf_rn(dvx, f, T.qx));
+    T.qy = __fmaf_rn(dxy.y, g, __fmaf_rn(dvy, f, T.qy));
+    T.qz = __fmaf_rn(dz, g, __fmaf_rn(dvz, f, T.qz));
+  }
+}
+
+template <bool JERK>
+__device__ __forceinline__ void tc_mix2_fold(TcMix2<JERK>& T) {
+  T.pot.add(T.sp); T.ax.add(T.sx); T.ay.add(T.sy); T.az.add(T.sz);
+  if (JERK) { T.jx.add(T.qx); T.jy.add(T.qy); T.jz.add(T.qz); }
+  T.sp = T.sx = T.sy = T.sz = T.qx = T.qy = T.qz = 0.f;
+}
+
+template <bool JERK>
+__device__ __forceinline__ void tc_mix2_init(TcMix2<JERK>& T, const TcBodies& b, const TcOut& out, int i, bool v,
+                                             double Xc, double Yc, double Zc, float excl_frac) {
+  T.xh = T.yh = T.zh = T.xl = T.yl = T.zl = T.vx = T.vy = T.vz = 0.f;
+  T.tau = 0.f;
+  T.eps2 = (float)b.eps2;
+  if (v) {
+    tc_split(b.x[i], Xc, T.xh, T.xl);
+    tc_split(b.y[i], Yc, T.yh, T.yl);
+    tc_split(b.z[i], Zc, T.zh, T.zl);
+    if (JERK) { T.vx = (float)b.vx[i]; T.vy = (float)b.vy[i]; T.vz = (float)b.vz[i]; }
+    const double a = sqrt(out.ax[i] * out.ax[i] + out.ay[i] * out.ay[i] + out.az[i] * out.az[i]);
+    T.tau = (float)(excl_frac * a);
+  }
+  T.sp = T.sx = T.sy = T.sz = T.qx = T.qy = T.qz = 0.f;
+  T.pot = T.ax = T.ay = T.az = T.jx = T.jy = T.jz = TcF2{0.f, 0.f};
+}
+
+template <bool JERK>
+__device__ __forceinline__ TcAcc<JERK> tc_mix2_total(const TcMix2<JERK>& T) {
+  TcAcc<JERK> a;
+  a.pot = T.pot.val(); a.ax = T.ax.val(); a.ay = T.ay.val(); a.az = T.az.val();
+  a.jx = T.jx.val(); a.jy = T.jy.val(); a.jz = T.jz.val();
+  return a;
+}
+
+template <bool JERK>
+__global__ void __launch_bounds__(kP2PWarps * 32, 6) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
                                                               const int* __restrict__ tstart,
                                                               const int* __restrict__ src, const TcBodies b,
-                                                              const TcCells c, TcOut out,
-    const unsigned* ntldev = nullptr) {
+                                                              const TcCells c, TcOut out, float excl_frac,
+                                                              const unsigned* ntldev = nullptr) {
   if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
-  // per warp source tile, three 16-byte vectors per source (one broadcast load each):
-  // (xh, yh, xl, yl) (zh, zl, mh, ml) (vx, vy, vz, -); x and y are consumed as packed pairs
+  // per warp: the source tile, three 16-byte vectors per source (one broadcast load each):
+  // (xh, yh, xl, yl) (zh, zl, mh, ml) (vx, vy, vz, -); the recorded strong pairs per target
   __shared__ float4 tile[kP2PWarps][32][3];
-  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4(*T)[3] = tile[w];
+  __shared__ int rec[kP2PWarps][32][kP2PRec];
+  __shared__ int nrec[kP2PWarps][32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float4(*TL)[3] = tile[w];
   for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
-    int t = tlist[k];
+    const int t = tlist[k];
     if (!c.has_sink[t]) continue;
     const double Xc = c.X[t], Yc = c.Y[t], Zc = c.Z[t];
-    int tb = c.begin[t], nt = c.nbody[t];
-    int sb = tstart[t], se = tstart[t + 1];
+    const int tb = c.begin[t], nt = c.nbody[t];
+    const int sb = tstart[t], se = tstart[t + 1];
     for (int t0 = 0; t0 < nt; t0 += 32) {
       // up to 32 targets per pass; a last pass of r <= 16 targets runs floor(32 / r) lane
       // groups of r lanes, each over every ng-th source
       const int r = min(32, nt - t0);
       const int gsz = r > 16 ? 32 : r, ng = 32 / gsz;
       const int grp = lane / gsz, ti = lane % gsz;
-      int i = tb + t0 + ti;
-      bool vi = grp < ng && (t0 + ti) < nt;
-      float xh = 0, yh = 0, zh = 0, xl = 0, yl = 0, zl = 0, vxi = 0, vyi = 0, vzi = 0;
-      if (vi) {
-        tc_split(b.x[i], Xc, xh, xl);
-        tc_split(b.y[i], Yc, yh, yl);
-        tc_split(b.z[i], Zc, zh, zl);
-        if (JERK) { vxi = (float)b.vx[i]; vyi = (float)b.vy[i]; vzi = (float)b.vz[i]; }
-      }
-      // negated target terms: x + (-y) rounds exactly as x - y, so the packed sums below
-      // give bit for bit the scalar tc_pair32 values used by the strongest-pair correction
-      const float2 nh = make_float2(-xh, -yh), nl = make_float2(-xl, -yl), nv = make_float2(-vxi, -vyi);
-      TcF2 pot = {0, 0}, ax = {0, 0}, ay = {0, 0}, az = {0, 0}, jx = {0, 0}, jy = {0, 0}, jz = {0, 0};
-      unsigned bestkey = 0u;  // strength bits of the strongest pair so far, low 5 bits cleared
-      int bj = -1;
+      const bool act = grp < ng && ti < r;
+      const int i = tb + t0 + ti;
+      nrec[w][lane] = 0;
+      TcMix2<JERK> A;
+      tc_mix2_init<JERK>(A, b, out, i, act, Xc, Yc, Zc, excl_frac);
+      __syncwarp();
       for (int q = sb; q < se; q++) {
-        int s = src[q];
-        int jb = c.begin[s], jn = c.nbody[s];
+        const int s = src[q];
+        const int jb = c.begin[s], jn = c.nbody[s];
         for (int j0 = 0; j0 < jn; j0 += 32) {
-          int cnt = min(32, jn - j0);
+          const int cnt = min(32, jn - j0);
           __syncwarp();
           if (lane < cnt) {
-            int j = jb + j0 + lane;
+            const int j = jb + j0 + lane;
             float4 s0, s1;
-            tc_split(b.x[j], Xc, s0.x, s0.z);
-            tc_split(b.y[j], Yc, s0.y, s0.w);
-            tc_split(b.z[j], Zc, s1.x, s1.y);
-            tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, s1.z, s1.w);
-            T[lane][0] = s0;
-            T[lane][1] = s1;
-            if (JERK) T[lane][2] = make_float4((float)b.vx[j], (float)b.vy[j], (float)b.vz[j], 0.f);
+            tc_mix2_source(b, j, Xc, Yc, Zc, s0, s1);
+            TL[lane][0] = s0;
+            TL[lane][1] = s1;
+            if (JERK) TL[lane][2] = make_float4((float)b.vx[j], (float)b.vy[j], (float)b.vz[j], 0.f);
           }
           __syncwarp();
-          float sp = 0, sz = 0, qz = 0;
-          float2 sxy = make_float2(0.f, 0.f), qxy = make_float2(0.f, 0.f);
-          unsigned key = 0u;  // (strength bits & ~31) | jj of this tile's strongest pair
-          if (vi) {
+          if (act) {
             for (int jj = grp; jj < cnt; jj += ng) {
-              const float4 s0 = T[jj][0], s1 = T[jj][1];
-              const float2 dxy = __fadd2_rn(__fadd2_rn(make_float2(s0.x, s0.y), nh),
-                                            __fadd2_rn(make_float2(s0.z, s0.w), nl));
-              const float dz = __fadd_rn(__fsub_rn(s1.x, zh), __fsub_rn(s1.y, zl));
-              const float r2 = __fmaf_rn(dxy.x, dxy.x, __fmaf_rn(dxy.y, dxy.y, __fmul_rn(dz, dz)));
-              float ri = 0.f;
-              if (r2 > 0.f) {
-                const float y = rsqrtf(r2);
-                const float e = __fmaf_rn(-__fmul_rn(r2, y), y, 1.f);
-                ri = __fmaf_rn(__fmul_rn(0.5f, y), e, y);
+              const float4 s0 = TL[jj][0], s1 = TL[jj][1];
+              const float4 s2 = JERK ? TL[jj][2] : make_float4(0.f, 0.f, 0.f, 0.f);
+              bool strong;
+              tc_mix2_pair<JERK>(A, s0, s1, s2, strong);
+              if (strong) {
+                const int o = atomicAdd(&nrec[w][ti], 1);
+                if (o < kP2PRec) rec[w][ti][o] = jb + j0 + jj;
               }
-              const float f0 = __fmaf_rn(s1.w, ri, __fmul_rn(s1.z, ri));
-              const float ri2 = __fmul_rn(ri, ri);
-              const float f = __fmul_rn(f0, ri2);
-              sp = __fadd_rn(sp, f0);
-              sxy = __ffma2_rn(dxy, make_float2(f, f), sxy);
-              sz = __fmaf_rn(dz, f, sz);
-              if (JERK) {
-                const float4 s2 = T[jj][2];
-                const float2 dv = __fadd2_rn(make_float2(s2.x, s2.y), nv);
-                const float dvz = __fsub_rn(s2.z, vzi);
-                const float vr = __fmul_rn(3.f, __fmaf_rn(dxy.x, dv.x, __fmaf_rn(dxy.y, dv.y, __fmul_rn(dz, dvz))));
-                const float g = __fmul_rn(__fmul_rn(-f, ri2), vr);
-                qxy = __ffma2_rn(dxy, make_float2(g, g), __ffma2_rn(dv, make_float2(f, f), qxy));
-                qz = __fmaf_rn(dz, g, __fmaf_rn(dvz, f, qz));
-              }
-              // m / r^2 >= 0, so its bits order like the value
-              key = max(key, (__float_as_uint(__fmul_rn(f0, ri)) & ~31u) | (unsigned)jj);
             }
           }
-          if ((key & ~31u) > bestkey) {
-            bestkey = key & ~31u;
-            bj = jb + j0 + (int)(key & 31u);
-          }
-          pot.add(sp); ax.add(sxy.x); ay.add(sxy.y); az.add(sz);
-          if (JERK) { jx.add(qxy.x); jy.add(qxy.y); jz.add(qz); }
+          tc_mix2_fold<JERK>(A);
         }
       }
-      TcAcc<JERK> a;
-      a.pot = pot.val(); a.ax = ax.val(); a.ay = ay.val(); a.az = az.val();
-      a.jx = jx.val(); a.jy = jy.val(); a.jz = jz.val();
-      if (vi && bj >= 0) {
-        // the strongest pair: remove its FP32 terms exactly, add its FP64 value
-        const int j = bj;
-        float sxh, syh, szh, sxl, syl, szl, mh, ml;
-        tc_split(b.x[j], Xc, sxh, sxl);
-        tc_split(b.y[j], Yc, syh, syl);
-        tc_split(b.z[j], Zc, szh, szl);
-        tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, mh, ml);
-        TcPair32 v = tc_pair32<JERK>(sxh, syh, szh, sxl, syl, szl, mh, ml, JERK ? (float)b.vx[j] : 0.f,
-                                     JERK ? (float)b.vy[j] : 0.f, JERK ? (float)b.vz[j] : 0.f, xh, yh, zh, xl, yl,
-                                     zl, vxi, vyi, vzi);
-        a.pot -= (double)v.f0;
-        a.ax -= (double)v.dx * (double)v.f;
-        a.ay -= (double)v.dy * (double)v.f;
-        a.az -= (double)v.dz * (double)v.f;
-        if (JERK) {
-          a.jx -= (double)v.dvx * (double)v.f + (double)v.dx * (double)v.g;
-          a.jy -= (double)v.dvy * (double)v.f + (double)v.dy * (double)v.g;
-          a.jz -= (double)v.dvz * (double)v.f + (double)v.dz * (double)v.g;
-        }
-        tc_p2p_one<JERK>(b.x[i], b.y[i], b.z[i], JERK ? b.vx[i] : 0.0, JERK ? b.vy[i] : 0.0, JERK ? b.vz[i] : 0.0,
-                         b, j, a);
-      }
+      __syncwarp();
+      TcAcc<JERK> a = tc_mix2_total<JERK>(A);
       a.add_groups(gsz, ng, grp);
-      if (vi && grp == 0 && (b.flags[i] & 1)) {
+      // group 0 finishes its targets: the recorded strong pairs in FP64; a target whose record
+      // list overflowed gets all its strong pairs from a second, warp-wide pass
+      const bool own = act && grp == 0;
+      const int nr = own ? nrec[w][ti] : 0;
+      if (own && nr <= kP2PRec) {
+        const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
+        const double vxi = JERK ? b.vx[i] : 0.0, vyi = JERK ? b.vy[i] : 0.0, vzi = JERK ? b.vz[i] : 0.0;
+        for (int e = 0; e < nr; e++) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, rec[w][ti][e], a);
+      }
+      unsigned mo = __ballot_sync(0xffffffffu, own && nr > kP2PRec);
+      while (mo) {
+        const int owner = __ffs(mo) - 1;
+        mo &= mo - 1;
+        const int io = tb + t0 + owner;
+        TcMix2<JERK> T;
+        tc_mix2_init<JERK>(T, b, out, io, true, Xc, Yc, Zc, excl_frac);
+        const double xi = b.x[io], yi = b.y[io], zi = b.z[io];
+        const double vxi = JERK ? b.vx[io] : 0.0, vyi = JERK ? b.vy[io] : 0.0, vzi = JERK ? b.vz[io] : 0.0;
+        TcAcc<JERK> s64;
+        s64.zero();
+        for (int q = sb; q < se; q++) {
+          const int s = src[q];
+          for (int j = c.begin[s] + lane; j < c.begin[s] + c.nbody[s]; j += 32) {
+            float4 s0, s1;
+            tc_mix2_source(b, j, Xc, Yc, Zc, s0, s1);
+            float2 dxy;
+            float dz, ri, f0;
+            if (tc_mix2_geom<JERK>(T, s0, s1, dxy, dz, ri, f0)) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, j, s64);
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s64.add_xor(o);
+        if (lane == owner) {
+          a.pot += s64.pot; a.ax += s64.ax; a.ay += s64.ay; a.az += s64.az;
+          if (JERK) { a.jx += s64.jx; a.jy += s64.jy; a.jz += s64.jz; }
+        }
+      }
+      if (own && (b.flags[i] & 1)) {
         out.pot[i] += a.pot;
         out.ax[i] += a.ax;
         out.ay[i] += a.ay;
@@ -646,6 +739,7 @@ __global__ void __launch_bounds__(kP2PWarps * 32) k_p2p_mixed(const int* __restr
           out.jz[i] += a.jz;
         }
       }
+      __syncwarp();
     }
   }
 }

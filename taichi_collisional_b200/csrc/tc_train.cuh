@@ -40,9 +40,9 @@ __global__ void __launch_bounds__(128) k_m2l_pairs(int K, const int* __restrict_
   const uint32_t twarp = s_tmem + ((uint32_t)(32 * w) << 16);
   tc_m2l_zero_warp<Q, false>(w, twarp);
   TcPairGeo pg = tc_pair_geo(c.X[t] - c.X[s], c.Y[t] - c.Y[s], c.Z[t] - c.Z[s]);
-  tc_m2l_fwd_warp<Q, false>(w, c.M + (size_t)s * NTP, pg.ez1, pg.ex1, buf, lane);
+  tc_m2l_fwd_warp<Q, false>(w, c.M + (size_t)s * NTP, pg.ez1, pg.ex1, buf, lane, Q);
   __syncthreads();
-  tc_m2l_back_warp<Q, false>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, twarp, valid);
+  tc_m2l_back_warp<Q, false>(w, buf, pg.rinv, lane, pg.ez1, pg.ex1, twarp, valid, Q);
   tc_m2l_readout_warp<Q, false>(w, twarp, acc, lane);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();

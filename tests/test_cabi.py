@@ -31,8 +31,10 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layouts_match_header():
     # tc_params: int p, int ncrit, double theta, int variant, int precision, int use_shift,
-    # double shift_u[3], int direct_below, int device
-    assert C.sizeof(tcb.Params) == 4 + 4 + 8 + 4 + 4 + 4 + 4 + 24 + 4 + 4 + 4 + 4 + 8 + 4 + 4 + 8 + 8
+    # double shift_u[3], int direct_below, int device, int selector, double selector_tol,
+    # int judge_n, double judge_tol, unsigned long long judge_seed, double softening
+    assert C.sizeof(tcb.Params) == 4 + 4 + 8 + 4 + 4 + 4 + 4 + 24 + 4 + 4 + 4 + 4 + 8 + 4 + 4 + 8 + 8 + 8
+    assert tcb.Params.softening.offset == 104
     assert tcb.Params.theta.offset == 8
     assert tcb.Params.shift_u.offset == 32
 
@@ -51,7 +53,8 @@ def test_defaults_and_orders():
 def test_create_rejects_bad_params_without_touching_the_gpu():
     L = tcb.load_library()
     h = C.c_void_p()
-    for bad in (dict(p=0), dict(p=17), dict(ncrit=0), dict(theta=0.0), dict(variant=5), dict(precision=9)):
+    for bad in (dict(p=0), dict(p=17), dict(ncrit=0), dict(theta=0.0), dict(variant=5), dict(precision=9),
+                dict(softening=-1.0), dict(softening=float("nan"))):
         prm = tcb.default_params(**bad)
         rc = L.tc_create(C.byref(prm), C.byref(h))
         assert rc in (1, 6), (bad, rc)

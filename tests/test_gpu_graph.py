@@ -144,3 +144,28 @@ def test_graph_survives_buffer_reallocation_by_other_calls():
         for k in ref:
             np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
     assert g.graph_ready()
+
+
+def test_whole_leapfrog_step_as_one_graph():
+    """tc_step_leapfrog with the graph on (kick-drift, evaluation, judge and kick captured as one
+    graph) gives the same bits, step after step, as the same steps launched directly."""
+    n = 1 << 15
+    t, d = _setup(n, seed=9)
+    d2 = {k: v.clone() for k, v in d.items()}
+    g = t.Gravity(p=10, ncrit=64, theta=0.4, variant=t.VARIANT_JERKS, precision=t.PREC_MIXED, judge_n=32)
+    gd = t.Gravity(p=10, ncrit=64, theta=0.4, variant=t.VARIANT_JERKS, precision=t.PREC_MIXED, judge_n=32)
+    g.set_graph(True)
+    out, out2 = _outs(n), _outs(n)
+    for o in (out, out2):
+        for v in o.values():
+            v.zero_()
+    for step in range(4):
+        g.step_leapfrog(d, out, 1.0 / 2048)
+        gd.step_leapfrog(d2, out2, 1.0 / 2048)
+        torch.cuda.synchronize()
+        if step:
+            assert g.graph_ready(), g.graph_note()
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert torch.equal(d[k], d2[k]), (k, step)
+        for k in out:
+            assert torch.equal(out[k], out2[k]), (k, step)

@@ -1,0 +1,55 @@
+"""The mixed-precision form at the headline's order: FP32 near field (strong pairs in FP64),
+FP64 far field, at p = 12, theta = 0.4, ncrit = 64 on Plummer spheres with Kroupa masses.
+
+The bar (the headline condition): the RMS relative acceleration error against FP64 direct
+sums at 4,096 seeded bodies is at most 1.1 times the plain FP64 form's, on three seeds, each
+on its initial state and on a state moved by leapfrog steps (close encounters and massive
+stars shift which pairs dominate a body's near field)."""
+import numpy as np
+import pytest
+
+import taichi_collisional_b200 as tcb
+from taichi_collisional_b200 import ics
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+RATIO = 1.1
+N = 1 << 20
+TARGETS = 4096
+
+
+def _err(out, ref, idx_t):
+    got = torch.stack([out["a" + c][idx_t] for c in "xyz"], 1).cpu().numpy()
+    want = np.stack([ref["a" + c] for c in "xyz"], 1)
+    e = np.linalg.norm(got - want, axis=1) / np.linalg.norm(want, axis=1)
+    return float(np.sqrt(np.mean(e ** 2)))
+
+
+@pytest.mark.parametrize("seed", [71, 72, 73])
+def test_mixed_error_within_1p1_of_fp64_at_p12(seed):
+    x, y, z, vx, vy, vz, m = ics.plummer_kroupa(N, seed)
+    st = {k: torch.tensor(a, dtype=torch.float64, device="cuda")
+          for k, a in zip(("x", "y", "z", "vx", "vy", "vz", "m"), (x, y, z, vx, vy, vz, m))}
+    g = {prec: tcb.Gravity(p=12, ncrit=64, theta=0.4, variant=tcb.VARIANT_JERKS, precision=prec)
+         for prec in (tcb.PREC_FP64, tcb.PREC_MIXED)}
+    idx = np.sort(np.random.default_rng(seed).choice(N, TARGETS, replace=False))
+    idx_t = torch.tensor(idx, device="cuda")
+    dt = 1.0 / 1024
+    for state in range(2):
+        out = {}
+        for prec, gg in g.items():
+            out[prec] = gg.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"])
+        ref = g[tcb.PREC_FP64].direct_sums(st["x"], st["y"], st["z"], st["m"], idx, st["vx"], st["vy"], st["vz"])
+        e64, emx = _err(out[tcb.PREC_FP64], ref, idx_t), _err(out[tcb.PREC_MIXED], ref, idx_t)
+        assert emx <= RATIO * e64, (seed, state, emx, e64)
+        if state == 0:
+            # move the state: 8 leapfrog steps with the FP64 accelerations
+            a = out[tcb.PREC_FP64]
+            for _ in range(8):
+                g[tcb.PREC_FP64].kick_drift(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], a["ax"],
+                                            a["ay"], a["az"], 0.5 * dt, dt)
+                a = g[tcb.PREC_FP64].evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"])
+                g[tcb.PREC_FP64].kick_drift(st["x"], st["y"], st["z"], st["vx"], st["vy"], st["vz"], a["ax"],
+                                            a["ay"], a["az"], 0.5 * dt, 0.0)
+    for gg in g.values():
+        gg.close()

@@ -337,3 +337,39 @@ def test_jerks_error_mac_matches_reference():
             assert pair_set(lists[k][0], lists[k][1], gkeys) == pair_set(d[k + "_t"], d[k + "_s"], rkeys), (name, k)
         _check_forces(out, d, True)
         g.close()
+
+
+@pytest.mark.parametrize("variant", [tcb.VARIANT_TOP, tcb.VARIANT_JERKS])
+def test_softened_near_field_and_direct_sums(variant):
+    """Plummer softening (tc_params.softening, no counterpart in the reference): the direct-sum
+    branch and tc_direct_sums equal a numpy FP64 softened direct sum; the FMM's near field is
+    softened and its far field stays Newtonian (O(eps^2 / r^2) at far-field separations), so
+    the FMM stays within its own truncation error of the softened direct sum."""
+    n, eps = 3000, 1e-3
+    x, y, z, vx, vy, vz, m = ics.plummer(n, 17)
+    X = np.stack([x, y, z], 1)
+    d = X[None, :, :] - X[:, None, :]
+    r2 = (d ** 2).sum(-1)
+    s2 = r2 + eps * eps
+    inv = np.where(r2 > 0, 1.0 / np.sqrt(s2), 0.0)
+    pot = (m[None, :] * inv).sum(1)
+    acc = (m[None, :, None] * d * (inv ** 3)[:, :, None]).sum(1)
+    jerk = variant == tcb.VARIANT_JERKS
+    vel = (vx, vy, vz) if jerk else (None, None, None)
+    g = tcb.Gravity(p=10, ncrit=32, theta=0.4, variant=variant, direct_below=1 << 30, softening=eps)
+    out = g.evaluate(x, y, z, m, *vel)
+    assert rel_err(out["pot"], pot).max() < 1e-12
+    assert rel_vec_err(vec(out, "a"), acc).max() < 1e-12
+    ds = g.direct_sums(x, y, z, m, np.arange(0, n, 7), *vel)
+    assert np.abs(ds["pot"] - pot[::7]).max() < 1e-12 * np.abs(pot).max()
+    g.close()
+    for prec in (tcb.PREC_FP64, tcb.PREC_MIXED):
+        g = tcb.Gravity(p=10, ncrit=32, theta=0.4, variant=variant, direct_below=0, precision=prec, softening=eps)
+        out = g.evaluate(x, y, z, m, *vel)
+        e = rel_vec_err(vec(out, "a"), acc)
+        assert np.sqrt(np.mean(e ** 2)) < 2e-5, prec
+        g0 = tcb.Gravity(p=10, ncrit=32, theta=0.4, variant=variant, direct_below=0, precision=prec)
+        out0 = g0.evaluate(x, y, z, m, *vel)
+        assert rel_vec_err(vec(out0, "a"), acc).max() > 1e-6  # softening changed the near field
+        g.close()
+        g0.close()

@@ -21,6 +21,7 @@ from tests._util import rel_vec_err, vec
 
 pytestmark = pytest.mark.gpu
 FP = C.POINTER(C.c_float)
+TOL_SEL = 1e-10  # per-pair truncation error budget, relative to the target cell's least |a|
 
 
 def _direct_err(out, d, idx):
@@ -99,15 +100,63 @@ def test_learned_selector_beats_the_analytic_estimate(trained):
     base = _direct_err(g.evaluate(x, y, z, m, vx, vy, vz), d, idx)
     res = {}
     for sel in (1, 2):
-        g.set_selector(sel, 1e-6)
+        g.set_selector(sel, TOL_SEL)
+        g.evaluate(x, y, z, m, vx, vy, vz)  # leaves |a| behind: the next call's per-target budget
         out = g.evaluate(x, y, z, m, vx, vy, vz)
         st = g.stats()
         res[sel] = (st["m2l_flop_fraction"], _direct_err(out, d, idx))
     # same tolerance: the network chooses cheaper orders than the conservative estimate ...
     assert res[2][0] < res[1][0] - 0.05
-    # ... and the step stays accurate (per-pair tolerance 1e-6 of the monopole force)
-    assert res[2][1] < 20 * base
+    # ... both select lower orders, and the evaluation stays accurate
+    assert res[1][0] < 1.0
+    assert res[2][1] < 1.5 * base and res[1][1] < 1.5 * base
     g.set_selector(0, 1e-9)
+
+
+def test_order_selection_with_no_budget_is_bit_identical_to_fixed_order():
+    """A tolerance too small for any lower order keeps every pair at p: the regrouped lists and
+    the per-batch order path give the same bits as the fixed-order evaluation."""
+    n = 1 << 16
+    x, y, z, vx, vy, vz, m = ics.plummer_kroupa(n, 64)
+    g0 = tcb.Gravity(p=12, ncrit=64, theta=0.4, variant=tcb.VARIANT_JERKS)
+    g1 = tcb.Gravity(p=12, ncrit=64, theta=0.4, variant=tcb.VARIANT_JERKS, selector=1, selector_tol=1e-300)
+    ref = g0.evaluate(x, y, z, m, vx, vy, vz)
+    g1.evaluate(x, y, z, m, vx, vy, vz)
+    out = g1.evaluate(x, y, z, m, vx, vy, vz)
+    st = g1.stats()
+    assert st["class_order"] == [12] and st["class_pairs"][0] == st["n_m2l"]
+    for k in ref:
+        np.testing.assert_array_equal(out[k], ref[k], err_msg=k)
+    g0.close()
+    g1.close()
+
+
+def test_order_selection_in_the_graph_matches_direct_launches():
+    """The selection runs inside the captured graph (no host round trip); replays give the same
+    bits as the same evaluation launched directly."""
+    torch = pytest.importorskip("torch")
+    n = 1 << 16
+    x, y, z, vx, vy, vz, m = ics.plummer_kroupa(n, 65)
+    d = {k: torch.tensor(a, device="cuda") for k, a in zip(("x", "y", "z", "vx", "vy", "vz", "m"),
+                                                           (x, y, z, vx, vy, vz, m))}
+    outs = [{k: torch.empty(n, dtype=torch.float64, device="cuda") for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
+            for _ in range(2)]
+    gg = tcb.Gravity(p=12, ncrit=64, theta=0.4, variant=tcb.VARIANT_JERKS, selector=1, selector_tol=TOL_SEL)
+    gd = tcb.Gravity(p=12, ncrit=64, theta=0.4, variant=tcb.VARIANT_JERKS, selector=1, selector_tol=TOL_SEL)
+    gg.set_graph(True)
+    for step in range(3):
+        for g, o in ((gg, outs[0]), (gd, outs[1])):
+            g.evaluate(d["x"], d["y"], d["z"], d["m"], d["vx"], d["vy"], d["vz"], out=o)
+        torch.cuda.synchronize()
+        if step >= 1:
+            assert gd.stats()["m2l_flop_fraction"] < 1.0
+        if step == 2:
+            assert gg.graph_ready(), gg.graph_note()
+            assert gg.stats()["m2l_flop_fraction"] == gd.stats()["m2l_flop_fraction"]
+        for k in outs[0]:
+            assert torch.equal(outs[0][k], outs[1][k]), (k, step)
+    gg.close()
+    gd.close()
 
 
 def test_judge_reports_and_redoes(trained):
@@ -115,7 +164,8 @@ def test_judge_reports_and_redoes(trained):
     w, norm = g.selector_weights()
     h = tcb.Gravity(p=12, ncrit=64, theta=0.4, variant=tcb.VARIANT_JERKS, judge_n=128, judge_tol=1e-12)
     h.set_selector_weights(w, norm)
-    h.set_selector(2, 1e-4)
+    h.set_selector(2, 1e-6)
+    h.evaluate(x, y, z, m, vx, vy, vz)  # fixed order (no budget yet); leaves |a| behind
     h.evaluate(x, y, z, m, vx, vy, vz)
     st = h.stats()
     assert st["judge_redo"] == 1  # 1e-12 cannot be met: the step was redone at fixed p

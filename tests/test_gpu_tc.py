@@ -60,3 +60,22 @@ def test_tc_far_field_error_at_fp32_floor():
         errs[prec] = np.sqrt(np.mean((np.linalg.norm(g - a, axis=1) / np.linalg.norm(a, axis=1)) ** 2))
     # p = 10 truncation error (~1e-7) dominates the FP32 rounding
     assert errs[tcb.PREC_MIXED_M2L] <= 1.1 * errs[tcb.PREC_FP64]
+
+
+def test_bounded_wait_runs_out_and_the_context_recovers():
+    """The tensor-core far field waits for its products with a bounded wait.  With the limit set
+    to a few clock cycles every wait runs out: the call returns TC_ERR_TIMEOUT (the kernel
+    stops issuing, waits with the default limit for the products in flight and frees its tensor
+    memory), and the same context then evaluates normally again once the limit is restored."""
+    n = 1 << 13
+    x, y, z, vx, vy, vz, m = ics.plummer(n, 77)
+    ref, _, _ = run(tcb.PREC_MIXED_M2L, x, y, z, m, vx, vy, vz, 8)
+    g = tcb.Gravity(p=8, ncrit=64, theta=0.4, variant=tcb.VARIANT_JERKS, precision=tcb.PREC_MIXED_M2L)
+    g.set_wait_limit(4)
+    with pytest.raises(tcb.TaichiError, match="timed out"):
+        g.evaluate(x, y, z, m, vx, vy, vz)
+    g.set_wait_limit(0)
+    out = g.evaluate(x, y, z, m, vx, vy, vz)
+    for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz"):
+        np.testing.assert_array_equal(out[k], ref[k], err_msg=k)
+    g.close()

@@ -134,6 +134,8 @@ struct tc_ctx {
   int amag_n = -1;
   DBuf<int> m2l_src2;
   DBuf<uint8_t> m2l_off;
+  DBuf<int> cls_rng;  // per order class and cell: begin, then end, of the class's source range
+  DBuf<float> cell_feat;  // per cell: the learned selector's per-cell features
   unsigned* d_hist = nullptr;  // 32 counters
   // learned selector
   bool mlp_ready = false;
@@ -205,6 +207,8 @@ struct tc_ctx {
   std::vector<const void*> gsig;  // buffers and capacities baked into the captured graph
   double gstep_dt = 0.0;          // the graph being planned holds a leapfrog step of this dt
   bool gselect = false;           // the captured graph selects per-pair orders
+  int gcls_q[TC_MAX_CLASSES];     // ... with these class orders
+  int gcls_n = 0;
   // error-controlled MAC of the top tree (tc_set_error_mac) and its low-order pre-pass
   bool emac = false;
   double emac_fa = 2.0e-7;
@@ -426,24 +430,34 @@ __global__ void k_p2p_count(const unsigned long long* __restrict__ keys, unsigne
 // per-pair orders with a per-target error budget (tc_order.cuh): the target scale of every cell
 // from the previous evaluation's accelerations, then each target's list regrouped by order
 // ----------------------------------------------------------------------------------------
-// the orders used by an evaluation (h[o]: pairs at order p - o), lowest first
-static void order_stats(tc_ctx* ctx, int p, const unsigned* h) {
+// With an order selector on, accepted pairs of a leaf target whose body counts multiply to at
+// most this many interactions are summed directly (exact) instead of by an M2L: below it the
+// near field's cost (about 3 ps of the whole GPU per FP32 interaction) is under a p = 12 M2L's
+// (about 1.7 ns per pair), scaled by (p + 1)^3.  0 (fixed order, the reference's lists) = off.
+static long long p2p_instead_max(const tc_params& prm) {
+  if (prm.selector <= 0) return 0;
+  const double s = (prm.p + 1.0) / 13.0;
+  return (long long)(256.0 * s * s * s);
+}
+
+// the orders used by an evaluation: h[k] pairs of class k, of order q[k] (ascending)
+static void order_stats(tc_ctx* ctx, int p, const unsigned* h, const int* q, int nclass) {
   ctx->n_classes = 0;
   double tot = 0.0, ff = 0.0;
-  for (int o = p; o >= 0; o--) {
-    if (!h[o]) continue;
-    const int q = p - o;
-    ctx->class_order[ctx->n_classes] = q;
-    ctx->class_pairs[ctx->n_classes] = h[o];
+  for (int k = 0; k < nclass; k++) {
+    if (!h[k]) continue;
+    ctx->class_order[ctx->n_classes] = q[k];
+    ctx->class_pairs[ctx->n_classes] = h[k];
     ctx->n_classes++;
-    tot += h[o];
-    ff += h[o] * std::pow((q + 1.0) / (p + 1.0), 3);
+    tot += h[k];
+    ff += h[k] * std::pow((q[k] + 1.0) / (p + 1.0), 3);
   }
   ctx->flop_frac = tot > 0 ? ff / tot : 1.0;
 }
 
 template <int P>
 static cudaError_t select_orders(tc_ctx* ctx, TcCells cv, int n, int ntl, const unsigned* ntldev, bool capture) {
+  using OC = TcOrderClasses<P>;
   cudaStream_t st = ctx->stream;
   const int nc = capture ? (int)ctx->ccap : ctx->ncell;
   cudaError_t e;
@@ -452,6 +466,7 @@ static cudaError_t select_orders(tc_ctx* ctx, TcCells cv, int n, int ntl, const 
   if ((e = ctx->body_scale.ensure((size_t)n)) != cudaSuccess) return e;
   if ((e = ctx->m2l_src2.ensure(ctx->m2l_src.n)) != cudaSuccess) return e;
   if ((e = ctx->m2l_off.ensure(ctx->m2l_src.n)) != cudaSuccess) return e;
+  if ((e = ctx->cls_rng.ensure((size_t)2 * OC::n * nc)) != cudaSuccess) return e;
   const int* d_ncell = capture ? &((TcLevels*)ctx->d_lv)->ncell : nullptr;
   k_cell_pn<P><<<std::min(nblocks(nc, 128), 148 * 16), 128, 0, st>>>(nc, cv.M, ctx->cell_pn.p, d_ncell);
   k_gather_scale<<<nblocks(n, 256), 256, 0, st>>>(n, ctx->perm.p, ctx->amag.p, ctx->body_scale.p);
@@ -462,16 +477,56 @@ static cudaError_t select_orders(tc_ctx* ctx, TcCells cv, int n, int ntl, const 
   for (int l = maxl; l >= 0; l--)
     k_min_acc<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->body_scale.p, ctx->cell_scale.p);
   if ((e = cudaMemsetAsync(ctx->d_hist, 0, 32 * sizeof(unsigned), st)) != cudaSuccess) return e;
-  TcClassOrders cls;
-  for (int i = 0; i < TC_MAX_CLASSES; i++) cls.q[i] = i < TcOrderClasses<P>::n ? TcOrderClasses<P>::q[i] : P;
+  TcClassOrders co;
+  for (int i = 0; i < TC_MAX_CLASSES; i++) co.q[i] = i < OC::n ? OC::q[i] : P;
+  double fact[2 * TC_PMAX_DEV + 2];
+  fact[0] = 1.0;
+  for (int i = 1; i < 2 * TC_PMAX_DEV + 2; i++) fact[i] = fact[i - 1] * (double)i;
+  for (int k = 0; k <= TC_PMAX_DEV; k++) co.comb[k] = k <= P ? fact[P] * (1.0 / fact[k]) * (1.0 / fact[P - k]) : 0.0;
   const int mode = ctx->prm.selector == 2 ? 2 : 1;
+  if (mode == 2) {
+    if ((e = ctx->cell_feat.ensure((size_t)nc * 5)) != cudaSuccess) return e;
+    k_cell_feat<P><<<std::min(nblocks(nc, 128), 148 * 16), 128, 0, st>>>(nc, cv, ctx->cell_pn.p, ctx->cell_feat.p,
+                                                                         d_ncell);
+  }
   const int grid = capture ? 148 * 8 : std::max(1, std::min(nblocks(ntl, 4), 148 * 8));
   k_select_order<P><<<grid, 128, 0, st>>>(ctx->m2l_tl.p, ntl, ctx->m2l_start.p, ctx->m2l_src.p, ctx->m2l_src2.p,
-                                          ctx->m2l_off.p, cv, ctx->cell_pn.p, ctx->cell_scale.p,
-                                          ctx->prm.selector_tol, mode, ctx->mlp_w.p, ctx->mlp_norm,
-                                          TcOrderClasses<P>::n, cls, ctx->d_hist, ntldev);
+                                          ctx->m2l_off.p, ctx->cls_rng.p, ctx->cls_rng.p + (size_t)OC::n * nc, nc,
+                                          cv, ctx->cell_pn.p, ctx->cell_scale.p, ctx->prm.selector_tol, mode,
+                                          ctx->mlp_w.p, ctx->mlp_norm, OC::n, co, ctx->cell_feat.p, ctx->d_hist,
+                                          ntldev);
   ctx->launches += 4 + maxl;
   return cudaGetLastError();
+}
+
+// one M2L launch per order class over the class ranges that select_orders wrote: persistent
+// grids (one CTA per SM) taking targets from a counter, the target count read on the device
+template <int P, bool JERK, int I = 0>
+static void m2l_class_launches(tc_ctx* ctx, TcCells cv, int ntl, const unsigned* ntldev, int nc) {
+  using OC = TcOrderClasses<P>;
+  if constexpr (I < OC::n) {
+    constexpr int Q = OC::q[I];
+    const size_t smem = (size_t)TcM2LSmem<Q>::TOTAL * sizeof(double);
+    unsigned* next = ctx->d_small + 11;
+    cudaMemsetAsync(next, 0, sizeof(unsigned), ctx->stream);
+    k_m2l<P, Q, JERK><<<ctx->nsm, tc_m2l_threads<Q>(), smem, ctx->stream>>>(
+        ctx->m2l_tl.p, ntl, ctx->cls_rng.p + (size_t)I * nc, ctx->m2l_src2.p, cv, ntldev, next,
+        ctx->cls_rng.p + (size_t)(OC::n + I) * nc);
+    ctx->launches++;
+    m2l_class_launches<P, JERK, I + 1>(ctx, cv, ntl, ntldev, nc);
+  }
+}
+
+template <int P, int I = 0>
+static void set_class_attrs() {
+  using OC = TcOrderClasses<P>;
+  if constexpr (I < OC::n) {
+    constexpr int Q = OC::q[I];
+    const int smem = (int)(TcM2LSmem<Q>::TOTAL * sizeof(double));
+    cudaFuncSetAttribute(k_m2l<P, Q, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_m2l<P, Q, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    set_class_attrs<P, I + 1>();
+  }
 }
 
 // ----------------------------------------------------------------------------------------
@@ -765,6 +820,7 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     return TC_OK;
   };
   TcMac mac;  // theta
+  mac.p2p_max = p2p_instead_max(prm);
   if (ctx->emac) {
     // ---- low-order pre-pass on the geometric cells -> acc_old (integrator.h:476-493;
     // taichi_with_jerks/integrator.h:326-360)
@@ -836,15 +892,21 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     // time-step pass: no far field (the reference skips M2L when get_steps is set)
   } else if (hs[0] > 0) {
     const int* m2l_src = ctx->m2l_src.p;
-    if (prm.selector > 0 && !mixed && ctx->amag_n == n && (prm.selector == 1 || ctx->mlp_ready)) {
+    bool classes = false;
+    if (prm.selector > 0 && !mixed && TcOrderClasses<P>::n > 1 && ctx->amag_n == n &&
+        (prm.selector == 1 || ctx->mlp_ready)) {
       cudaError_t ce = select_orders<P>(ctx, cv, n, (int)hs[0], nullptr, false);
       if (ce != cudaSuccess) return cuda_fail(ctx, ce, "order selection");
-      m2l_src = ctx->m2l_src2.p;
+      m2l_class_launches<P, JERK>(ctx, cv, (int)hs[0], nullptr, ctx->ncell);
       unsigned h[32];
       TC_CK(cudaMemcpyAsync(h, ctx->d_hist, sizeof(h), cudaMemcpyDeviceToHost, st));
       TC_CK(cudaStreamSynchronize(st));
-      order_stats(ctx, P, h);
+      order_stats(ctx, P, h, TcOrderClasses<P>::q, TcOrderClasses<P>::n);
+      classes = true;
     }
+    if (classes) {
+      // done: one launch per order class
+    } else
     if (mixed && P <= TC_TC_QMAX) {
       if constexpr (P <= TC_TC_QMAX) {
         TC_CK(tc_ensure_bins<P>(ctx));
@@ -995,10 +1057,14 @@ static void run_fmm_graph(tc_ctx* ctx, int n) {
   const double theta2 = prm.theta * prm.theta;
   k_trav_init<<<1, 1, 0, st>>>(ctx->front[0].p, ctx->d_cnt);
   const int nsteps = 2 * (TC_MAX_LEVEL + 1) + 2;
-  for (int s = 0; s < nsteps; s++)
-    k_trav_step<<<148 * 8, 256, 0, st>>>(s, ctx->front[s & 1].p, ctx->front[(s + 1) & 1].p, ctx->fcap, ctx->d_cnt, cv,
-                                         theta2, prm.variant == TC_VARIANT_TOP, sbits, ctx->m2l.p, ctx->mcap,
-                                         ctx->p2p.p, ctx->pcap, ctx->d_err);
+  {
+    TcMac mac;  // theta
+    mac.p2p_max = p2p_instead_max(prm);
+    for (int s = 0; s < nsteps; s++)
+      k_trav_step<<<148 * 8, 256, 0, st>>>(s, ctx->front[s & 1].p, ctx->front[(s + 1) & 1].p, ctx->fcap, ctx->d_cnt,
+                                           cv, theta2, prm.variant == TC_VARIANT_TOP, sbits, ctx->m2l.p, ctx->mcap,
+                                           ctx->p2p.p, ctx->pcap, ctx->d_err, mac);
+  }
   L += 1 + nsteps;
   graph_check(ctx, "traversal");
   // ---- sort lists (counts on the device) and per-target offsets
@@ -1027,15 +1093,18 @@ static void run_fmm_graph(tc_ctx* ctx, int n) {
   TcOut o = out_view(ctx, n, JERK);
   cudaMemsetAsync(ctx->outs.p, 0, sizeof(double) * (size_t)n * (JERK ? 7 : 4), st);
   cudaMemsetAsync(ctx->d_small + 10, 0, sizeof(unsigned), st);
-  const int* m2l_src = ctx->m2l_src.p;
+  if (TcOrderClasses<P>::n < 2) ctx->gselect = false;  // one class: nothing to select
   if (ctx->gselect) {  // per-pair orders (the previous replay left |a| in ctx->amag)
+    for (int i = 0; i < TcOrderClasses<P>::n; i++) ctx->gcls_q[i] = TcOrderClasses<P>::q[i];
+    ctx->gcls_n = TcOrderClasses<P>::n;
     select_orders<P>(ctx, cv, n, ccap, ctx->d_small, true);
-    m2l_src = ctx->m2l_src2.p;
-    L += 4 + TC_MAX_LEVEL;
+    m2l_class_launches<P, JERK>(ctx, cv, ccap, ctx->d_small, ccap);
+    L += 4 + TC_MAX_LEVEL + TcOrderClasses<P>::n;
     graph_check(ctx, "order selection");
+  } else {
+    k_m2l<P, P, JERK><<<ctx->nsm, tc_m2l_threads<P>(), (size_t)TcM2LSmem<P>::TOTAL * sizeof(double), st>>>(
+        ctx->m2l_tl.p, ccap, ctx->m2l_start.p, ctx->m2l_src.p, cv, ctx->d_small, ctx->d_small + 10);
   }
-  k_m2l<P, P, JERK><<<ctx->nsm, tc_m2l_threads<P>(), (size_t)TcM2LSmem<P>::TOTAL * sizeof(double), st>>>(
-      ctx->m2l_tl.p, ccap, ctx->m2l_start.p, m2l_src, cv, ctx->d_small, ctx->d_small + 10);
   graph_check(ctx, "M2L");
   graph_event(ctx, 4, st);
   // ---- downward (before the near field: the mixed near field reads the far-field acceleration)
@@ -1113,6 +1182,7 @@ static tc_status judge(tc_ctx* ctx, int n, int nt, bool jerk, double* rms) {
 
 template <int P>
 static void set_m2l_attrs() {
+  set_class_attrs<P>();
   size_t smem = (size_t)TcM2LSmem<P>::TOTAL * sizeof(double);
   cudaFuncSetAttribute(k_m2l<P, P, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   cudaFuncSetAttribute(k_m2l<P, P, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1404,7 +1474,7 @@ tc_status tc_destroy(tc_ctx* ctx) {
   ctx->tsum.release(); ctx->diag.release(); ctx->p2p_part.release();
   ctx->ev_d.release(); ctx->ev_u.release(); ctx->ev_i.release(); ctx->ev_f.release();
   ctx->amag.release(); ctx->body_scale.release(); ctx->cell_scale.release(); ctx->m2l_src2.release();
-  ctx->m2l_off.release(); ctx->kd_scratch.release(); ctx->kd_index.release(); ctx->kd_flags.release();
+  ctx->m2l_off.release(); ctx->cls_rng.release(); ctx->cell_feat.release(); ctx->kd_scratch.release(); ctx->kd_index.release(); ctx->kd_flags.release();
   ctx->low_f.release();
   if (ctx->d_root) cudaFree(ctx->d_root);
   if (ctx->d_lv) cudaFree(ctx->d_lv);
@@ -1691,7 +1761,7 @@ static void graph_signature(const tc_ctx* c, std::vector<const void*>& s) {
                         c->p2p_start.p, c->p2p_src.p,  c->m2l_tl.p,    c->p2p_tl.p,    c->leaves.p,
                         c->judge_idx.p, c->judge_out.p, c->p2p_part.p, c->bpart.p,     c->tc_bins.p,
                         c->amag.p,      c->body_scale.p, c->cell_scale.p, c->m2l_src2.p, c->m2l_off.p,
-                        c->cell_pn.p,   c->mlp_w.p};
+                        c->cell_pn.p,   c->mlp_w.p,      c->cls_rng.p,    c->cell_feat.p};
   s.assign(bufs, bufs + sizeof(bufs) / sizeof(bufs[0]));
   const size_t caps[] = {c->ccap, c->mcap, c->pcap, c->fcap, c->expn.n, c->p2p_part.n};
   for (size_t v : caps) s.push_back((const void*)(uintptr_t)v);
@@ -1840,7 +1910,8 @@ static void graph_plan(tc_ctx* ctx, int n, const TcGraphKey& key, const double* 
     return;
   if (ctx->prm.selector > 0 &&
       (ctx->cell_pn.ensure(ccap * (ctx->prm.p + 1)) || ctx->cell_scale.ensure(ccap) || ctx->body_scale.ensure(N) ||
-       ctx->amag.ensure(N) || ctx->m2l_src2.ensure(ctx->m2l_src.n) || ctx->m2l_off.ensure(ctx->m2l_src.n)))
+       ctx->amag.ensure(N) || ctx->m2l_src2.ensure(ctx->m2l_src.n) || ctx->m2l_off.ensure(ctx->m2l_src.n) ||
+       ctx->cls_rng.ensure((size_t)2 * TC_MAX_CLASSES * ccap) || ctx->cell_feat.ensure(ccap * 5)))
     return;
   // orders are selected in the graph once an evaluation of these bodies left its |a| behind
   ctx->gselect = ctx->prm.selector > 0 && ctx->amag_n == n;
@@ -1957,7 +2028,7 @@ static tc_status evaluate_graph(tc_ctx* ctx, int n, const double* x, const doubl
       ctx->class_order[0] = ctx->prm.p;
       ctx->class_pairs[0] = (long long)ctx->n_m2l;
       ctx->flop_frac = 1.0;
-      if (ctx->gselect) order_stats(ctx, ctx->prm.p, h.hist);
+      if (ctx->gselect) order_stats(ctx, ctx->prm.p, h.hist, ctx->gcls_q, ctx->gcls_n);
       if (ctx->prm.selector > 0) ctx->amag_n = n;  // the replay left its |a| for the next one
       ctx->judge_redo = 0;
       ctx->judge_rms = 0.0;

@@ -396,8 +396,9 @@ __device__ __forceinline__ void tc_bar_group(int grp) {
 template <int Q>
 constexpr int tc_m2l_threads() { return 128 * TcM2LGroups<Q>::G; }
 
-// M2L of order Q <= P over a per-target list; expansions are stored with order P.  Adds
-// into L (zeroed before the first M2L launch of an evaluation).  One CTA per SM (shared
+// M2L of order Q <= P over a per-target list (or, with `tend`, one order class's range of it);
+// expansions are stored with order P.  Adds into L (zeroed before the first M2L launch of an
+// evaluation).  One CTA per SM (shared
 // memory), which owns the tensor memory it allocates.  One target per CTA, or, with `next`
 // (a counter zeroed before the launch), a persistent grid whose CTAs take targets in turn.
 template <int P, int Q, bool JERK>
@@ -405,7 +406,8 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
                                                                const int* __restrict__ tstart,
                                                                const int* __restrict__ src, TcCells c,
                                                                const unsigned* ntldev = nullptr,
-                                                               unsigned* next = nullptr) {
+                                                               unsigned* next = nullptr,
+                                                               const int* __restrict__ tend = nullptr) {
   using SM = TcM2LSmem<Q>;
   using TM = TcM2LTmem<Q>;
   constexpr int NTQ = SM::NT, NTP = (P + 1) * (P + 1);
@@ -440,9 +442,10 @@ __global__ void __launch_bounds__(tc_m2l_threads<Q>(), 1) k_m2l(const int* __res
   double* buf = tc_m2l_smem + SM::BUF + grp * NTQ * 32;
   for (;;) {
   const int t = tlist[ti];
-  const int s_beg = tstart[t], s_end = tstart[t + 1];
+  // the target's sources: [tstart[t], tstart[t + 1]), or one order class's range of them
+  const int s_beg = tstart[t], s_end = tend ? tend[t] : tstart[t + 1];
   const double Xt = c.X[t], Yt = c.Y[t], Zt = c.Z[t];
-  for (int arr = 0; arr < (c.has_sink[t] ? (JERK ? 2 : 1) : 0); arr++) {
+  for (int arr = 0; arr < (c.has_sink[t] && s_end > s_beg ? (JERK ? 2 : 1) : 0); arr++) {
     const double* Mbase = arr ? c.Md : c.M;
     tc_m2l_zero_warp<Q, QUIRK>(w, twarp);
     for (int b0 = s_beg + grp * 32; b0 < s_end; b0 += 32 * G) {

@@ -94,6 +94,68 @@ __device__ __forceinline__ void tc_mlp_forward(const float* __restrict__ w, int 
   }
 }
 
+// Inference of the selector network with compile-time sizes, every loop unrolled so the hidden
+// activations stay in registers; w is the parameter block in shared memory (the same layout as
+// tc_mlp_forward), tanh the hardware approximation.
+template <int NOUT>
+__device__ __forceinline__ void tc_mlp_infer(const float* __restrict__ w, const float* x, float* y) {
+  const float* W1 = w;
+  const float* b1 = W1 + kMlpH * kMlpIn;
+  const float* W2 = b1 + kMlpH;
+  const float* b2 = W2 + kMlpH * kMlpH;
+  const float* W3 = b2 + kMlpH;
+  const float* b3 = W3 + kMlpH * kMlpH;
+  const float* W4 = b3 + kMlpH;
+  const float* b4 = W4 + NOUT * kMlpH;
+  float a[kMlpH], h[kMlpH];
+#pragma unroll
+  for (int j = 0; j < kMlpH; j++) {
+    float s = b1[j];
+#pragma unroll
+    for (int i = 0; i < kMlpIn; i++) s = fmaf(W1[j * kMlpIn + i], x[i], s);
+    a[j] = tc_tanh_fast(s);
+  }
+#pragma unroll
+  for (int j = 0; j < kMlpH; j++) {
+    float s = b2[j];
+#pragma unroll
+    for (int i = 0; i < kMlpH; i++) s = fmaf(W2[j * kMlpH + i], a[i], s);
+    h[j] = tc_tanh_fast(s);
+  }
+#pragma unroll
+  for (int j = 0; j < kMlpH; j++) {
+    float s = b3[j];
+#pragma unroll
+    for (int i = 0; i < kMlpH; i++) s = fmaf(W3[j * kMlpH + i], h[i], s);
+    a[j] = tc_tanh_fast(s);
+  }
+#pragma unroll
+  for (int j = 0; j < NOUT; j++) {
+    float s = b4[j];
+#pragma unroll
+    for (int i = 0; i < kMlpH; i++) s = fmaf(W4[j * kMlpH + i], a[i], s);
+    y[j] = s;
+  }
+}
+
+// The per-cell part of the selector's features (tc_pair_features): the source spectrum ratios
+// (f2..f5) and log of the body count, feat[c * 5 + k]
+template <int P>
+__global__ void k_cell_feat(int ncell, const TcCells c, const double* __restrict__ pn, float* __restrict__ feat,
+                            const int* ncdev = nullptr) {
+  if (ncdev) ncell = *ncdev;  // device-sized launch (graph)
+  for (int ci = blockIdx.x * blockDim.x + threadIdx.x; ci < ncell; ci += gridDim.x * blockDim.x) {
+    const double* ps = pn + (size_t)ci * (P + 1);
+    const double p0 = fmax(ps[0], 1e-300), rs = c.R[ci];
+    for (int j = 0; j < 4; j++) {
+      const int deg = 2 * (j + 1);
+      const double v = deg <= P ? ps[deg] / (p0 * pow(rs, (double)deg)) : 0.0;
+      feat[(size_t)ci * 5 + j] = tc_clampf((float)log(fmax(v, 1e-30)), -69.f, 10.f);
+    }
+    feat[(size_t)ci * 5 + 4] = (float)log((double)c.nbody[ci]);
+  }
+}
+
 // loss = mean over samples and outputs of (y - target)^2; gradients accumulated into g
 __global__ void k_mlp_grad(int ns, int nout, const float* __restrict__ feat, const float* __restrict__ target,
                            const float* __restrict__ w, TcMlpNorm norm, float* __restrict__ g,

@@ -13,10 +13,11 @@
 //     per-degree multipole power (integrator.h:527-539);
 //   learned: the MLP of tc_mlp.cuh, which predicts log10 of each class's error relative to the
 //     source's monopole acceleration M_s / r^2, rescaled to an absolute error.
-// Each target's source list is then stably regrouped by order (one warp per target), and every
-// entry carries its order in the top bits of the source index (kM2LOrderShift), so one M2L launch
-// serves all orders: a batch of 32 pairs runs at the largest order among them.  Nothing here
-// synchronises with the host, so the selection is part of the captured graph.
+// Each target's source list is then stably regrouped by order class (one warp per target) and
+// every class runs as its own M2L launch of that order (k_m2l<P, Q>, each with its balanced
+// per-degree work split) over per-target ranges; the launches are persistent grids that read
+// their counts on the device, so nothing here synchronises with the host and the selection is
+// part of the captured graph.
 #pragma once
 #include "tc_mlp.cuh"
 
@@ -24,9 +25,11 @@ namespace tc {
 
 constexpr int kOrderMin = 3;  // lowest order a pair may get
 
-// the orders the learned selector's outputs stand for (TcOrderClasses)
+// the orders of the classes (TcOrderClasses) and the binomials C(P, k) of the estimate as the
+// reference forms them (kernel_fast_lean.h:139)
 struct TcClassOrders {
   int q[TC_MAX_CLASSES];
+  double comb[TC_PMAX_DEV + 1];
 };
 
 // |a| of each body in caller order (the next evaluation's error budget)
@@ -43,55 +46,76 @@ __global__ void k_gather_scale(int n, const int* __restrict__ perm, const double
   if (i < n) sc[i] = amag[perm[i]];
 }
 
-// absolute truncation-error estimate of an order-q M2L for the pair (the reference's estimate)
-__device__ __forceinline__ double tc_est_abs_err(double r, double rt, double rs, const double* pns, int q) {
-  double sum = 0.0, rk = 1.0, binom = 1.0;
-  for (int k = 0; k <= q; k++) {
-    sum += binom * pns[q - k] * rk;
-    rk *= rt;
-    binom = binom * (q - k) / (k + 1);
-  }
-  return 8.0 * fmax(rt, rs) / (rt + rs) * sum * pow(r, -(double)(q + 2));
-}
-
-// order of one pair (mode 1 analytic, 2 learned)
+// Class (index into TcClassOrders) of one pair: mode 1 analytic, 2 learned.  The analytic
+// selector evaluates the reference's estimate once, at the full order P,
+//   E_P = 8 max(Rt, Rs) / (Rt + Rs) r^-(P+2) sum_k C(P, k) Pn_s[P-k] Rt^k,
+// and scales it to lower orders by the convergence ratio rho = (Rt + Rs) / r of the pair
+// (E_q ~ E_P rho^(q-P), the geometric decay of the estimate's leading term), so the order is
+// q = P - floor(ln(budget / E_P) / ln(1 / rho)), rounded up to the next class.
 template <int P>
-__device__ __forceinline__ int tc_pair_order(const TcCells& c, int t, int s, const double* __restrict__ pn,
+__device__ __forceinline__ int tc_pair_class(const TcCells& c, int t, int s, const double* __restrict__ pn,
                                              double budget, int mode, const float* sw, const TcMlpNorm& norm,
-                                             int nclass, const int* cls_order) {
-  if (!(budget > 0.0)) return P;
+                                             int nclass, const int* cls_order, const double* comb,
+                                             const float* __restrict__ featc) {
+  if (!(budget > 0.0)) return nclass - 1;
   const double dx = c.X[t] - c.X[s], dy = c.Y[t] - c.Y[s], dz = c.Z[t] - c.Z[s];
-  const double r = sqrt(dx * dx + dy * dy + dz * dz);
+  const double r2 = dx * dx + dy * dy + dz * dz, r = sqrt(r2);
   const double* pns = pn + (size_t)s * (P + 1);
   if (mode == 2) {
-    float x[kMlpIn], a1[kMlpH], a2[kMlpH], a3[kMlpH], y[kMlpOutMax];
-    tc_pair_features(c, t, s, pn, P, x);
+    // the features of tc_pair_features: the geometry per pair, the rest per cell (featc)
+    constexpr int NO = TcOrderClasses<P>::n;
+    float x[kMlpIn], y[NO];
+    x[0] = (float)log(c.R[t] / r);
+    x[1] = (float)log(c.R[s] / r);
+#pragma unroll
+    for (int j = 0; j < 5; j++) x[2 + j] = featc[(size_t)s * 5 + j];
+    x[7] = featc[(size_t)t * 5 + 4];
+#pragma unroll
     for (int i = 0; i < kMlpIn; i++) x[i] = (x[i] - norm.mean[i]) * norm.inv_std[i];
-    tc_mlp_forward<true>(sw, nclass, x, a1, a2, a3, y);
+    tc_mlp_infer<NO>(sw, x, y);
     // log10 of the budget relative to the source's monopole acceleration
-    const double mono = fmax(pns[0], 1e-300) / (r * r);
-    const float lim = (float)log10(budget / mono);
-    for (int i = 0; i < nclass - 1; i++)
-      if (y[i] + norm.out_mean <= lim) return cls_order[i];
-    return P;
+    const float lim = (float)log10(budget * r2 / fmax(pns[0], 1e-300));
+#pragma unroll
+    for (int i = 0; i < NO - 1; i++)
+      if (y[i] + norm.out_mean <= lim) return i;
+    return NO - 1;
   }
-  for (int q = kOrderMin; q < P; q++)
-    if (tc_est_abs_err(r, c.R[t], c.R[s], pns, q) <= budget) return q;
-  return P;
+  const double rt = c.R[t], rs = c.R[s];
+  double sum = 0.0, rk = 1.0;
+#pragma unroll
+  for (int k = 0; k <= P; k++) {
+    sum += comb[k] * pns[P - k] * rk;
+    rk *= rt;
+  }
+  double rp = r2;  // r^(P+2)
+#pragma unroll
+  for (int k = 0; k < P; k++) rp *= r;
+  const double ep = 8.0 * fmax(rt, rs) / (rt + rs) * sum / rp;
+  if (!(ep > budget)) {
+    const double rho = (rt + rs) / r;
+    int q = kOrderMin;
+    if (rho > 0.0 && rho < 1.0 && ep > 0.0) q = P - (int)floor(log(budget / ep) / -log(rho));
+    for (int i = 0; i < nclass; i++)
+      if (cls_order[i] >= q) return i;
+  }
+  return nclass - 1;
 }
 
-// One warp per target of the M2L target list: every pair's order (pass 1, kept in `off` as
-// P - q), then the target's entries regrouped by order, stably, into src_out with the order in
-// the top bits (pass 2).  hist[P - q] counts the pairs of each order.
+// One warp per target of the M2L target list: every pair's class (pass 1, kept in `cls`), then
+// the target's entries regrouped by class, lowest order first, stably, into src_out (pass 2):
+// class k of target t occupies [cbeg[k * cstride + t], cend[k * cstride + t]), cstride being the
+// cell capacity of those arrays (the M2L launches index them with the same stride).  hist[k]
+// counts the pairs of class k.
 template <int P>
 __global__ void __launch_bounds__(128) k_select_order(const int* __restrict__ tlist, int ntl,
                                                       const int* __restrict__ tstart, const int* __restrict__ src_in,
-                                                      int* __restrict__ src_out, uint8_t* __restrict__ off,
+                                                      int* __restrict__ src_out, uint8_t* __restrict__ cls,
+                                                      int* __restrict__ cbeg, int* __restrict__ cend, int cstride,
                                                       const TcCells c, const double* __restrict__ pn,
                                                       const double* __restrict__ cell_scale, double tol, int mode,
                                                       const float* __restrict__ w, TcMlpNorm norm, int nclass,
-                                                      TcClassOrders cls, unsigned* __restrict__ hist,
-                                                      const unsigned* ntldev = nullptr) {
+                                                      TcClassOrders co, const float* __restrict__ featc,
+                                                      unsigned* __restrict__ hist, const unsigned* ntldev = nullptr) {
   __shared__ float sw[kMlpParamMax];
   __shared__ unsigned cnt[4][32], base[4][32];
   __shared__ unsigned sh[32];
@@ -111,13 +135,13 @@ __global__ void __launch_bounds__(128) k_select_order(const int* __restrict__ tl
       const int e = q0 + lane;
       if (e < end) {
         const int s = src_in[e] & kM2LSrcMask;
-        const int o = P - tc_pair_order<P>(c, t, s, pn, budget, mode, sw, norm, nclass, cls.q);
-        off[e] = (uint8_t)o;
-        atomicAdd(&cnt[wi][o], 1u);
+        const int ci = tc_pair_class<P>(c, t, s, pn, budget, mode, sw, norm, nclass, co.q, co.comb, featc);
+        cls[e] = (uint8_t)ci;
+        atomicAdd(&cnt[wi][ci], 1u);
       }
     }
     __syncwarp();
-    // exclusive prefix over the orders (lane = P - q), full orders first
+    // exclusive prefix over the classes (lane = class)
     const unsigned v = cnt[wi][lane];
     unsigned incl = v;
     for (int d = 1; d < 32; d <<= 1) {
@@ -125,17 +149,21 @@ __global__ void __launch_bounds__(128) k_select_order(const int* __restrict__ tl
       if (lane >= d) incl += u;
     }
     base[wi][lane] = incl - v;
+    if (lane < nclass) {
+      cbeg[(size_t)lane * cstride + t] = beg + (int)(incl - v);
+      cend[(size_t)lane * cstride + t] = beg + (int)incl;
+    }
     if (v) atomicAdd(&sh[lane], v);
     __syncwarp();
     for (int q0 = beg; q0 < end; q0 += 32) {
       const int e = q0 + lane;
       const bool ok = e < end;
-      const int o = ok ? off[e] : 31;
-      const unsigned peers = __match_any_sync(0xffffffffu, o);
+      const int ci = ok ? cls[e] : 31;
+      const unsigned peers = __match_any_sync(0xffffffffu, ci);
       const unsigned rank = __popc(peers & ((1u << lane) - 1u));
-      if (ok) src_out[beg + base[wi][o] + rank] = (src_in[e] & kM2LSrcMask) | (o << kM2LOrderShift);
+      if (ok) src_out[beg + base[wi][ci] + rank] = src_in[e] & kM2LSrcMask;
       __syncwarp();
-      if (ok && rank == 0) base[wi][o] += __popc(peers);
+      if (ok && rank == 0) base[wi][ci] += __popc(peers);
       __syncwarp();
     }
   }

@@ -627,17 +627,16 @@ __device__ __forceinline__ TcAcc<JERK> tc_mix2_total(const TcMix2<JERK>& T) {
 }
 
 template <bool JERK>
-__global__ void __launch_bounds__(kP2PWarps * 32, 6) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
-                                                              const int* __restrict__ tstart,
-                                                              const int* __restrict__ src, const TcBodies b,
-                                                              const TcCells c, TcOut out, float excl_frac,
-                                                              const unsigned* ntldev = nullptr) {
+__global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
+                                                                 const int* __restrict__ tstart,
+                                                                 const int* __restrict__ src, const TcBodies b,
+                                                                 const TcCells c, TcOut out, float excl_frac,
+                                                                 const unsigned* ntldev = nullptr) {
   if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
   // per warp: the source tile, three 16-byte vectors per source (one broadcast load each):
-  // (xh, yh, xl, yl) (zh, zl, mh, ml) (vx, vy, vz, -); the recorded strong pairs per target
+  // (xh, yh, xl, yl) (zh, zl, mh, ml) (vx, vy, vz, -); each lane's recorded strong pairs
   __shared__ float4 tile[kP2PWarps][32][3];
-  __shared__ int rec[kP2PWarps][32][kP2PRec];
-  __shared__ int nrec[kP2PWarps][32];
+  __shared__ int rec[kP2PWarps][kP2PRec][32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4(*TL)[3] = tile[w];
   for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
@@ -654,10 +653,9 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 6) k_p2p_mixed(const int* __re
       const int grp = lane / gsz, ti = lane % gsz;
       const bool act = grp < ng && ti < r;
       const int i = tb + t0 + ti;
-      nrec[w][lane] = 0;
+      int nrl = 0;  // strong pairs this lane met (its own sources: every ng-th of each tile)
       TcMix2<JERK> A;
       tc_mix2_init<JERK>(A, b, out, i, act, Xc, Yc, Zc, excl_frac);
-      __syncwarp();
       for (int q = sb; q < se; q++) {
         const int s = src[q];
         const int jb = c.begin[s], jn = c.nbody[s];
@@ -680,31 +678,32 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 6) k_p2p_mixed(const int* __re
               bool strong;
               tc_mix2_pair<JERK>(A, s0, s1, s2, strong);
               if (strong) {
-                const int o = atomicAdd(&nrec[w][ti], 1);
-                if (o < kP2PRec) rec[w][ti][o] = jb + j0 + jj;
+                if (nrl < kP2PRec) rec[w][nrl][lane] = jb + j0 + jj;
+                nrl++;
               }
             }
           }
           tc_mix2_fold<JERK>(A);
         }
       }
-      __syncwarp();
       TcAcc<JERK> a = tc_mix2_total<JERK>(A);
-      a.add_groups(gsz, ng, grp);
-      // group 0 finishes its targets: the recorded strong pairs in FP64; a target whose record
-      // list overflowed gets all its strong pairs from a second, warp-wide pass
-      const bool own = act && grp == 0;
-      const int nr = own ? nrec[w][ti] : 0;
-      if (own && nr <= kP2PRec) {
+      // each lane adds its own recorded strong pairs in FP64 (a lane whose list overflowed gets
+      // all of its strong pairs from the warp-wide pass below instead)
+      const bool ovf = act && nrl > kP2PRec;
+      if (act && !ovf && nrl > 0) {
         const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
         const double vxi = JERK ? b.vx[i] : 0.0, vyi = JERK ? b.vy[i] : 0.0, vzi = JERK ? b.vz[i] : 0.0;
-        for (int e = 0; e < nr; e++) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, rec[w][ti][e], a);
+        for (int e = 0; e < nrl; e++) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, rec[w][e][lane], a);
       }
-      unsigned mo = __ballot_sync(0xffffffffu, own && nr > kP2PRec);
+      a.add_groups(gsz, ng, grp);
+      unsigned mo = __ballot_sync(0xffffffffu, ovf);
       while (mo) {
-        const int owner = __ffs(mo) - 1;
+        // lane L overflowed: the whole warp goes over L's sources (group L / gsz: every ng-th of
+        // each tile) and adds the strong ones in FP64 to the target's group-0 lane
+        const int L = __ffs(mo) - 1;
         mo &= mo - 1;
-        const int io = tb + t0 + owner;
+        const int gL = L / gsz, tL = L % gsz;
+        const int io = tb + t0 + tL;
         TcMix2<JERK> T;
         tc_mix2_init<JERK>(T, b, out, io, true, Xc, Yc, Zc, excl_frac);
         const double xi = b.x[io], yi = b.y[io], zi = b.z[io];
@@ -713,22 +712,25 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 6) k_p2p_mixed(const int* __re
         s64.zero();
         for (int q = sb; q < se; q++) {
           const int s = src[q];
-          for (int j = c.begin[s] + lane; j < c.begin[s] + c.nbody[s]; j += 32) {
+          const int jb = c.begin[s], jn = c.nbody[s];
+          for (int u = lane; u < jn; u += 32) {
+            if ((u & 31) % ng != gL) continue;  // the tile position decides the group
             float4 s0, s1;
-            tc_mix2_source(b, j, Xc, Yc, Zc, s0, s1);
+            tc_mix2_source(b, jb + u, Xc, Yc, Zc, s0, s1);
             float2 dxy;
             float dz, ri, f0;
-            if (tc_mix2_geom<JERK>(T, s0, s1, dxy, dz, ri, f0)) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, j, s64);
+            if (tc_mix2_geom<JERK>(T, s0, s1, dxy, dz, ri, f0))
+              tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, jb + u, s64);
           }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s64.add_xor(o);
-        if (lane == owner) {
+        if (lane == tL) {
           a.pot += s64.pot; a.ax += s64.ax; a.ay += s64.ay; a.az += s64.az;
           if (JERK) { a.jx += s64.jx; a.jy += s64.jy; a.jz += s64.jz; }
         }
       }
-      if (own && (b.flags[i] & 1)) {
+      if (act && grp == 0 && (b.flags[i] & 1)) {
         out.pot[i] += a.pot;
         out.ax[i] += a.ax;
         out.ay[i] += a.ay;
@@ -739,7 +741,6 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 6) k_p2p_mixed(const int* __re
           out.jz[i] += a.jz;
         }
       }
-      __syncwarp();
     }
   }
 }

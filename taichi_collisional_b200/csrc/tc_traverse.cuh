@@ -25,6 +25,9 @@ struct TcMac {
   const double* pn = nullptr;       // (p + 1) per cell
   const double* min_acc = nullptr;  // per cell
   double comb[TC_PMAX_DEV + 1];
+  // > 0: an accepted pair whose target is a leaf and whose body counts multiply to at most this
+  // becomes a P2P pair (exact, and cheaper than its M2L); the order selectors' form only
+  long long p2p_max = 0;
 };
 
 // x^-k correctly rounded (k >= 1): x^k in double-double by repeated products, then the
@@ -146,6 +149,7 @@ __global__ void k_trav_step(int s, const int2* __restrict__ fin, int2* __restric
       if (accept) {
         int ni = c.nbody[i], nj = c.nbody[j];
         act = (mac.mode != 1 && top_variant && ((ni <= 2 && nj <= 8) || (nj <= 2 && ni <= 8))) ? 1 : 0;
+        if (mac.p2p_max > 0 && nci == 0 && (long long)ni * nj <= mac.p2p_max) act = 1;
       } else if (nci == 0 && ncj == 0) {
         act = 1;
       } else if (ncj == 0 || (c.R[i] >= c.R[j] && nci != 0)) {

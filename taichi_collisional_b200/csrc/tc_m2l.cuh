@@ -106,9 +106,12 @@ __device__ __forceinline__ void tc_m2l_fwd(const double* __restrict__ Ms, cd ez1
 // translation along z to output degree N, then rotation back; accumulate into the lane's
 // column of the shared accumulator.  Factors (n+k)! / r^(n+k+1) are formed on the fly.
 // Pair batches processed at once by one CTA (each batch by 4 warps); limited by shared memory.
+// Lower orders need less shared memory and tensor memory per group, so they run more groups
+// (warps) per SM to hide the latency of their shorter per-batch work: 6 groups at order <= 8,
+// 5 at order <= 10 (the most the 512 tensor-memory columns allow), 4 up to 12, 2 above.
 template <int P>
 struct TcM2LGroups {
-  static constexpr int G = (P >= 14) ? 2 : 4;
+  static constexpr int G = (P >= 14) ? 2 : (P <= 8 ? 6 : (P <= 10 ? 5 : 4));
 };
 
 // ---------------------------------------------------------------------------------------

@@ -373,3 +373,24 @@ def test_softened_near_field_and_direct_sums(variant):
         assert rel_vec_err(vec(out0, "a"), acc).max() > 1e-6  # softening changed the near field
         g.close()
         g0.close()
+
+
+def test_small_plain_case_against_the_live_reference():
+    """The small plain-method configuration -- 16,384 equal-mass Plummer bodies, the top tree,
+    p = 8, theta = 0.5, ncrit = 64 -- against the reference's own FMM run here (oracle/_ref,
+    compiled from its sources), per particle within 1e-12, and against FP64 direct sums."""
+    if not oracle.ref_available(oracle.VARIANT_TOP, 8):
+        pytest.skip("the reference build (oracle/_ref) is not present")
+    n = 16384
+    x, y, z, vx, vy, vz, m = ics.plummer(n, 2029)
+    ref = oracle.ref_evaluate(x, y, z, m, p=8, theta=0.5, ncrit=64, variant=oracle.VARIANT_TOP,
+                              nthreads=os.cpu_count() or 1)
+    g = tcb.Gravity(p=8, ncrit=64, theta=0.5, variant=tcb.VARIANT_TOP, direct_below=0)
+    out = g.evaluate(x, y, z, m)
+    g.close()
+    assert rel_vec_err(vec(out, "a"), vec(ref, "a")).max() < TOL
+    assert rel_err(out["pot"], ref["pot"]).max() < TOL
+    idx = np.random.default_rng(5).choice(n, 512, replace=False)
+    d = oracle.direct(x, y, z, m, targets=idx)
+    e = rel_vec_err(vec({k: out[k][idx] for k in ("ax", "ay", "az")}, "a"), vec(d, "a"))
+    assert np.sqrt(np.mean(e ** 2)) < 1e-3  # the FMM's own truncation error at p = 8, theta = 0.5

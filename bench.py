@@ -35,12 +35,22 @@ WORKLOAD = {"workload": "plummer_kroupa_N4194304_p12_theta0.4_ncrit64_jerks", "n
             "l2": "inputs larger than L2 (7 x 32 MiB state)", "ics": "plummer_kroupa"}
 
 
+def metric_name():
+    """The headline metric on the headline workload; the workload's own name otherwise."""
+    if WORKLOAD["workload"] == "plummer_kroupa_N4194304_p12_theta0.4_ncrit64_jerks":
+        return METRIC
+    return "particle-steps/s of the leapfrog step (%s), mixed vs FP64 GPU FMM" % WORKLOAD["workload"]
+
+
 def set_workload(args):
     """The workload named by the flags (the defaults are the headline: 4M Plummer/Kroupa, p = 12,
     theta = 0.4, ncrit = 64; --ics fractal --n 2097152 --ncrit 32 is the deep fractal cluster,
     --ics plummer --n 1048576 --p 10 the equal-mass million-body case)."""
-    WORKLOAD.update(n=args.n, p=args.p, theta=args.theta, ncrit=args.ncrit, ics=args.ics)
+    eps = args.softening if args.softening is not None else (1e-4 if args.ics == "fractal" else 0.0)
+    WORKLOAD.update(n=args.n, p=args.p, theta=args.theta, ncrit=args.ncrit, ics=args.ics, softening=eps)
     WORKLOAD["workload"] = "%s_N%d_p%d_theta%g_ncrit%d_jerks" % (args.ics, args.n, args.p, args.theta, args.ncrit)
+    if eps > 0:
+        WORKLOAD["workload"] += "_eps%g" % eps
     WORKLOAD["l2"] = ("inputs larger than L2 (7 x %.0f MiB state)" % (8 * args.n / 2 ** 20) if 56 * args.n > 126e6
                       else "inputs fit in L2")
 CPU_SAMPLE_N = 131072
@@ -65,6 +75,9 @@ def parse():
                     help="energy drift over one time unit of leapfrog steps, FP64 and mixed forms "
                          "(defaults there: 16,777,216 Plummer/Kroupa bodies, p = 16, theta = 0.5)")
     ap.add_argument("--dt", type=float, default=0.0, help="--energy-drift: the step (default 1/64)")
+    ap.add_argument("--softening", type=float, default=None,
+                    help="Plummer softening of the pair interactions (default 1e-4 for the fractal cluster, whose "
+                         "unsoftened close pairs blow up under a shared step, else 0)")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_m2l"])
     ap.add_argument("--judge", type=int, default=256, help="bodies checked against FP64 direct sums each step")
     ap.add_argument("--selector", type=int, default=0, choices=[0, 1, 2],
@@ -272,7 +285,7 @@ def run_reference(args, rank):
               "p=%d, theta=%g, ncrit=%d, %s" % (k, n, p, WORKLOAD["theta"], WORKLOAD["ncrit"],
                                                 "the reference's OpenMP + vectorclass build" if kind == "reference"
                                                 else "the oracle port"))
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+    line = {"metric": metric_name(), "value": value, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": k, "warmup": warm, "ms_per_step": 1e3 * sec / k,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Plummer sphere, Kroupa IMF masses)",
@@ -569,7 +582,7 @@ def main():
     out = {k: torch.empty(n, dtype=torch.float64, device=dev) for k in ("ax", "ay", "az", "pot", "jx", "jy", "jz")}
     prec = {"fp64": tcb.PREC_FP64, "mixed": tcb.PREC_MIXED, "mixed_m2l": tcb.PREC_MIXED_M2L}[args.precision]
     g = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
-                    precision=prec, device=local, judge_n=args.judge)
+                    precision=prec, device=local, judge_n=args.judge, softening=WORKLOAD["softening"])
     train = None
     if args.selector == 2:  # the learned selector, trained on the GPU on pairs of this workload (untimed)
         rep = g.train_selector(x, y, z, m, vx, vy, vz, nsamples=16384, iters=1500, seed=5)
@@ -622,7 +635,8 @@ def main():
     fp64 = None
     if not args.no_fp64_arm and args.precision != "fp64":
         g64 = tcb.Gravity(p=p, ncrit=WORKLOAD["ncrit"], theta=WORKLOAD["theta"], variant=tcb.VARIANT_JERKS,
-                          precision=tcb.PREC_FP64, device=local, judge_n=args.judge)
+                          precision=tcb.PREC_FP64, device=local, judge_n=args.judge,
+                          softening=WORKLOAD["softening"])
         g64.set_graph(not args.no_graph)
         st64 = {k: v.clone() for k, v in st.items()}
         out64 = {k: torch.empty_like(v) for k, v in out.items()}
@@ -728,6 +742,12 @@ def main():
             "phase_ms": {k: round(v, 3) for k, v in per.items()},
             "other": {k: {"ms": round(v[0], 3), "tflops": round(v[1] / (v[0] * 1e-3) / 1e12, 3) if v[0] else None}
                       for k, v in kern.items()}}
+    if args.precision != "fp64" and per["ms_p2p"] > 0:
+        # the mixed near field computes in FP32: its fraction of the measured FP32 FMA throughput
+        fp32_peak = g.probe_peak(1) / 1e3
+        ach32 = p2p_flops / (per["ms_p2p"] * 1e-3) / 1e12
+        roof["other"]["k_p2p"].update(bound="fp32", peak=round(fp32_peak, 3),
+                                      frac=round(ach32 / fp32_peak, 4) if fp32_peak > 0 else None)
 
     cb = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -742,7 +762,7 @@ def main():
         except Exception as e:
             cb = {"value": None, "error": str(e)}
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        line = {"metric": metric_name(), "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
                 "data": "synthetic (seeded Plummer sphere, Kroupa IMF masses)",

@@ -438,19 +438,36 @@ __global__ void k_scatter_out(int n, const int* __restrict__ perm, TcOut s, doub
 namespace tc {
 
 // ---------------------------------------------------------------------------------------
-// Mixed-precision near field: FP32 interactions, compensated sums, the strongest pair in FP64.
-// Positions and masses enter as FP32 (hi, lo) pairs formed in FP64 (positions relative to
-// the target cell centre), so dx = (xj_hi - xi_hi) + (xj_lo - xi_lo) carries only its final
-// FP32 rounding even for close pairs; 1/r is the hardware estimate refined by one Newton
-// step; each 32-source tile is summed in FP32 and folded into (hi, lo) accumulators with a
-// two-sum; the final per-target sum is formed in FP64.
+// k_p2p_mixed: the mixed-precision near field.
 //
-// The FP32 error of a target's near field is dominated by its strongest interaction (a close
-// neighbour or a massive star): each lane tracks the source with the largest m / r^2 and, after
-// the loop, replaces that pair's FP32 contribution by its FP64 value.  The pair arithmetic uses
-// explicitly rounded intrinsics (no contraction), so the contribution recomputed for removal is
-// bit-identical to the one that was summed.
+// One warp per target leaf, one target per lane; a last pass of r <= 16 targets runs
+// floor(32 / r) lane groups, each over every ng-th source pair of each tile (so small leaves
+// still fill the warp).
+//
+// Arithmetic.  Sources are staged per 32-source tile as FP32 (hi, lo) pairs of positions
+// relative to the target cell's centre and of masses, formed in FP64, so dx = (xj_hi - xi_hi)
+// + (xj_lo - xi_lo) carries one rounding even for close pairs.  Each lane evaluates two
+// sources at once with the packed FP32x2 instructions of sm_100 (FADD2/FMUL2/FFMA2: one issue
+// for two pairs); the tile stores the two sources' fields side by side so one 16-byte
+// broadcast load feeds both halves.  1/r is the hardware estimate refined by one Newton
+// step; each tile's FP32 sums are folded into (hi, lo) accumulators by a two-sum; the final
+// sums are FP64.
+//
+// Accuracy.  The FP32 pair terms carry a few units of 2^-24 each, and so does their per-tile
+// FP32 sum -- relative to the largest term in the sum.  A term far larger than the target's
+// acceleration would leave an error far larger than the FMM's own.  So every pair whose
+// strength m / r^2 exceeds tau = excl_frac |a_far| (the target's far-field acceleration,
+// which the downward pass has already written into out) is left out of the FP32 sums and
+// recorded; after the loop the recorded pairs are added in FP64.  A lane with more than kP2PRec
+// strong pairs (a zero far field makes every pair strong) goes over its sources a second time,
+// in the same tiles and lane groups, and adds every strong pair in FP64 (the same FP32 test
+// decides).
 // ---------------------------------------------------------------------------------------
+constexpr int kP2PRec = 16;
+// strong-pair threshold: pairs with m / r^2 above this fraction of the far-field acceleration
+// are summed in FP64
+constexpr float kP2PExclFrac = 1e-2f;
+
 struct TcF2 {
   float hi, lo;
   __device__ __forceinline__ void add(float t) {  // two-sum
@@ -463,44 +480,6 @@ struct TcF2 {
   __device__ __forceinline__ double val() const { return (double)hi + (double)lo; }
 };
 
-// one FP32 pair: f0 = m / r (potential), f = m / r^3 (acceleration factor), g the jerk's
-// radial factor; the accumulated terms are f0, d f and dv f + d g
-struct TcPair32 {
-  float dx, dy, dz, ri, f0, f, dvx, dvy, dvz, g;
-};
-
-template <bool JERK>
-__device__ __forceinline__ TcPair32 tc_pair32(float sxh, float syh, float szh, float sxl, float syl, float szl,
-                                              float mh, float ml, float svx, float svy, float svz, float xh,
-                                              float yh, float zh, float xl, float yl, float zl, float vxi,
-                                              float vyi, float vzi) {
-  TcPair32 v;
-  v.dx = __fadd_rn(__fsub_rn(sxh, xh), __fsub_rn(sxl, xl));
-  v.dy = __fadd_rn(__fsub_rn(syh, yh), __fsub_rn(syl, yl));
-  v.dz = __fadd_rn(__fsub_rn(szh, zh), __fsub_rn(szl, zl));
-  float r2 = __fmaf_rn(v.dx, v.dx, __fmaf_rn(v.dy, v.dy, __fmul_rn(v.dz, v.dz)));
-  v.ri = 0.f;
-  if (r2 > 0.f) {
-    // one Newton step on the hardware estimate: y' = y + y (1 - r2 y^2) / 2
-    float y = rsqrtf(r2);
-    float e = __fmaf_rn(-__fmul_rn(r2, y), y, 1.f);
-    v.ri = __fmaf_rn(__fmul_rn(0.5f, y), e, y);
-  }
-  v.f0 = __fmaf_rn(ml, v.ri, __fmul_rn(mh, v.ri));
-  float ri2 = __fmul_rn(v.ri, v.ri);
-  v.f = __fmul_rn(v.f0, ri2);
-  if (JERK) {
-    v.dvx = __fsub_rn(svx, vxi);
-    v.dvy = __fsub_rn(svy, vyi);
-    v.dvz = __fsub_rn(svz, vzi);
-    float vr = __fmul_rn(3.f, __fmaf_rn(v.dx, v.dvx, __fmaf_rn(v.dy, v.dvy, __fmul_rn(v.dz, v.dvz))));
-    v.g = __fmul_rn(__fmul_rn(-v.f, ri2), vr);
-  } else {
-    v.dvx = v.dvy = v.dvz = v.g = 0.f;
-  }
-  return v;
-}
-
 // FP32 (hi, lo) split of x - c
 __device__ __forceinline__ void tc_split(double x, double c, float& h, float& l) {
   double d = x - c;
@@ -508,118 +487,150 @@ __device__ __forceinline__ void tc_split(double x, double c, float& h, float& l)
   l = (float)(d - (double)h);
 }
 
-// ---------------------------------------------------------------------------------------
-// k_p2p_mixed: the mixed-precision near field.
-//
-// One warp per target leaf, one target per lane; a last pass of r <= 16 targets runs
-// floor(32 / r) lane groups, each over every ng-th source of each 32-source tile (so small
-// leaves still fill the warp).
-//
-// Accuracy.  The FP32 pair terms carry a few units of 2^-24 each, and so does their per-tile
-// FP32 sum -- relative to the largest term in the sum.  A term far larger than the target's
-// acceleration would leave an error far larger than the FMM's own.  So every pair whose
-// strength m / r^2 exceeds tau = excl_frac |a_far| (the target's far-field acceleration,
-// which the downward pass has already written into out) is left out of the FP32 sums and
-// recorded; after the loop the recorded pairs are added in FP64.  For a target with more than
-// kP2PRec strong pairs (a zero far field makes every pair strong) the whole warp runs a second
-// pass over its sources that adds every strong pair in FP64 (the same FP32 test decides).
-// Sources are staged per tile as FP32 (hi, lo) pairs of positions relative to the target
-// cell's centre and of masses, so dx = (xj_hi - xi_hi) + (xj_lo - xi_lo) has one rounding even
-// for close pairs; 1/r is the hardware estimate refined by one Newton step; each tile's FP32
-// sums are folded into (hi, lo) accumulators by a two-sum; the final sums are FP64.
-// ---------------------------------------------------------------------------------------
-constexpr int kP2PRec = 16;
-// strong-pair threshold: pairs with m / r^2 above this fraction of the far-field acceleration
-// are summed in FP64
-constexpr float kP2PExclFrac = 1e-2f;
+__device__ __forceinline__ float2 tc_f2(float a) { return make_float2(a, a); }
 
-template <bool JERK>
-struct TcMix2 {  // one target's FP32 state
-  float xh, yh, zh, xl, yl, zl, vx, vy, vz, tau, eps2;
-  float sp, sx, sy, sz, qx, qy, qz;  // this tile's sums
-  TcF2 pot, ax, ay, az, jx, jy, jz;  // compensated totals
+// the hardware 1/sqrt estimate (inputs here are never subnormal: r2 + eps2 of a pair that is
+// kept, or 0 for a pair that is dropped)
+__device__ __forceinline__ float tc_rsqrt_est(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// A tile: 32 sources as 16 pairs (2p, 2p + 1); field group g of pair p is one float4 holding
+// both sources' values of two fields: g0 (xh, yh), g1 (zh, xl), g2 (yl, zl), g3 (mh, ml),
+// g4 (vx, vy), g5 (vz, -), each as (source 2p, source 2p + 1).
+constexpr int kP2PGroups = 6;
+struct TcTile {
+  float4 g[kP2PGroups][16];
 };
 
-// the FP32 geometry of one pair: difference, 1/r, m/r, and whether m/r^2 exceeds the target's
-// threshold.  The only definition of "strong": the main loop and the overflow pass both call it.
+// one target's FP32 state; the target's fields are negated and duplicated into both halves
 template <bool JERK>
-__device__ __forceinline__ bool tc_mix2_geom(const TcMix2<JERK>& T, const float4 s0, const float4 s1, float2& dxy,
-                                             float& dz, float& ri, float& f0) {
-  dxy = __fadd2_rn(__fadd2_rn(make_float2(s0.x, s0.y), make_float2(-T.xh, -T.yh)),
-                   __fadd2_rn(make_float2(s0.z, s0.w), make_float2(-T.xl, -T.yl)));
-  dz = __fadd_rn(__fsub_rn(s1.x, T.zh), __fsub_rn(s1.y, T.zl));
-  const float r2 = __fmaf_rn(dxy.x, dxy.x, __fmaf_rn(dxy.y, dxy.y, __fmul_rn(dz, dz)));
-  ri = 0.f;
-  if (r2 > 0.f) {
-    const float rs = __fadd_rn(r2, T.eps2);  // softened (eps2 = 0: unchanged)
-    const float y = rsqrtf(rs);
-    const float e = __fmaf_rn(-__fmul_rn(rs, y), y, 1.f);
-    ri = __fmaf_rn(__fmul_rn(0.5f, y), e, y);
+struct TcMixP {
+  float2 nxh, nyh, nzh, nxl, nyl, nzl, nvx, nvy, nvz, eps2;
+  float tau;
+  float2 sp, sx, sy, sz, qx, qy, qz;  // this tile's sums, one per half
+  TcF2 pot, ax, ay, az, jx, jy, jz;   // compensated totals
+};
+
+// stage source j (or a zero-mass source at the cell centre when j < 0) at tile slot l
+template <bool JERK>
+__device__ __forceinline__ void tc_tile_put(TcTile& T, int l, const TcBodies& b, int j, double Xc, double Yc,
+                                            double Zc) {
+  float xh = 0.f, yh = 0.f, zh = 0.f, xl = 0.f, yl = 0.f, zl = 0.f, mh = 0.f, ml = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+  if (j >= 0) {
+    tc_split(b.x[j], Xc, xh, xl);
+    tc_split(b.y[j], Yc, yh, yl);
+    tc_split(b.z[j], Zc, zh, zl);
+    tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, mh, ml);
+    if (JERK) { vx = (float)b.vx[j]; vy = (float)b.vy[j]; vz = (float)b.vz[j]; }
   }
-  f0 = __fmaf_rn(s1.w, ri, __fmul_rn(s1.z, ri));
-  return __fmul_rn(f0, ri) > T.tau;  // m / r^2 above the target's threshold: FP64 instead
-}
-
-// a source body as the tile stages it: (xh, yh, xl, yl) (zh, zl, mh, ml) relative to the target
-// cell's centre
-__device__ __forceinline__ void tc_mix2_source(const TcBodies& b, int j, double Xc, double Yc, double Zc, float4& s0,
-                                               float4& s1) {
-  tc_split(b.x[j], Xc, s0.x, s0.z);
-  tc_split(b.y[j], Yc, s0.y, s0.w);
-  tc_split(b.z[j], Zc, s1.x, s1.y);
-  tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, s1.z, s1.w);
-}
-
-template <bool JERK>
-__device__ __forceinline__ void tc_mix2_pair(TcMix2<JERK>& T, const float4 s0, const float4 s1, const float4 s2,
-                                             bool& strong) {
-  float2 dxy;
-  float dz, ri, f0;
-  strong = tc_mix2_geom<JERK>(T, s0, s1, dxy, dz, ri, f0);
-  if (strong) f0 = 0.f;
-  const float ri2 = __fmul_rn(ri, ri);
-  const float f = __fmul_rn(f0, ri2);
-  T.sp = __fadd_rn(T.sp, f0);
-  T.sx = __fmaf_rn(dxy.x, f, T.sx);
-  T.sy = __fmaf_rn(dxy.y, f, T.sy);
-  T.sz = __fmaf_rn(dz, f, T.sz);
+  const int p = l >> 1, h = l & 1;
+  float* g0 = reinterpret_cast<float*>(&T.g[0][p]);
+  float* g1 = reinterpret_cast<float*>(&T.g[1][p]);
+  float* g2 = reinterpret_cast<float*>(&T.g[2][p]);
+  float* g3 = reinterpret_cast<float*>(&T.g[3][p]);
+  g0[h] = xh; g0[2 + h] = yh;
+  g1[h] = zh; g1[2 + h] = xl;
+  g2[h] = yl; g2[2 + h] = zl;
+  g3[h] = mh; g3[2 + h] = ml;
   if (JERK) {
-    const float dvx = __fsub_rn(s2.x, T.vx), dvy = __fsub_rn(s2.y, T.vy), dvz = __fsub_rn(s2.z, T.vz);
-    const float vr = __fmul_rn(3.f, __fmaf_rn(dxy.x, dvx, __fmaf_rn(dxy.y, dvy, __fmul_rn(dz, dvz))));
-    const float g = __fmul_rn(__fmul_rn(-f, ri2), vr);
-    T.qx = __fmaf_rn(dxy.x, g, __fmaf_rn(dvx, f, T.qx));
-    T.qy = __fmaf_rn(dxy.y, g, __fmaf_rn(dvy, f, T.qy));
-    T.qz = __fmaf_rn(dz, g, __fmaf_rn(dvz, f, T.qz));
+    float* g4 = reinterpret_cast<float*>(&T.g[4][p]);
+    float* g5 = reinterpret_cast<float*>(&T.g[5][p]);
+    g4[h] = vx; g4[2 + h] = vy;
+    g5[h] = vz;
+  }
+}
+
+// The FP32 geometry of source pair p: differences, 1/r, m/r, and whether each half's m/r^2
+// exceeds the target's threshold.  The only definition of "strong": the main loop and the
+// overflow pass both call it.
+template <bool JERK>
+__device__ __forceinline__ void tc_mixp_geom(const TcMixP<JERK>& T, const TcTile& S, int p, float2& dx, float2& dy,
+                                             float2& dz, float2& ri, float2& f0, bool& sa, bool& sb) {
+  const float4 g0 = S.g[0][p], g1 = S.g[1][p], g2 = S.g[2][p], g3 = S.g[3][p];
+  dx = __fadd2_rn(__fadd2_rn(make_float2(g0.x, g0.y), T.nxh), __fadd2_rn(make_float2(g1.z, g1.w), T.nxl));
+  dy = __fadd2_rn(__fadd2_rn(make_float2(g0.z, g0.w), T.nyh), __fadd2_rn(make_float2(g2.x, g2.y), T.nyl));
+  dz = __fadd2_rn(__fadd2_rn(make_float2(g1.x, g1.y), T.nzh), __fadd2_rn(make_float2(g2.z, g2.w), T.nzl));
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+  const float2 rs = __fadd2_rn(r2, T.eps2);  // softened (eps2 = 0: unchanged)
+  const float2 y = make_float2(tc_rsqrt_est(rs.x), tc_rsqrt_est(rs.y));
+  // one Newton step: ri = y + (y / 2) (1 - rs y^2), written as y - (y / 2) (rs y^2 - 1)
+  const float2 e = __ffma2_rn(__fmul2_rn(rs, y), y, tc_f2(-1.f));
+  ri = __ffma2_rn(__fmul2_rn(y, tc_f2(-0.5f)), e, y);
+  ri.x = r2.x > 0.f ? ri.x : 0.f;  // coincident bodies (and the target itself) add nothing
+  ri.y = r2.y > 0.f ? ri.y : 0.f;
+  f0 = __ffma2_rn(make_float2(g3.z, g3.w), ri, __fmul2_rn(make_float2(g3.x, g3.y), ri));
+  const float2 st = __fmul2_rn(f0, ri);
+  sa = st.x > T.tau;
+  sb = st.y > T.tau;
+}
+
+template <bool JERK>
+__device__ __forceinline__ void tc_mixp_pair(TcMixP<JERK>& T, const TcTile& S, int p, bool& sa, bool& sb) {
+  float2 dx, dy, dz, ri, f0;
+  tc_mixp_geom<JERK>(T, S, p, dx, dy, dz, ri, f0, sa, sb);
+  if (sa) f0.x = 0.f;  // strong: summed in FP64 instead
+  if (sb) f0.y = 0.f;
+  const float2 ri2 = __fmul2_rn(ri, ri);
+  const float2 f = __fmul2_rn(f0, ri2);
+  T.sp = __fadd2_rn(T.sp, f0);
+  T.sx = __ffma2_rn(dx, f, T.sx);
+  T.sy = __ffma2_rn(dy, f, T.sy);
+  T.sz = __ffma2_rn(dz, f, T.sz);
+  if (JERK) {
+    const float4 g4 = S.g[4][p];
+    const float2 g5 = *reinterpret_cast<const float2*>(&S.g[5][p]);
+    const float2 dvx = __fadd2_rn(make_float2(g4.x, g4.y), T.nvx);
+    const float2 dvy = __fadd2_rn(make_float2(g4.z, g4.w), T.nvy);
+    const float2 dvz = __fadd2_rn(g5, T.nvz);
+    // g = -f / r^2 * 3 (d . dv)
+    const float2 vrn = __fmul2_rn(tc_f2(-3.f), __ffma2_rn(dx, dvx, __ffma2_rn(dy, dvy, __fmul2_rn(dz, dvz))));
+    const float2 g = __fmul2_rn(__fmul2_rn(f, ri2), vrn);
+    T.qx = __ffma2_rn(dx, g, __ffma2_rn(dvx, f, T.qx));
+    T.qy = __ffma2_rn(dy, g, __ffma2_rn(dvy, f, T.qy));
+    T.qz = __ffma2_rn(dz, g, __ffma2_rn(dvz, f, T.qz));
   }
 }
 
 template <bool JERK>
-__device__ __forceinline__ void tc_mix2_fold(TcMix2<JERK>& T) {
-  T.pot.add(T.sp); T.ax.add(T.sx); T.ay.add(T.sy); T.az.add(T.sz);
-  if (JERK) { T.jx.add(T.qx); T.jy.add(T.qy); T.jz.add(T.qz); }
-  T.sp = T.sx = T.sy = T.sz = T.qx = T.qy = T.qz = 0.f;
+__device__ __forceinline__ void tc_mixp_fold(TcMixP<JERK>& T) {
+  T.pot.add(__fadd_rn(T.sp.x, T.sp.y));
+  T.ax.add(__fadd_rn(T.sx.x, T.sx.y));
+  T.ay.add(__fadd_rn(T.sy.x, T.sy.y));
+  T.az.add(__fadd_rn(T.sz.x, T.sz.y));
+  if (JERK) {
+    T.jx.add(__fadd_rn(T.qx.x, T.qx.y));
+    T.jy.add(__fadd_rn(T.qy.x, T.qy.y));
+    T.jz.add(__fadd_rn(T.qz.x, T.qz.y));
+  }
+  T.sp = T.sx = T.sy = T.sz = T.qx = T.qy = T.qz = tc_f2(0.f);
 }
 
 template <bool JERK>
-__device__ __forceinline__ void tc_mix2_init(TcMix2<JERK>& T, const TcBodies& b, const TcOut& out, int i, bool v,
+__device__ __forceinline__ void tc_mixp_init(TcMixP<JERK>& T, const TcBodies& b, const TcOut& out, int i, bool v,
                                              double Xc, double Yc, double Zc, float excl_frac) {
-  T.xh = T.yh = T.zh = T.xl = T.yl = T.zl = T.vx = T.vy = T.vz = 0.f;
+  float xh = 0.f, yh = 0.f, zh = 0.f, xl = 0.f, yl = 0.f, zl = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
   T.tau = 0.f;
-  T.eps2 = (float)b.eps2;
   if (v) {
-    tc_split(b.x[i], Xc, T.xh, T.xl);
-    tc_split(b.y[i], Yc, T.yh, T.yl);
-    tc_split(b.z[i], Zc, T.zh, T.zl);
-    if (JERK) { T.vx = (float)b.vx[i]; T.vy = (float)b.vy[i]; T.vz = (float)b.vz[i]; }
+    tc_split(b.x[i], Xc, xh, xl);
+    tc_split(b.y[i], Yc, yh, yl);
+    tc_split(b.z[i], Zc, zh, zl);
+    if (JERK) { vx = (float)b.vx[i]; vy = (float)b.vy[i]; vz = (float)b.vz[i]; }
     const double a = sqrt(out.ax[i] * out.ax[i] + out.ay[i] * out.ay[i] + out.az[i] * out.az[i]);
     T.tau = (float)(excl_frac * a);
   }
-  T.sp = T.sx = T.sy = T.sz = T.qx = T.qy = T.qz = 0.f;
+  T.nxh = tc_f2(-xh); T.nyh = tc_f2(-yh); T.nzh = tc_f2(-zh);
+  T.nxl = tc_f2(-xl); T.nyl = tc_f2(-yl); T.nzl = tc_f2(-zl);
+  T.nvx = tc_f2(-vx); T.nvy = tc_f2(-vy); T.nvz = tc_f2(-vz);
+  T.eps2 = tc_f2((float)b.eps2);
+  T.sp = T.sx = T.sy = T.sz = T.qx = T.qy = T.qz = tc_f2(0.f);
   T.pot = T.ax = T.ay = T.az = T.jx = T.jy = T.jz = TcF2{0.f, 0.f};
 }
 
 template <bool JERK>
-__device__ __forceinline__ TcAcc<JERK> tc_mix2_total(const TcMix2<JERK>& T) {
+__device__ __forceinline__ TcAcc<JERK> tc_mixp_total(const TcMixP<JERK>& T) {
   TcAcc<JERK> a;
   a.pot = T.pot.val(); a.ax = T.ax.val(); a.ay = T.ay.val(); a.az = T.az.val();
   a.jx = T.jx.val(); a.jy = T.jy.val(); a.jz = T.jz.val();
@@ -633,12 +644,11 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __re
                                                                  const TcCells c, TcOut out, float excl_frac,
                                                                  const unsigned* ntldev = nullptr) {
   if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
-  // per warp: the source tile, three 16-byte vectors per source (one broadcast load each):
-  // (xh, yh, xl, yl) (zh, zl, mh, ml) (vx, vy, vz, -); each lane's recorded strong pairs
-  __shared__ float4 tile[kP2PWarps][32][3];
+  // per warp: the source tile and each lane's recorded strong pairs
+  __shared__ TcTile tile[kP2PWarps];
   __shared__ int rec[kP2PWarps][kP2PRec][32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4(*TL)[3] = tile[w];
+  TcTile& TL = tile[w];
   for (int k = blockIdx.x * kP2PWarps + w; k < ntl; k += gridDim.x * kP2PWarps) {
     const int t = tlist[k];
     if (!c.has_sink[t]) continue;
@@ -647,89 +657,77 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __re
     const int sb = tstart[t], se = tstart[t + 1];
     for (int t0 = 0; t0 < nt; t0 += 32) {
       // up to 32 targets per pass; a last pass of r <= 16 targets runs floor(32 / r) lane
-      // groups of r lanes, each over every ng-th source
+      // groups of r lanes, each over every ng-th source pair
       const int r = min(32, nt - t0);
       const int gsz = r > 16 ? 32 : r, ng = 32 / gsz;
       const int grp = lane / gsz, ti = lane % gsz;
       const bool act = grp < ng && ti < r;
       const int i = tb + t0 + ti;
-      int nrl = 0;  // strong pairs this lane met (its own sources: every ng-th of each tile)
-      TcMix2<JERK> A;
-      tc_mix2_init<JERK>(A, b, out, i, act, Xc, Yc, Zc, excl_frac);
+      int nrl = 0;  // strong pairs this lane met
+      TcMixP<JERK> A;
+      tc_mixp_init<JERK>(A, b, out, i, act, Xc, Yc, Zc, excl_frac);
       for (int q = sb; q < se; q++) {
         const int s = src[q];
         const int jb = c.begin[s], jn = c.nbody[s];
         for (int j0 = 0; j0 < jn; j0 += 32) {
-          const int cnt = min(32, jn - j0);
+          const int cnt = min(32, jn - j0), np = (cnt + 1) >> 1;
           __syncwarp();
-          if (lane < cnt) {
-            const int j = jb + j0 + lane;
-            float4 s0, s1;
-            tc_mix2_source(b, j, Xc, Yc, Zc, s0, s1);
-            TL[lane][0] = s0;
-            TL[lane][1] = s1;
-            if (JERK) TL[lane][2] = make_float4((float)b.vx[j], (float)b.vy[j], (float)b.vz[j], 0.f);
-          }
+          if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, lane < cnt ? jb + j0 + lane : -1, Xc, Yc, Zc);
           __syncwarp();
           if (act) {
-            for (int jj = grp; jj < cnt; jj += ng) {
-              const float4 s0 = TL[jj][0], s1 = TL[jj][1];
-              const float4 s2 = JERK ? TL[jj][2] : make_float4(0.f, 0.f, 0.f, 0.f);
-              bool strong;
-              tc_mix2_pair<JERK>(A, s0, s1, s2, strong);
-              if (strong) {
-                if (nrl < kP2PRec) rec[w][nrl][lane] = jb + j0 + jj;
-                nrl++;
+            for (int p = grp; p < np; p += ng) {
+              bool sa, sbb;
+              tc_mixp_pair<JERK>(A, TL, p, sa, sbb);
+              if (sa | sbb) {
+                if (sa) {
+                  if (nrl < kP2PRec) rec[w][nrl][lane] = jb + j0 + 2 * p;
+                  nrl++;
+                }
+                if (sbb) {
+                  if (nrl < kP2PRec) rec[w][nrl][lane] = jb + j0 + 2 * p + 1;
+                  nrl++;
+                }
               }
             }
           }
-          tc_mix2_fold<JERK>(A);
+          tc_mixp_fold<JERK>(A);
         }
       }
-      TcAcc<JERK> a = tc_mix2_total<JERK>(A);
-      // each lane adds its own recorded strong pairs in FP64 (a lane whose list overflowed gets
-      // all of its strong pairs from the warp-wide pass below instead)
+      TcAcc<JERK> a = tc_mixp_total<JERK>(A);
       const bool ovf = act && nrl > kP2PRec;
+      if (__any_sync(0xffffffffu, ovf)) {
+        // a lane whose list overflowed goes over its own sources again (the same tiles, the same
+        // lane groups) and adds every strong pair in FP64; the other lanes only stage the tiles
+        const double xi = ovf ? b.x[i] : 0.0, yi = ovf ? b.y[i] : 0.0, zi = ovf ? b.z[i] : 0.0;
+        const double vxi = (JERK && ovf) ? b.vx[i] : 0.0, vyi = (JERK && ovf) ? b.vy[i] : 0.0,
+                     vzi = (JERK && ovf) ? b.vz[i] : 0.0;
+        for (int q = sb; q < se; q++) {
+          const int s = src[q];
+          const int jb = c.begin[s], jn = c.nbody[s];
+          for (int j0 = 0; j0 < jn; j0 += 32) {
+            const int cnt = min(32, jn - j0), np = (cnt + 1) >> 1;
+            __syncwarp();
+            if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, lane < cnt ? jb + j0 + lane : -1, Xc, Yc, Zc);
+            __syncwarp();
+            if (ovf) {
+              for (int p = grp; p < np; p += ng) {
+                float2 dx, dy, dz, ri, f0;
+                bool sa, sbb;
+                tc_mixp_geom<JERK>(A, TL, p, dx, dy, dz, ri, f0, sa, sbb);
+                if (sa) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, jb + j0 + 2 * p, a);
+                if (sbb) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, jb + j0 + 2 * p + 1, a);
+              }
+            }
+          }
+        }
+      }
+      // each lane adds its own recorded strong pairs in FP64
       if (act && !ovf && nrl > 0) {
         const double xi = b.x[i], yi = b.y[i], zi = b.z[i];
         const double vxi = JERK ? b.vx[i] : 0.0, vyi = JERK ? b.vy[i] : 0.0, vzi = JERK ? b.vz[i] : 0.0;
         for (int e = 0; e < nrl; e++) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, rec[w][e][lane], a);
       }
       a.add_groups(gsz, ng, grp);
-      unsigned mo = __ballot_sync(0xffffffffu, ovf);
-      while (mo) {
-        // lane L overflowed: the whole warp goes over L's sources (group L / gsz: every ng-th of
-        // each tile) and adds the strong ones in FP64 to the target's group-0 lane
-        const int L = __ffs(mo) - 1;
-        mo &= mo - 1;
-        const int gL = L / gsz, tL = L % gsz;
-        const int io = tb + t0 + tL;
-        TcMix2<JERK> T;
-        tc_mix2_init<JERK>(T, b, out, io, true, Xc, Yc, Zc, excl_frac);
-        const double xi = b.x[io], yi = b.y[io], zi = b.z[io];
-        const double vxi = JERK ? b.vx[io] : 0.0, vyi = JERK ? b.vy[io] : 0.0, vzi = JERK ? b.vz[io] : 0.0;
-        TcAcc<JERK> s64;
-        s64.zero();
-        for (int q = sb; q < se; q++) {
-          const int s = src[q];
-          const int jb = c.begin[s], jn = c.nbody[s];
-          for (int u = lane; u < jn; u += 32) {
-            if ((u & 31) % ng != gL) continue;  // the tile position decides the group
-            float4 s0, s1;
-            tc_mix2_source(b, jb + u, Xc, Yc, Zc, s0, s1);
-            float2 dxy;
-            float dz, ri, f0;
-            if (tc_mix2_geom<JERK>(T, s0, s1, dxy, dz, ri, f0))
-              tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, jb + u, s64);
-          }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) s64.add_xor(o);
-        if (lane == tL) {
-          a.pot += s64.pot; a.ax += s64.ax; a.ay += s64.ay; a.az += s64.az;
-          if (JERK) { a.jx += s64.jx; a.jy += s64.jy; a.jz += s64.jz; }
-        }
-      }
       if (act && grp == 0 && (b.flags[i] & 1)) {
         out.pot[i] += a.pot;
         out.ax[i] += a.ax;

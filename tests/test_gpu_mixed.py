@@ -53,3 +53,43 @@ def test_mixed_error_within_1p1_of_fp64_at_p12(seed):
                                             a["ay"], a["az"], 0.5 * dt, 0.0)
     for gg in g.values():
         gg.close()
+
+
+@pytest.mark.parametrize("n", [12, 60, 200])
+@pytest.mark.parametrize("variant", [tcb.VARIANT_TOP, tcb.VARIANT_JERKS])
+def test_every_pair_strong_without_a_far_field(n, variant):
+    """One leaf and no far field: every pair is strong, so the mixed form sums every pair in FP64
+    -- through the per-lane lists (n = 12) or the second pass of lanes whose list overflowed
+    (n = 60, 200: two passes of targets) -- and matches the FP64 form to rounding."""
+    rng = np.random.default_rng(n)
+    x, y, z, vx, vy, vz = (rng.normal(size=n) for _ in range(6))
+    m = rng.uniform(0.5, 1.5, size=n) / n
+    out = {}
+    for prec in (tcb.PREC_FP64, tcb.PREC_MIXED):
+        g = tcb.Gravity(p=12, ncrit=256, theta=0.4, variant=variant, precision=prec, direct_below=0)
+        out[prec] = g.evaluate(x, y, z, m, vx, vy, vz)
+        g.close()
+    keys = ("pot", "ax", "ay", "az") + (("jx", "jy", "jz") if variant == tcb.VARIANT_JERKS else ())
+    for k in keys:
+        a, b = out[tcb.PREC_MIXED][k], out[tcb.PREC_FP64][k]
+        assert np.max(np.abs(a - b)) <= 1e-13 * np.max(np.abs(b)), k
+
+
+def test_mixed_error_on_the_fractal_cluster():
+    """The deep fractal cluster (ncrit = 32), where close neighbours dominate most bodies'
+    accelerations and many near-field pairs are strong: the same 1.1 bar."""
+    n = 1 << 18
+    x, y, z, vx, vy, vz, m = ics.fractal(n, 2026)
+    st = {k: torch.tensor(a, dtype=torch.float64, device="cuda")
+          for k, a in zip(("x", "y", "z", "vx", "vy", "vz", "m"), (x, y, z, vx, vy, vz, m))}
+    idx = np.sort(np.random.default_rng(3).choice(n, 2048, replace=False))
+    idx_t = torch.tensor(idx, device="cuda")
+    out, ref = {}, None
+    for prec in (tcb.PREC_FP64, tcb.PREC_MIXED):
+        g = tcb.Gravity(p=12, ncrit=32, theta=0.4, variant=tcb.VARIANT_JERKS, precision=prec)
+        out[prec] = g.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"])
+        if ref is None:
+            ref = g.direct_sums(st["x"], st["y"], st["z"], st["m"], idx, st["vx"], st["vy"], st["vz"])
+        g.close()
+    e64, emx = _err(out[tcb.PREC_FP64], ref, idx_t), _err(out[tcb.PREC_MIXED], ref, idx_t)
+    assert emx <= RATIO * e64, (emx, e64)

@@ -80,10 +80,12 @@ def parse():
                          "unsoftened close pairs blow up under a shared step, else 0)")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_m2l"])
     ap.add_argument("--judge", type=int, default=256, help="bodies checked against FP64 direct sums each step")
-    ap.add_argument("--selector", type=int, default=0, choices=[0, 1, 2],
-                    help="per-pair far-field order: 0 fixed p, 1 analytic estimate, 2 learned (trained on the GPU "
-                         "on pairs of this workload before the timed region)")
-    ap.add_argument("--selector-tol", type=float, default=1e-10,
+    ap.add_argument("--selector", type=int, default=2, choices=[0, 1, 2],
+                    help="per-pair far-field order: 0 fixed p, 1 analytic estimate, 2 learned (the default: trained "
+                         "on the GPU on pairs of this workload before the timed region)")
+    ap.add_argument("--train-ics", default=None, choices=["plummer_kroupa", "plummer", "fractal"],
+                    help="--selector 2: train on these initial conditions (same n) instead of the workload's own")
+    ap.add_argument("--selector-tol", type=float, default=3e-9,
                     help="per-pair truncation error budget relative to the target cell's least |a|")
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip timing the plain FP64 form alongside")
     ap.add_argument("--accuracy-targets", type=int, default=4096,
@@ -507,6 +509,12 @@ def run_energy_drift(args):
         out = {k: torch.zeros(n, dtype=torch.float64, device="cuda") for k in ("ax", "ay", "az", "pot", "jx", "jy",
                                                                                  "jz")}
         g = tcb.Gravity(p=p, ncrit=ncrit, theta=theta, variant=tcb.VARIANT_JERKS, precision=prec)
+        if name == "mixed" and args.selector:
+            if args.selector == 2:
+                rep = g.train_selector(x, y, z, m, vx, vy, vz, nsamples=16384, iters=1500, seed=5)
+                line["training"] = {k: rep[k] for k in ("samples", "val_loss", "seconds", "class_order")}
+            g.set_selector(args.selector, args.selector_tol)
+            line["selector"] = {"kind": ["fixed p", "analytic", "learned"][args.selector], "tol": args.selector_tol}
         g.set_graph(True)
         g.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"], out=out)
 
@@ -524,7 +532,8 @@ def run_energy_drift(args):
         ms = e_start.elapsed_time(e_end)
         e1 = energy()
         line[name] = {"E0": e0, "E1": e1, "rel_energy_drift": abs(e1 - e0) / abs(e0), "ms_per_step": ms / nstep,
-                      "particle_steps_per_s": n * nstep / (ms * 1e-3), "m2l_pairs": g.stats()["n_m2l"]}
+                      "particle_steps_per_s": n * nstep / (ms * 1e-3), "m2l_pairs": g.stats()["n_m2l"],
+                      "m2l_flop_fraction": g.stats()["m2l_flop_fraction"]}
         g.close()
         del st, out
         torch.cuda.empty_cache()
@@ -585,8 +594,10 @@ def main():
                     precision=prec, device=local, judge_n=args.judge, softening=WORKLOAD["softening"])
     train = None
     if args.selector == 2:  # the learned selector, trained on the GPU on pairs of this workload (untimed)
-        rep = g.train_selector(x, y, z, m, vx, vy, vz, nsamples=16384, iters=1500, seed=5)
+        tr = (x, y, z, vx, vy, vz, m) if not args.train_ics else make_ics(n, 2026 + rank, args.train_ics)
+        rep = g.train_selector(tr[0], tr[1], tr[2], tr[6], tr[3], tr[4], tr[5], nsamples=16384, iters=1500, seed=5)
         train = {k: rep[k] for k in ("samples", "iters", "train_loss", "val_loss", "seconds", "class_order")}
+        train["ics"] = args.train_ics or WORKLOAD["ics"]
     if args.selector:
         g.set_selector(args.selector, args.selector_tol)
     g.set_graph(not args.no_graph)  # the first evaluation captures, the later ones replay

@@ -442,7 +442,8 @@ namespace tc {
 //
 // One warp per target leaf, one target per lane; a last pass of r <= 16 targets runs
 // floor(32 / r) lane groups, each over every ng-th source pair of each tile (so small leaves
-// still fill the warp).
+// still fill the warp).  A tile takes the next 32 bodies of the target's source cells read as
+// one sequence, so small source leaves still fill it.
 //
 // Arithmetic.  Sources are staged per 32-source tile as FP32 (hi, lo) pairs of positions
 // relative to the target cell's centre and of masses, formed in FP64, so dx = (xj_hi - xi_hi)
@@ -637,6 +638,29 @@ __device__ __forceinline__ TcAcc<JERK> tc_mixp_total(const TcMixP<JERK>& T) {
   return a;
 }
 
+// The next tile of a target's sources, taken as one sequence of bodies (its source cells'
+// bodies one after the other), so a tile holds 32 sources even where the source leaves are
+// small.  (q, off) is the warp-uniform cursor: the next source cell and the next body in it.
+// Returns the tile's count; lane l gets the body index of slot l (-1 past the count).
+__device__ __forceinline__ int tc_next_tile(const int* __restrict__ src, const TcCells& c, int se, int& q, int& off,
+                                            int lane, int& myj) {
+  int fill = 0;
+  myj = -1;
+  while (fill < 32 && q < se) {
+    const int s = src[q];
+    const int jb = c.begin[s], jn = c.nbody[s];
+    const int take = min(32 - fill, jn - off);
+    if (lane >= fill && lane < fill + take) myj = jb + off + lane - fill;
+    fill += take;
+    off += take;
+    if (off >= jn) {
+      q++;
+      off = 0;
+    }
+  }
+  return fill;
+}
+
 template <bool JERK>
 __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
                                                                  const int* __restrict__ tstart,
@@ -646,6 +670,7 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __re
   if (ntldev) ntl = (int)*ntldev;  // device-sized launch (graph)
   // per warp: the source tile and each lane's recorded strong pairs
   __shared__ TcTile tile[kP2PWarps];
+  __shared__ int tj[kP2PWarps][32];  // body index of each tile slot
   __shared__ int rec[kP2PWarps][kP2PRec][32];
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   TcTile& TL = tile[w];
@@ -666,32 +691,30 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __re
       int nrl = 0;  // strong pairs this lane met
       TcMixP<JERK> A;
       tc_mixp_init<JERK>(A, b, out, i, act, Xc, Yc, Zc, excl_frac);
-      for (int q = sb; q < se; q++) {
-        const int s = src[q];
-        const int jb = c.begin[s], jn = c.nbody[s];
-        for (int j0 = 0; j0 < jn; j0 += 32) {
-          const int cnt = min(32, jn - j0), np = (cnt + 1) >> 1;
-          __syncwarp();
-          if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, lane < cnt ? jb + j0 + lane : -1, Xc, Yc, Zc);
-          __syncwarp();
-          if (act) {
-            for (int p = grp; p < np; p += ng) {
-              bool sa, sbb;
-              tc_mixp_pair<JERK>(A, TL, p, sa, sbb);
-              if (sa | sbb) {
-                if (sa) {
-                  if (nrl < kP2PRec) rec[w][nrl][lane] = jb + j0 + 2 * p;
-                  nrl++;
-                }
-                if (sbb) {
-                  if (nrl < kP2PRec) rec[w][nrl][lane] = jb + j0 + 2 * p + 1;
-                  nrl++;
-                }
+      for (int q = sb, off = 0; q < se;) {
+        int myj;
+        const int cnt = tc_next_tile(src, c, se, q, off, lane, myj), np = (cnt + 1) >> 1;
+        __syncwarp();
+        if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, myj, Xc, Yc, Zc);
+        tj[w][lane] = myj;
+        __syncwarp();
+        if (act) {
+          for (int p = grp; p < np; p += ng) {
+            bool sa, sbb;
+            tc_mixp_pair<JERK>(A, TL, p, sa, sbb);
+            if (sa | sbb) {
+              if (sa) {
+                if (nrl < kP2PRec) rec[w][nrl][lane] = tj[w][2 * p];
+                nrl++;
+              }
+              if (sbb) {
+                if (nrl < kP2PRec) rec[w][nrl][lane] = tj[w][2 * p + 1];
+                nrl++;
               }
             }
           }
-          tc_mixp_fold<JERK>(A);
         }
+        tc_mixp_fold<JERK>(A);
       }
       TcAcc<JERK> a = tc_mixp_total<JERK>(A);
       const bool ovf = act && nrl > kP2PRec;
@@ -701,22 +724,20 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __re
         const double xi = ovf ? b.x[i] : 0.0, yi = ovf ? b.y[i] : 0.0, zi = ovf ? b.z[i] : 0.0;
         const double vxi = (JERK && ovf) ? b.vx[i] : 0.0, vyi = (JERK && ovf) ? b.vy[i] : 0.0,
                      vzi = (JERK && ovf) ? b.vz[i] : 0.0;
-        for (int q = sb; q < se; q++) {
-          const int s = src[q];
-          const int jb = c.begin[s], jn = c.nbody[s];
-          for (int j0 = 0; j0 < jn; j0 += 32) {
-            const int cnt = min(32, jn - j0), np = (cnt + 1) >> 1;
-            __syncwarp();
-            if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, lane < cnt ? jb + j0 + lane : -1, Xc, Yc, Zc);
-            __syncwarp();
-            if (ovf) {
-              for (int p = grp; p < np; p += ng) {
-                float2 dx, dy, dz, ri, f0;
-                bool sa, sbb;
-                tc_mixp_geom<JERK>(A, TL, p, dx, dy, dz, ri, f0, sa, sbb);
-                if (sa) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, jb + j0 + 2 * p, a);
-                if (sbb) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, jb + j0 + 2 * p + 1, a);
-              }
+        for (int q = sb, off = 0; q < se;) {
+          int myj;
+          const int cnt = tc_next_tile(src, c, se, q, off, lane, myj), np = (cnt + 1) >> 1;
+          __syncwarp();
+          if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, myj, Xc, Yc, Zc);
+          tj[w][lane] = myj;
+          __syncwarp();
+          if (ovf) {
+            for (int p = grp; p < np; p += ng) {
+              float2 dx, dy, dz, ri, f0;
+              bool sa, sbb;
+              tc_mixp_geom<JERK>(A, TL, p, dx, dy, dz, ri, f0, sa, sbb);
+              if (sa) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, tj[w][2 * p], a);
+              if (sbb) tc_p2p_one<JERK>(xi, yi, zi, vxi, vyi, vzi, b, tj[w][2 * p + 1], a);
             }
           }
         }

@@ -46,8 +46,11 @@ def set_workload(args):
     """The workload named by the flags (the defaults are the headline: 4M Plummer/Kroupa, p = 12,
     theta = 0.4, ncrit = 64; --ics fractal --n 2097152 --ncrit 32 is the deep fractal cluster,
     --ics plummer --n 1048576 --p 10 the equal-mass million-body case)."""
-    eps = args.softening if args.softening is not None else (1e-4 if args.ics == "fractal" else 0.0)
-    WORKLOAD.update(n=args.n, p=args.p, theta=args.theta, ncrit=args.ncrit, ics=args.ics, softening=eps)
+    eps = args.softening
+    # the step of the timed leapfrog: the cold fractal cluster's unsoftened close pairs need a far
+    # shorter one than the Plummer sphere's (1/4096 blows it up within a few steps)
+    dt = args.dt if args.dt > 0 else (1e-6 if args.ics == "fractal" else 1.0 / 4096)
+    WORKLOAD.update(n=args.n, p=args.p, theta=args.theta, ncrit=args.ncrit, ics=args.ics, softening=eps, dt=dt)
     WORKLOAD["workload"] = "%s_N%d_p%d_theta%g_ncrit%d_jerks" % (args.ics, args.n, args.p, args.theta, args.ncrit)
     if eps > 0:
         WORKLOAD["workload"] += "_eps%g" % eps
@@ -74,10 +77,11 @@ def parse():
     ap.add_argument("--energy-drift", action="store_true",
                     help="energy drift over one time unit of leapfrog steps, FP64 and mixed forms "
                          "(defaults there: 16,777,216 Plummer/Kroupa bodies, p = 16, theta = 0.5)")
-    ap.add_argument("--dt", type=float, default=0.0, help="--energy-drift: the step (default 1/64)")
-    ap.add_argument("--softening", type=float, default=None,
-                    help="Plummer softening of the pair interactions (default 1e-4 for the fractal cluster, whose "
-                         "unsoftened close pairs blow up under a shared step, else 0)")
+    ap.add_argument("--dt", type=float, default=0.0,
+                    help="the leapfrog step (default 1/4096; 1e-6 on the fractal cluster; --energy-drift: 1/64)")
+    ap.add_argument("--softening", type=float, default=0.0,
+                    help="Plummer softening of the pair interactions (the far field stays unsoftened, so it "
+                         "should be well below the smallest M2L separation)")
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed_m2l"])
     ap.add_argument("--judge", type=int, default=256, help="bodies checked against FP64 direct sums each step")
     ap.add_argument("--selector", type=int, default=2, choices=[0, 1, 2],
@@ -85,7 +89,7 @@ def parse():
                          "on the GPU on pairs of this workload before the timed region)")
     ap.add_argument("--train-ics", default=None, choices=["plummer_kroupa", "plummer", "fractal"],
                     help="--selector 2: train on these initial conditions (same n) instead of the workload's own")
-    ap.add_argument("--selector-tol", type=float, default=3e-9,
+    ap.add_argument("--selector-tol", type=float, default=2e-9,
                     help="per-pair truncation error budget relative to the target cell's least |a|")
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip timing the plain FP64 form alongside")
     ap.add_argument("--accuracy-targets", type=int, default=4096,
@@ -245,7 +249,7 @@ def run_reference(args, rank):
         n, p = args.n, args.p
         x, y, z, vx, vy, vz, m = make_ics(n, 2026)
         run, kind, cores = cpu_runner(x, y, z, vx, vy, vz, m, p, WORKLOAD["theta"], WORKLOAD["ncrit"])
-        dt = 1.0 / 4096
+        dt = WORKLOAD["dt"]
         acc = {"ax": np.zeros(n), "ay": np.zeros(n), "az": np.zeros(n)}
 
         def step():
@@ -601,7 +605,7 @@ def main():
     if args.selector:
         g.set_selector(args.selector, args.selector_tol)
     g.set_graph(not args.no_graph)  # the first evaluation captures, the later ones replay
-    dt = 1.0 / 4096
+    dt = WORKLOAD["dt"]
 
     def evaluate():
         g.evaluate(st["x"], st["y"], st["z"], st["m"], st["vx"], st["vy"], st["vz"], out=out)

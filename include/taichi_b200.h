@@ -196,7 +196,8 @@ tc_status tc_set_selector_weights(tc_ctx* ctx, const float* w, const float* norm
  * for checking the hand-written backward pass. */
 tc_status tc_mlp_loss_grad(int ns, int n_out, const float* feat, const float* labels, const float* w,
                            const float* norm, float* grad, float* loss);
-/* Predicted log10 errors [ns x n_out] of the network for given features (host arrays). */
+/* Predicted log10 errors [ns x n_out] of the network for given features (host arrays), by the
+ * same tensor-core (TF32 operands, FP32 accumulation) inference the order selection runs. */
 tc_status tc_mlp_predict(int ns, int n_out, const float* feat, const float* w, const float* norm, float* pred);
 
 /* FP64 leapfrog update on device arrays (the integrator step around each evaluation):

@@ -478,7 +478,14 @@ static cudaError_t select_orders(tc_ctx* ctx, TcCells cv, int n, int ntl, const 
     k_min_acc<<<gc, 128, 0, st>>>(l, cv, d_start, d_count, ctx->body_scale.p, ctx->cell_scale.p);
   if ((e = cudaMemsetAsync(ctx->d_hist, 0, 32 * sizeof(unsigned), st)) != cudaSuccess) return e;
   TcClassOrders co;
-  for (int i = 0; i < TC_MAX_CLASSES; i++) co.q[i] = i < OC::n ? OC::q[i] : P;
+  for (int i = 0; i < TC_MAX_CLASSES; i++) {
+    co.q[i] = i < OC::n ? OC::q[i] : P;
+    co.below[i] = 0;
+  }
+  for (int l = 0; l < TcClassLaunches<P>::n; l++) {
+    const int f = TcClassLaunches<P>::first(l), e2 = TcClassLaunches<P>::first(l + 1);
+    for (int i = f; i < e2; i++) co.below[i] = OC::q[e2 - 1] - OC::q[i];
+  }
   double fact[2 * TC_PMAX_DEV + 2];
   fact[0] = 1.0;
   for (int i = 1; i < 2 * TC_PMAX_DEV + 2; i++) fact[i] = fact[i - 1] * (double)i;
@@ -504,14 +511,16 @@ static cudaError_t select_orders(tc_ctx* ctx, TcCells cv, int n, int ntl, const 
 template <int P, bool JERK, int I = 0>
 static void m2l_class_launches(tc_ctx* ctx, TcCells cv, int ntl, const unsigned* ntldev, int nc) {
   using OC = TcOrderClasses<P>;
-  if constexpr (I < OC::n) {
-    constexpr int Q = OC::q[I];
+  using CL = TcClassLaunches<P>;
+  if constexpr (I < CL::n) {
+    constexpr int F = CL::first(I), E = CL::first(I + 1);  // classes [F, E), at the order of E - 1
+    constexpr int Q = OC::q[E - 1];
     const size_t smem = (size_t)TcM2LSmem<Q>::TOTAL * sizeof(double);
     unsigned* next = ctx->d_small + 11;
     cudaMemsetAsync(next, 0, sizeof(unsigned), ctx->stream);
     k_m2l<P, Q, JERK><<<ctx->nsm, tc_m2l_threads<Q>(), smem, ctx->stream>>>(
-        ctx->m2l_tl.p, ntl, ctx->cls_rng.p + (size_t)I * nc, ctx->m2l_src2.p, cv, ntldev, next,
-        ctx->cls_rng.p + (size_t)(OC::n + I) * nc);
+        ctx->m2l_tl.p, ntl, ctx->cls_rng.p + (size_t)F * nc, ctx->m2l_src2.p, cv, ntldev, next,
+        ctx->cls_rng.p + (size_t)(OC::n + E - 1) * nc);
     ctx->launches++;
     m2l_class_launches<P, JERK, I + 1>(ctx, cv, ntl, ntldev, nc);
   }
@@ -1099,7 +1108,7 @@ static void run_fmm_graph(tc_ctx* ctx, int n) {
     ctx->gcls_n = TcOrderClasses<P>::n;
     select_orders<P>(ctx, cv, n, ccap, ctx->d_small, true);
     m2l_class_launches<P, JERK>(ctx, cv, ccap, ctx->d_small, ccap);
-    L += 4 + TC_MAX_LEVEL + TcOrderClasses<P>::n;
+    L += 4 + TC_MAX_LEVEL + TcClassLaunches<P>::n;
     graph_check(ctx, "order selection");
   } else {
     k_m2l<P, P, JERK><<<ctx->nsm, tc_m2l_threads<P>(), (size_t)TcM2LSmem<P>::TOTAL * sizeof(double), st>>>(
@@ -2444,14 +2453,21 @@ tc_status tc_mlp_loss_grad(int ns, int n_out, const float* feat, const float* la
   return TC_OK;
 }
 
-__global__ void k_mlp_predict(int ns, int nout, const float* __restrict__ feat, const float* __restrict__ w,
-                              TcMlpNorm norm, float* __restrict__ pred) {
-  int k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= ns) return;
-  float x[kMlpIn], a1[kMlpH], a2[kMlpH], a3[kMlpH], y[kMlpOutMax];
-  for (int i = 0; i < kMlpIn; i++) x[i] = (feat[(size_t)k * kMlpIn + i] - norm.mean[i]) * norm.inv_std[i];
-  tc_mlp_forward(w, nout, x, a1, a2, a3, y);
-  for (int j = 0; j < nout; j++) pred[(size_t)k * nout + j] = y[j] + norm.out_mean;
+// the selector's own inference (tensor cores, a warp per 32 samples), as k_select_order runs it
+__global__ void __launch_bounds__(128) k_mlp_predict(int ns, int nout, const float* __restrict__ feat,
+                                                     const float* __restrict__ w, TcMlpNorm norm,
+                                                     float* __restrict__ pred) {
+  __shared__ TcMlpTc T;
+  __shared__ float act[4][32 * kMlpActS];
+  tc_mlp_tc_load(T, w, nout, threadIdx.x, blockDim.x);
+  __syncthreads();
+  const int k = blockIdx.x * blockDim.x + threadIdx.x, wi = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float x[kMlpIn], y[kMlpOutMax];
+  for (int i = 0; i < kMlpIn; i++)
+    x[i] = k < ns ? (feat[(size_t)k * kMlpIn + i] - norm.mean[i]) * norm.inv_std[i] : 0.f;
+  tc_mlp_infer_tc<kMlpOutMax>(T, act[wi], x, y, lane);
+  if (k < ns)
+    for (int j = 0; j < nout; j++) pred[(size_t)k * nout + j] = y[j] + norm.out_mean;
 }
 
 tc_status tc_mlp_predict(int ns, int n_out, const float* feat, const float* w, const float* norm, float* pred) {

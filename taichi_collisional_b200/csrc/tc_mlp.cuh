@@ -94,11 +94,27 @@ __device__ __forceinline__ void tc_mlp_forward(const float* __restrict__ w, int 
   }
 }
 
-// Inference of the selector network with compile-time sizes, every loop unrolled so the hidden
-// activations stay in registers; w is the parameter block in shared memory (the same layout as
-// tc_mlp_forward), tanh the hardware approximation.
-template <int NOUT>
-__device__ __forceinline__ void tc_mlp_infer(const float* __restrict__ w, const float* x, float* y) {
+// The same network on the tensor cores, for the 32 pairs of a warp at once: each layer is a
+// [32 pairs x K] x [K x 32] product in mma.sync m16n8k8 TF32 tiles with FP32 accumulation; the
+// activations pass between layers through the warp's shared buffer.  TF32 keeps 10 bits of the
+// operands, so the outputs (log10 errors) differ from the FP32 forward by about 1e-3 -- far below
+// the network's own scatter (0.2 dex).
+struct TcMlpTc {
+  static constexpr int S1 = 12, S = 36;  // padded row strides (conflict-free fragment loads)
+  float W1[kMlpH * S1], W2[kMlpH * S], W3[kMlpH * S], W4[8 * S];
+  float b1[kMlpH], b2[kMlpH], b3[kMlpH], b4[8];
+};
+constexpr int kMlpActS = 36;  // row stride of a warp's activation buffer (32 rows)
+
+__device__ __forceinline__ float tc_to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+// weights (the flat layout of tc_mlp_forward) -> TF32, padded rows; W4 / b4 rows >= nout zero
+__device__ __forceinline__ void tc_mlp_tc_load(TcMlpTc& T, const float* __restrict__ w, int nout, int tid,
+                                               int nthr) {
   const float* W1 = w;
   const float* b1 = W1 + kMlpH * kMlpIn;
   const float* W2 = b1 + kMlpH;
@@ -106,36 +122,89 @@ __device__ __forceinline__ void tc_mlp_infer(const float* __restrict__ w, const 
   const float* W3 = b2 + kMlpH;
   const float* b3 = W3 + kMlpH * kMlpH;
   const float* W4 = b3 + kMlpH;
-  const float* b4 = W4 + NOUT * kMlpH;
-  float a[kMlpH], h[kMlpH];
-#pragma unroll
-  for (int j = 0; j < kMlpH; j++) {
-    float s = b1[j];
-#pragma unroll
-    for (int i = 0; i < kMlpIn; i++) s = fmaf(W1[j * kMlpIn + i], x[i], s);
-    a[j] = tc_tanh_fast(s);
+  const float* b4 = W4 + nout * kMlpH;
+  for (int i = tid; i < kMlpH * kMlpIn; i += nthr) T.W1[(i / kMlpIn) * TcMlpTc::S1 + i % kMlpIn] = tc_to_tf32(W1[i]);
+  for (int i = tid; i < kMlpH * kMlpH; i += nthr) {
+    T.W2[(i / kMlpH) * TcMlpTc::S + i % kMlpH] = tc_to_tf32(W2[i]);
+    T.W3[(i / kMlpH) * TcMlpTc::S + i % kMlpH] = tc_to_tf32(W3[i]);
   }
-#pragma unroll
-  for (int j = 0; j < kMlpH; j++) {
-    float s = b2[j];
-#pragma unroll
-    for (int i = 0; i < kMlpH; i++) s = fmaf(W2[j * kMlpH + i], a[i], s);
-    h[j] = tc_tanh_fast(s);
+  for (int i = tid; i < 8 * kMlpH; i += nthr)
+    T.W4[(i / kMlpH) * TcMlpTc::S + i % kMlpH] = i / kMlpH < nout ? tc_to_tf32(W4[i]) : 0.f;
+  for (int i = tid; i < kMlpH; i += nthr) {
+    T.b1[i] = b1[i];
+    T.b2[i] = b2[i];
+    T.b3[i] = b3[i];
   }
+  for (int i = tid; i < 8; i += nthr) T.b4[i] = i < nout ? b4[i] : 0.f;
+}
+
+__device__ __forceinline__ void tc_mma_tf32(float* d, const uint32_t* a, const uint32_t* b) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// one layer in place in act (32 rows): out[r][n] = f(bias[n] + sum_k act[r][k] W[n][k]) for the
+// NT * 8 outputs; fragment layouts of m16n8k8: A (g, t) (g + 8, t) (g, t + 4) (g + 8, t + 4),
+// B (k = t, n = g) (k = t + 4, n = g), C (g, 2t) (g, 2t + 1) (g + 8, 2t) (g + 8, 2t + 1), with
+// g = lane / 4, t = lane % 4
+template <int K, int NT, bool TANH>
+__device__ __forceinline__ void tc_mlp_tc_layer(float* act, const float* W, int ws, const float* bias, int lane) {
+  const int g = lane >> 2, t = lane & 3;
 #pragma unroll
-  for (int j = 0; j < kMlpH; j++) {
-    float s = b3[j];
+  for (int mt = 0; mt < 2; mt++) {
+    float acc[NT][4];
 #pragma unroll
-    for (int i = 0; i < kMlpH; i++) s = fmaf(W3[j * kMlpH + i], h[i], s);
-    a[j] = tc_tanh_fast(s);
+    for (int nt = 0; nt < NT; nt++) {
+      acc[nt][0] = acc[nt][2] = bias[nt * 8 + 2 * t];
+      acc[nt][1] = acc[nt][3] = bias[nt * 8 + 2 * t + 1];
+    }
+#pragma unroll
+    for (int kt = 0; kt < K / 8; kt++) {
+      const float* r0 = act + (mt * 16 + g) * kMlpActS + kt * 8;
+      const float* r1 = r0 + 8 * kMlpActS;
+      uint32_t a[4];
+      a[0] = __float_as_uint(tc_to_tf32(r0[t]));
+      a[1] = __float_as_uint(tc_to_tf32(r1[t]));
+      a[2] = __float_as_uint(tc_to_tf32(r0[t + 4]));
+      a[3] = __float_as_uint(tc_to_tf32(r1[t + 4]));
+#pragma unroll
+      for (int nt = 0; nt < NT; nt++) {
+        const float* wr = W + (nt * 8 + g) * ws + kt * 8;
+        const uint32_t b[2] = {__float_as_uint(wr[t]), __float_as_uint(wr[t + 4])};
+        tc_mma_tf32(acc[nt], a, b);
+      }
+    }
+    __syncwarp();  // rows mt * 16 .. + 15 are read by every lane before they are overwritten
+#pragma unroll
+    for (int nt = 0; nt < NT; nt++) {
+      float* o0 = act + (mt * 16 + g) * kMlpActS + nt * 8 + 2 * t;
+      float* o1 = o0 + 8 * kMlpActS;
+      o0[0] = TANH ? tc_tanh_fast(acc[nt][0]) : acc[nt][0];
+      o0[1] = TANH ? tc_tanh_fast(acc[nt][1]) : acc[nt][1];
+      o1[0] = TANH ? tc_tanh_fast(acc[nt][2]) : acc[nt][2];
+      o1[1] = TANH ? tc_tanh_fast(acc[nt][3]) : acc[nt][3];
+    }
+    __syncwarp();
   }
+}
+
+// warp-wide: every lane passes its pair's standardised features x and gets its outputs y
+template <int NOUT>
+__device__ __forceinline__ void tc_mlp_infer_tc(const TcMlpTc& T, float* act, const float* x, float* y, int lane) {
+  static_assert(NOUT <= 8, "one output tile");
 #pragma unroll
-  for (int j = 0; j < NOUT; j++) {
-    float s = b4[j];
+  for (int i = 0; i < kMlpIn; i++) act[lane * kMlpActS + i] = x[i];
+  __syncwarp();
+  tc_mlp_tc_layer<kMlpIn, 4, true>(act, T.W1, TcMlpTc::S1, T.b1, lane);
+  tc_mlp_tc_layer<kMlpH, 4, true>(act, T.W2, TcMlpTc::S, T.b2, lane);
+  tc_mlp_tc_layer<kMlpH, 4, true>(act, T.W3, TcMlpTc::S, T.b3, lane);
+  tc_mlp_tc_layer<kMlpH, 1, false>(act, T.W4, TcMlpTc::S, T.b4, lane);
 #pragma unroll
-    for (int i = 0; i < kMlpH; i++) s = fmaf(W4[j * kMlpH + i], a[i], s);
-    y[j] = s;
-  }
+  for (int j = 0; j < NOUT; j++) y[j] = act[lane * kMlpActS + j];
+  __syncwarp();
 }
 
 // The per-cell part of the selector's features (tc_pair_features): the source spectrum ratios

@@ -641,14 +641,28 @@ __device__ __forceinline__ TcAcc<JERK> tc_mixp_total(const TcMixP<JERK>& T) {
 // The next tile of a target's sources, taken as one sequence of bodies (its source cells'
 // bodies one after the other), so a tile holds 32 sources even where the source leaves are
 // small.  (q, off) is the warp-uniform cursor: the next source cell and the next body in it.
-// Returns the tile's count; lane l gets the body index of slot l (-1 past the count).
+// The first body and body count of cells q0 + l are held by lane l (cjb, cjn), reloaded 32 cells
+// at a time.  Returns the tile's count; lane l gets the body index of slot l (-1 past the count).
+__device__ __forceinline__ void tc_src_cells(const int* __restrict__ src, const TcCells& c, int q0, int se, int lane,
+                                             int& cjb, int& cjn) {
+  cjb = 0;
+  cjn = 0;
+  if (q0 + lane < se) {
+    const int s = src[q0 + lane];
+    cjb = c.begin[s];
+    cjn = c.nbody[s];
+  }
+}
 __device__ __forceinline__ int tc_next_tile(const int* __restrict__ src, const TcCells& c, int se, int& q, int& off,
-                                            int lane, int& myj) {
+                                            int& q0, int& cjb, int& cjn, int lane, int& myj) {
   int fill = 0;
   myj = -1;
   while (fill < 32 && q < se) {
-    const int s = src[q];
-    const int jb = c.begin[s], jn = c.nbody[s];
+    if (q >= q0 + 32) {
+      q0 = q;
+      tc_src_cells(src, c, q0, se, lane, cjb, cjn);
+    }
+    const int jb = __shfl_sync(0xffffffffu, cjb, q - q0), jn = __shfl_sync(0xffffffffu, cjn, q - q0);
     const int take = min(32 - fill, jn - off);
     if (lane >= fill && lane < fill + take) myj = jb + off + lane - fill;
     fill += take;
@@ -691,9 +705,11 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __re
       int nrl = 0;  // strong pairs this lane met
       TcMixP<JERK> A;
       tc_mixp_init<JERK>(A, b, out, i, act, Xc, Yc, Zc, excl_frac);
+      int q0 = sb, cjb, cjn;
+      tc_src_cells(src, c, q0, se, lane, cjb, cjn);
       for (int q = sb, off = 0; q < se;) {
         int myj;
-        const int cnt = tc_next_tile(src, c, se, q, off, lane, myj), np = (cnt + 1) >> 1;
+        const int cnt = tc_next_tile(src, c, se, q, off, q0, cjb, cjn, lane, myj), np = (cnt + 1) >> 1;
         __syncwarp();
         if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, myj, Xc, Yc, Zc);
         tj[w][lane] = myj;
@@ -724,9 +740,11 @@ __global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __re
         const double xi = ovf ? b.x[i] : 0.0, yi = ovf ? b.y[i] : 0.0, zi = ovf ? b.z[i] : 0.0;
         const double vxi = (JERK && ovf) ? b.vx[i] : 0.0, vyi = (JERK && ovf) ? b.vy[i] : 0.0,
                      vzi = (JERK && ovf) ? b.vz[i] : 0.0;
+        q0 = sb;
+        tc_src_cells(src, c, q0, se, lane, cjb, cjn);
         for (int q = sb, off = 0; q < se;) {
           int myj;
-          const int cnt = tc_next_tile(src, c, se, q, off, lane, myj), np = (cnt + 1) >> 1;
+          const int cnt = tc_next_tile(src, c, se, q, off, q0, cjb, cjn, lane, myj), np = (cnt + 1) >> 1;
           __syncwarp();
           if (lane < 2 * np) tc_tile_put<JERK>(TL, lane, b, myj, Xc, Yc, Zc);
           tj[w][lane] = myj;

@@ -30,6 +30,22 @@ struct TcOrderClasses<16> {
   static __host__ __device__ constexpr int at(int i) { return i < 2 ? 10 + 2 * i : 16; }
 };
 
+// The M2L launches of the order classes: launch i runs classes [first(i), first(i + 1)), at the
+// order of its last class.  A pair of a lower class in a launch carries its own order in its
+// source entry, and a 32-pair batch runs at the highest order among its pairs.  At p = 12 the
+// two upper classes share a launch: the order-12 class alone is short per target (about 60
+// pairs, two batches), which would leave most of a launch's warp groups idle.
+template <int P>
+struct TcClassLaunches {
+  static constexpr int n = TcOrderClasses<P>::n;
+  static __host__ __device__ constexpr int first(int i) { return i; }
+};
+template <>
+struct TcClassLaunches<12> {
+  static constexpr int n = 2;
+  static __host__ __device__ constexpr int first(int i) { return i == 0 ? 0 : (i == 1 ? 1 : 3); }
+};
+
 #define TC_MAX_CLASSES 6
 #define TC_NFEAT 8
 

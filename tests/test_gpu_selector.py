@@ -67,7 +67,8 @@ def test_mlp_gradient_matches_numpy_oracle():
     pred = np.zeros((ns, nout), np.float32)
     assert L.tc_mlp_predict(ns, nout, feat.ctypes.data_as(FP), w.ctypes.data_as(FP), norm.ctypes.data_as(FP),
                             pred.ctypes.data_as(FP)) == 0
-    assert np.abs(pred - omlp.predict(w, nout, feat, norm.astype(np.float64))).max() < 1e-4
+    # the selector's inference has TF32 operands and the hardware tanh: about 1e-3 in log10 units
+    assert np.abs(pred - omlp.predict(w, nout, feat, norm.astype(np.float64))).max() < 1e-2
 
 
 @pytest.fixture(scope="module")

@@ -431,13 +431,15 @@ __global__ void k_p2p_count(const unsigned long long* __restrict__ keys, unsigne
 // from the previous evaluation's accelerations, then each target's list regrouped by order
 // ----------------------------------------------------------------------------------------
 // With an order selector on, accepted pairs of a leaf target whose body counts multiply to at
-// most this many interactions are summed directly (exact) instead of by an M2L: below it the
-// near field's cost (about 3 ps of the whole GPU per FP32 interaction) is under a p = 12 M2L's
-// (about 1.7 ns per pair), scaled by (p + 1)^3.  0 (fixed order, the reference's lists) = off.
+// most this many interactions are summed directly (exact) instead of by an M2L, scaled by
+// (p + 1)^3.  At N = 4M, p = 12 the step time is flat from 256 to 1024 (the near field's
+// FP32 interactions, about 2.7 ps of the whole GPU each, against about 2 ns per M2L pair) while
+// the force error falls (1.28e-8 -> 1.11e-8 RMS at 512); 0 (fixed order, the reference's
+// lists) = off.
 static long long p2p_instead_max(const tc_params& prm) {
   if (prm.selector <= 0) return 0;
   const double s = (prm.p + 1.0) / 13.0;
-  return (long long)(256.0 * s * s * s);
+  return (long long)(512.0 * s * s * s);
 }
 
 // the orders used by an evaluation: h[k] pairs of class k, of order q[k] (ascending)

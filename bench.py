@@ -89,7 +89,7 @@ def parse():
                          "on the GPU on pairs of this workload before the timed region)")
     ap.add_argument("--train-ics", default=None, choices=["plummer_kroupa", "plummer", "fractal"],
                     help="--selector 2: train on these initial conditions (same n) instead of the workload's own")
-    ap.add_argument("--selector-tol", type=float, default=2e-9,
+    ap.add_argument("--selector-tol", type=float, default=3e-9,
                     help="per-pair truncation error budget relative to the target cell's least |a|")
     ap.add_argument("--no-fp64-arm", action="store_true", help="skip timing the plain FP64 form alongside")
     ap.add_argument("--accuracy-targets", type=int, default=4096,

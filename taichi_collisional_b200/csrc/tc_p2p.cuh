@@ -675,8 +675,11 @@ __device__ __forceinline__ int tc_next_tile(const int* __restrict__ src, const T
   return fill;
 }
 
+// Seven CTAs (28 warps) per SM: the register cap (73) spills a few words per thread, and the
+// occupancy still wins at N = 4M (79.6 ms against 84.2 ms at five CTAs, 81.2 at six; the compensated
+// totals kept in shared memory instead of registers measured no better).
 template <bool JERK>
-__global__ void __launch_bounds__(kP2PWarps * 32, 5) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
+__global__ void __launch_bounds__(kP2PWarps * 32, 7) k_p2p_mixed(const int* __restrict__ tlist, int ntl,
                                                                  const int* __restrict__ tstart,
                                                                  const int* __restrict__ src, const TcBodies b,
                                                                  const TcCells c, TcOut out, float excl_frac,

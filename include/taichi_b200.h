@@ -63,8 +63,12 @@ typedef struct {
   int device;         /* CUDA device ordinal                                               */
   int selector;       /* far-field order per pair: 0 fixed p (the reference), 1 analytic error
                          estimate (the reference's MAC estimate, traverse_eager.h:82-96),
-                         2 learned (MLP, after tc_train_selector)                         */
-  double selector_tol;/* per-pair tolerance: |acc error| <= tol * M_source / r^2            */
+                         2 learned (MLP, after tc_train_selector).  With a selector on,
+                         accepted pairs of a leaf target whose body counts multiply to at most
+                         512 ((p+1)/13)^3 are summed directly instead of by an M2L          */
+  double selector_tol;/* per-pair budget: the predicted |acc error| of a pair's M2L at most tol
+                         times the least |a| among the target cell's bodies in the previous
+                         evaluation of the same bodies (the first evaluation runs at fixed p) */
   int judge_n;        /* >0: after each evaluation, FP64 direct sums at judge_n seeded bodies;
                          with a selector, an RMS relative acceleration error above judge_tol
                          makes the call redo the far field at the fixed order p             */

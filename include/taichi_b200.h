@@ -281,6 +281,17 @@ tc_status tc_split_order(tc_ctx* ctx, int n, const double* timestep, double dt, 
 tc_status tc_evolve_hold_dkd(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
                              double* ez, double* vx, double* vy, double* vz, double* m, double* timestep,
                              double* pot, int* id, double dt_param, double dt, tc_evolve_stats* st);
+/* The same step with the reference's default scheme, the force-gradient integrator of its
+ * GRADIENT / OUTPUTACC build: do_evolve with evolve_split_omelyan (integrator.h:720-812) --
+ * kicks of dt / 6 around the recursion and the drifts, and in the middle kick_gradient
+ * (integrator.h:313-376): 2 dt / 3 kicks with the forces evaluated at x + acc dt^2 / 24, acc
+ * being the force of the last kick_naive, whose GRADIENT form gives every body the least time
+ * step of its system (integrator.h:254-299).  Arguments and outputs as tc_evolve_hold_dkd;
+ * acc is kept inside the context (3 n doubles more).  Where kick_gradient stores an
+ * uninitialised array as the potential, the potential stays as the preceding kick set it. */
+tc_status tc_evolve_omelyan(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
+                            double* ez, double* vx, double* vy, double* vz, double* m, double* timestep,
+                            double* pot, int* id, double dt_param, double dt, tc_evolve_stats* st);
 
 /* Hermite 4th-order step with one shared time step (Makino & Aarseth 1992), consuming the
  * accelerations and jerks of the jerks tree; no counterpart in the reference, whose jerks tree

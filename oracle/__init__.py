@@ -460,14 +460,14 @@ def ref_split(ts, dt):
     return perm, nf
 
 
-def integ_shim_path():
-    return os.path.join(HERE, "_ref", "libtcref_integ_shim_%s.so" % _isa())
+def integ_shim_path(gradient=False):
+    return os.path.join(HERE, "_ref", "libtcref_integ_shim_%s%s.so" % ("grad_" if gradient else "", _isa()))
 
 
-def _evolve_lib(shim):
-    key = "integ_shim" if shim else "integ"
+def _evolve_lib(shim, gradient=False):
+    key = ("integ_shim_grad" if gradient else "integ_shim") if shim else "integ"
     if shim and key not in _ref_libs:
-        _ref_libs[key] = C.CDLL(integ_shim_path())
+        _ref_libs[key] = C.CDLL(integ_shim_path(gradient))
     L = _ref_libs[key] if shim else _integ_ref()
     L.tcr_evolve_hold.argtypes = [C.c_int] + [_dp] * 12 + [_ip, C.c_int, C.c_double, C.c_double, C.c_double,
                                                            C.c_double]
@@ -485,6 +485,18 @@ def ref_evolve_hold(state, *, ncrit, theta, force_accuracy, dt_param, dt, shim=F
     st = {k: np.array(state[k], dtype=np.float64) for k in EVOLVE_KEYS}
     st["id"] = np.array(state["id"], dtype=np.int32)
     L = _evolve_lib(shim)
+    t = L.tcr_evolve_hold(len(st["x"]), *[_d(st[k]) for k in EVOLVE_KEYS], st["id"].ctypes.data_as(_ip), ncrit,
+                          theta, force_accuracy, dt_param, dt)
+    return st, t
+
+
+def ref_evolve_gradient(state, *, ncrit, theta, force_accuracy, dt_param, dt):
+    """One do_evolve step of the reference's force-gradient scheme (evolve_split_omelyan, its
+    GRADIENT / OUTPUTACC build) over this repository's force evaluation through the C++ shim.
+    Returns (new state, simtime)."""
+    st = {k: np.array(state[k], dtype=np.float64) for k in EVOLVE_KEYS}
+    st["id"] = np.array(state["id"], dtype=np.int32)
+    L = _evolve_lib(True, gradient=True)
     t = L.tcr_evolve_hold(len(st["x"]), *[_d(st[k]) for k in EVOLVE_KEYS], st["id"].ctypes.data_as(_ip), ncrit,
                           theta, force_accuracy, dt_param, dt)
     return st, t

@@ -7,7 +7,9 @@
 //   drift with COMPSUM (integrator.h:42, :642-656),
 //   split by time step (integrator.h:591-640),
 //   one do_evolve step (integrator.h:873-890) of the HOLD scheme evolve_split_hold_dkd
-//   (integrator.h:834-871) with the reference's own force evaluation (error-controlled MAC),
+//   (integrator.h:834-871) with the reference's own force evaluation (error-controlled MAC) --
+//   or, in a build with GRADIENT and OUTPUTACC, of the force-gradient scheme
+//   evolve_split_omelyan (integrator.h:720-812),
 // so the oracle's restatements and the CUDA kernels can be pinned against them.  The same
 // source, compiled with TCR_SHIM, drives the reference's integrator over this repository's
 // force evaluation instead (taichi_collisional_b200/host/tc_force_shim.hpp): the Makefile then
@@ -90,8 +92,8 @@ int tcr_split(int n, const double* ts, double dt, int* perm) {
   return (int)fast.n;
 }
 
-// one do_evolve(mainsys, dt) of the HOLD scheme on n particles (arrays in and out, in the order
-// the particles end in; id[] follows them); returns diag->simtime advanced
+// one do_evolve(mainsys, dt) of the build's scheme (HOLD, or GRADIENT) on n particles (arrays in
+// and out, in the order the particles end in; id[] follows them); returns diag->simtime advanced
 double tcr_evolve_hold(int n, double* x, double* y, double* z, double* ex, double* ey, double* ez, double* vx,
                        double* vy, double* vz, double* m, double* ts, double* pot, int* id, int nc, double th,
                        double fa, double dtp, double dt) {

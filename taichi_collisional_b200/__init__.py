@@ -60,7 +60,7 @@ EXPORTS = ["tc_default_params", "tc_create", "tc_destroy", "tc_set_stream", "tc_
            "tc_pmax", "tc_order_supported", "tc_kick_drift", "tc_probe_peak", "tc_evaluate_direct_noalloc",
            "tc_train_selector", "tc_get_selector_data", "tc_selector_nparam", "tc_get_selector_weights",
            "tc_set_selector_weights", "tc_mlp_loss_grad", "tc_mlp_predict", "tc_set_selector", "tc_tc_bins", "tc_direct_sums", "tc_evaluate_steps", "tc_set_graph", "tc_graph_ready", "tc_graph_note", "tc_set_error_mac", "tc_get_acc_old", "tc_hermite_predict", "tc_hermite_correct",
-           "tc_system_diagnostics", "tc_drift_compensated", "tc_split_order", "tc_evolve_hold_dkd", "tc_step_leapfrog",
+           "tc_system_diagnostics", "tc_drift_compensated", "tc_split_order", "tc_evolve_hold_dkd", "tc_evolve_omelyan", "tc_step_leapfrog",
            "tc_set_wait_limit"]
 NOALLOC_MAX_N = 16384
 
@@ -132,6 +132,8 @@ def load_library(path=LIB_PATH):
     L.tc_evolve_hold_dkd.argtypes = [C.c_void_p, C.c_int] + [C.c_void_p] * 13 + [C.c_double, C.c_double,
                                                                                  C.POINTER(EvolveStats)]
     L.tc_evolve_hold_dkd.restype = C.c_int
+    L.tc_evolve_omelyan.argtypes = L.tc_evolve_hold_dkd.argtypes
+    L.tc_evolve_omelyan.restype = C.c_int
     L.tc_probe_peak.argtypes = [C.c_void_p, C.c_int]
     L.tc_probe_peak.restype = C.c_double
     L.tc_evaluate_direct_noalloc.argtypes = [C.c_int] + [C.c_void_p] * 8 + [C.c_void_p] * 7 + [C.c_int, C.c_void_p]
@@ -385,6 +387,15 @@ class Gravity:
         rc = self._L.tc_evolve_hold_dkd(self._h, len(state["x"]), *[_ptr(state[k]) for k in EVOLVE_KEYS],
                                         _ptr(state["id"]), float(dt_param), float(dt), C.byref(st))
         self._check(rc, "tc_evolve_hold_dkd")
+        return {k: getattr(st, k) for k, _ in EvolveStats._fields_}
+
+    def evolve_omelyan(self, state, dt_param, dt):
+        """One step dt of the reference's default force-gradient scheme (tc_evolve_omelyan), as
+        evolve_hold_dkd."""
+        st = EvolveStats()
+        rc = self._L.tc_evolve_omelyan(self._h, len(state["x"]), *[_ptr(state[k]) for k in EVOLVE_KEYS],
+                                       _ptr(state["id"]), float(dt_param), float(dt), C.byref(st))
+        self._check(rc, "tc_evolve_omelyan")
         return {k: getattr(st, k) for k, _ in EvolveStats._fields_}
 
     def hermite_predict(self, x, y, z, vx, vy, vz, a, save, dt):

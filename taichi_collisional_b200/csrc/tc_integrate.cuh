@@ -44,7 +44,8 @@ __global__ void k_split_pairs(int ns, int nf, const double* __restrict__ ts, dou
 }
 
 struct TcEvArrays {
-  double* d[12];  // x y z ex ey ez vx vy vz m timestep pot
+  double* d[15];  // x y z ex ey ez vx vy vz m timestep pot (+ acc x y z for the gradient scheme)
+  int nd;         // how many of d travel with the particles (12, or 15 with acc)
   int* id;
 };
 
@@ -53,7 +54,8 @@ __global__ void k_split_swap(int nswap, TcEvArrays a, const int* __restrict__ po
   if (r >= nswap) return;
   const int L = posL[r], R = posR[r];
 #pragma unroll
-  for (int q = 0; q < 12; q++) {
+  for (int q = 0; q < 15; q++) {
+    if (q >= a.nd) break;
     const double t = a.d[q][L];
     a.d[q][L] = a.d[q][R];
     a.d[q][R] = t;
@@ -109,11 +111,49 @@ __global__ void k_ev_zero_pot(int nk, double* __restrict__ pot) {
   if (k < nk) pot[k] = 0.0;
 }
 
+// The GRADIENT build of kick_naive (integrator.h:254-299): every sink's time step becomes the
+// least over the system, 1 / sqrt(sqrt(sum 1/tau^4)) minimised (HUGE when every sum is 0), and
+// (OUTPUTACC) its acc the pass's force.  Time steps are >= 0, so their bit patterns order as
+// the values do and one atomicMin finds the least.
+__global__ void k_ev_ts_min(int ns, const double* __restrict__ tsum, unsigned long long* __restrict__ mn) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < ns) atomicMin(mn, (unsigned long long)__double_as_longlong(1.0 / sqrt(sqrt(tsum[k]))));
+}
+__global__ void k_ev_naive_grad(int ns, const double* __restrict__ ax, const double* __restrict__ ay,
+                                const double* __restrict__ az, const double* __restrict__ apot,
+                                const unsigned long long* __restrict__ mn, double* __restrict__ ts,
+                                double* __restrict__ pot, double* __restrict__ accx, double* __restrict__ accy,
+                                double* __restrict__ accz) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  ts[k] = __longlong_as_double((long long)*mn);
+  pot[k] = apot[k];
+  accx[k] = ax[k];
+  accy[k] = ay[k];
+  accz[k] = az[k];
+}
+
+// kick_gradient's positions (integrator.h:313-351): X = pos + acc dt^2 / 24
+__global__ void k_ev_shift(int ns, const double* __restrict__ x, const double* __restrict__ y,
+                           const double* __restrict__ z, const double* __restrict__ accx,
+                           const double* __restrict__ accy, const double* __restrict__ accz, double fac,
+                           double* __restrict__ xs, double* __restrict__ ys, double* __restrict__ zs) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ns) return;
+  xs[k] = x[k] + accx[k] * fac;
+  ys[k] = y[k] + accy[k] * fac;
+  zs[k] = z[k] + accz[k] * fac;
+}
+
+__global__ void k_ev_set_u64(unsigned long long* p, unsigned long long v) { *p = v; }
+
 struct TcEvolve {
   tc_ctx* ctx;
   TcEvArrays a;
   double dt_param;
   double *ax, *ay, *az, *apot, *tsum;
+  double *xs, *ys, *zs;    // kick_gradient's shifted positions (gradient scheme only)
+  unsigned long long* mn;  // the least time step of a GRADIENT kick_naive (bit pattern)
   uint32_t* cnt;
   uint32_t* sums;
   int *posL, *posR, *small;
@@ -187,7 +227,7 @@ struct TcEvolve {
     if (nswap > 0) {
       k_split_pairs<<<nblocks(ns, 256), 256, 0, s>>>(ns, nf, ts, adt, cnt, posL, posR);
       TcEvArrays sub = a;
-      for (int q = 0; q < 12; q++) sub.d[q] += off;
+      for (int q = 0; q < a.nd; q++) sub.d[q] += off;
       sub.id += off;
       k_split_swap<<<nblocks(nswap, 256), 256, 0, s>>>(nswap, sub, posL, posR);
     }
@@ -235,6 +275,113 @@ struct TcEvolve {
     if (nf > 0 && (r = hold_dkd(clevel + 1, off, nf, dt / 2, true)) != TC_OK) return r;
     return TC_OK;
   }
+  // kick_naive(clevel, s, 0, 0, 0, true) as the GRADIENT build runs it (integrator.h:254-299)
+  tc_status naive_grad(int off, int ns) {
+    const cudaStream_t s = ctx->stream;
+    tc_status r = tc_evaluate_steps(ctx, ns, X(0, off), X(1, off), X(2, off), X(6, off), X(7, off), X(8, off),
+                                    X(9, off), nullptr, dt_param, ax, ay, az, apot, tsum, TC_MEM_DEVICE);
+    if (r != TC_OK) return r;
+    k_ev_set_u64<<<1, 1, 0, s>>>(mn, 0x7FF0000000000000ull);  // +inf (HUGE_VAL)
+    k_ev_ts_min<<<nblocks(ns, 256), 256, 0, s>>>(ns, tsum, mn);
+    k_ev_naive_grad<<<nblocks(ns, 256), 256, 0, s>>>(ns, ax, ay, az, apot, mn, X(10, off), X(11, off), X(12, off),
+                                                     X(13, off), X(14, off));
+    st.n_evaluations++;
+    return cudaGetLastError() == cudaSuccess ? TC_OK : TC_ERR_CUDA;
+  }
+
+  // kick_gradient (integrator.h:313-376) of [k0, k1) with the flags in fl over [off, off + ns):
+  // the forces at X = pos + acc dt^2 / 24, then v += F 2 dt / 3.  The reference then stores an
+  // uninitialised array as the potential; the potential is left as the last kick set it.
+  tc_status gkick(int off, int ns, int k0, int k1, double dt) {
+    const cudaStream_t s = ctx->stream;
+    k_ev_shift<<<nblocks(ns, 256), 256, 0, s>>>(ns, X(0, off), X(1, off), X(2, off), X(12, off), X(13, off),
+                                                X(14, off), dt * dt / 24.0, xs, ys, zs);
+    tc_status r = tc_evaluate(ctx, ns, xs, ys, zs, nullptr, nullptr, nullptr, X(9, off), fl, ax, ay, az, apot, nullptr,
+                              nullptr, nullptr, TC_MEM_DEVICE);
+    st.n_evaluations++;
+    if (r != TC_OK) return r;
+    if (k1 > k0)
+      k_ev_kick<<<nblocks(k1 - k0, 256), 256, 0, s>>>(k0, k1, ax, ay, az, apot, X(6, off), X(7, off), X(8, off),
+                                                      X(11, off), dt * 2.0 / 3.0, 0);
+    return cudaGetLastError() == cudaSuccess ? TC_OK : TC_ERR_CUDA;
+  }
+
+  // the dt / 6 kicks that open and close evolve_split_omelyan (integrator.h:741-754, :797-811)
+  tc_status omelyan_outer(int off, int ns, int nf, double dtk) {
+    const int nslow = ns - nf;
+    tc_status r;
+    if (ns > 128) {
+      if (nslow > 0) {
+        flags(ns, nf, 2, 3);  // kick(slow, fast, dt / 6, sinks_are_fast = false)
+        if ((r = kick(off, ns, nf, ns, dtk, false)) != TC_OK) return r;
+      }
+      if (nf > 0 && nslow > 0) {
+        flags(ns, nf, 1, 2);  // kick(fast, slow, dt / 6, sinks_are_fast = true)
+        if ((r = kick(off, ns, 0, nf, dtk, false)) != TC_OK) return r;
+      } else if (nf > 0) {
+        k_ev_zero_pot<<<nblocks(nf, 256), 256, 0, ctx->stream>>>(nf, X(11, off));  // no source: F = 0, p = 0
+      }
+    } else if (nslow > 0) {
+      flags(ns, nf, 2, 3);  // kick_cpu(slow, join(slow, fast), dt / 6)
+      if ((r = kick(off, ns, nf, ns, dtk, true)) != TC_OK) return r;
+      if (nf > 0) {
+        flags(ns, nf, 1, 2);  // kick_cpu(fast, slow, dt / 6)
+        if ((r = kick(off, ns, 0, nf, dtk, true)) != TC_OK) return r;
+      }
+    }
+    return TC_OK;
+  }
+
+  // evolve_split_omelyan(clevel, s, stime, etime, dt, calc_timestep) (integrator.h:720-812), the
+  // force-gradient scheme of the reference's default build (GRADIENT, OUTPUTACC), on
+  // s = [off, off + ns)
+  tc_status omelyan(int clevel, int off, int ns, double dt, bool calc_timestep) {
+    if (clevel > kMaxLevelEvolve) {
+      ctx->err = "time-step hierarchy deeper than 64 levels (a time step is zero or not finite)";
+      return TC_ERR_ARG;
+    }
+    st.max_level = std::max(st.max_level, clevel);
+    tc_status r;
+    if (calc_timestep && (r = naive_grad(off, ns)) != TC_OK) return r;
+    int nf = 0;
+    if ((r = split(off, ns, dt, &nf)) != TC_OK) return r;
+    const int nslow = ns - nf;
+    if (nf == 0) st.simtime += dt;
+    if ((r = omelyan_outer(off, ns, nf, dt / 6)) != TC_OK) return r;
+    if (nf > 0 && (r = omelyan(clevel + 1, off, nf, dt / 2, false)) != TC_OK) return r;
+    if ((r = drift(off + nf, nslow, dt / 2)) != TC_OK) return r;
+    // the middle: zero-length kicks that set the potential, then the gradient kicks (2 dt / 3)
+    // with the positions shifted by the acc of the last kick_naive
+    if (nslow > 0) {
+      flags(nslow, 0, 3, 3);  // kick(slow, zerosys, 0): the slow bodies alone
+      if ((r = kick(off + nf, nslow, 0, nslow, 0.0, false)) != TC_OK) return r;
+      flags(nslow, 0, 3, 3);  // kick_gradient(slow, zerosys, dt)
+      if ((r = gkick(off + nf, nslow, 0, nslow, dt)) != TC_OK) return r;
+      if (nf > 0) {
+        flags(ns, nf, 2, 1);  // kick(slow, fast, 0, sinks_are_fast = true)
+        if ((r = kick(off, ns, nf, ns, 0.0, false)) != TC_OK) return r;
+      } else {
+        k_ev_zero_pot<<<nblocks(nslow, 256), 256, 0, ctx->stream>>>(nslow, X(11, off + nf));
+      }
+    }
+    if (nf > 0) {
+      if (nslow > 0) {
+        flags(ns, nf, 1, 2);  // kick(fast, slow, 0, sinks_are_fast = true)
+        if ((r = kick(off, ns, 0, nf, 0.0, false)) != TC_OK) return r;
+      } else {
+        k_ev_zero_pot<<<nblocks(nf, 256), 256, 0, ctx->stream>>>(nf, X(11, off));
+      }
+    }
+    if (nslow > 0 && nf > 0) {
+      flags(ns, nf, 2, 1);  // kick_gradient(slow, fast, dt, true)
+      if ((r = gkick(off, ns, nf, ns, dt)) != TC_OK) return r;
+      flags(ns, nf, 1, 2);  // kick_gradient(fast, slow, dt, true)
+      if ((r = gkick(off, ns, 0, nf, dt)) != TC_OK) return r;
+    }
+    if ((r = drift(off + nf, nslow, dt / 2)) != TC_OK) return r;
+    if (nf > 0 && (r = omelyan(clevel + 1, off, nf, dt / 2, true)) != TC_OK) return r;
+    return omelyan_outer(off, ns, nf, dt / 6);
+  }
   static constexpr int kMaxLevelEvolve = 64;  // MAXLEVEL, integrator.h:8
 };
 
@@ -267,10 +414,11 @@ extern "C" tc_status tc_split_order(tc_ctx* ctx, int n, const double* timestep, 
   return TC_OK;
 }
 
-extern "C" tc_status tc_evolve_hold_dkd(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
-                                        double* ez, double* vx, double* vy, double* vz, double* m, double* timestep,
-                                        double* pot, int* id, double dt_param, double dt, tc_evolve_stats* st) {
-  using namespace tc;
+namespace tc {
+// one do_evolve(s, dt) (integrator.h:873-890) of the HOLD (gradient = false) or the GRADIENT scheme
+static tc_status tc_evolve_run(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
+                               double* ez, double* vx, double* vy, double* vz, double* m, double* timestep,
+                               double* pot, int* id, double dt_param, double dt, tc_evolve_stats* st, bool gradient) {
   if (!ctx || n <= 0 || !x || !y || !z || !ex || !ey || !ez || !vx || !vy || !vz || !m || !timestep || !pot || !id ||
       !(dt != 0.0) || !std::isfinite(dt))
     return TC_ERR_ARG;
@@ -279,8 +427,10 @@ extern "C" tc_status tc_evolve_hold_dkd(tc_ctx* ctx, int n, double* x, double* y
     return TC_ERR_UNSUPPORTED;
   }
   TC_CK(cudaSetDevice(ctx->prm.device));
-  TC_CK(ctx->ev_d.ensure(5 * (size_t)n));
-  TC_CK(ctx->ev_u.ensure((size_t)n + (size_t)n / 4096 + 2));
+  TC_CK(ctx->ev_d.ensure((gradient ? 11 : 5) * (size_t)n));
+  // marks and scan sums (n + n / 4096 + 2), then the 8-byte least time step on an even index
+  const size_t mn_at = ((size_t)n + (size_t)n / 4096 + 3) & ~(size_t)1;
+  TC_CK(ctx->ev_u.ensure(mn_at + 2));
   TC_CK(ctx->ev_i.ensure(2 * (size_t)n + 2));
   TC_CK(ctx->ev_f.ensure((size_t)n));
   // systems of at most kDirectMax bodies are kicked by direct sums (kick_cpu)
@@ -293,18 +443,40 @@ extern "C" tc_status tc_evolve_hold_dkd(tc_ctx* ctx, int n, double* x, double* y
   E.ctx = ctx;
   double* arr[12] = {x, y, z, ex, ey, ez, vx, vy, vz, m, timestep, pot};
   for (int q = 0; q < 12; q++) E.a.d[q] = arr[q];
+  E.a.nd = 12;
   E.a.id = id;
   E.dt_param = dt_param;
   E.ax = ctx->ev_d.p; E.ay = E.ax + n; E.az = E.ay + n; E.apot = E.az + n; E.tsum = E.apot + n;
+  E.xs = E.ys = E.zs = nullptr;
+  if (gradient) {
+    // the particles' acc (OUTPUTACC) travels with them through the splits
+    E.a.d[12] = E.tsum + n; E.a.d[13] = E.a.d[12] + n; E.a.d[14] = E.a.d[13] + n;
+    E.a.nd = 15;
+    E.xs = E.a.d[14] + n; E.ys = E.xs + n; E.zs = E.ys + n;
+  }
   E.cnt = ctx->ev_u.p; E.sums = E.cnt + n;
+  E.mn = (unsigned long long*)(ctx->ev_u.p + mn_at);
   E.posL = ctx->ev_i.p; E.posR = E.posL + n; E.small = E.posR + n;
   E.fl = ctx->ev_f.p;
   E.st = tc_evolve_stats{};
   // do_evolve (integrator.h:873-890): kick_naive(0, s, 0, 0, 0, true), then the scheme with
   // calc_timestep = true, whose first act is the same kick_naive on the same state; the
   // result of the first is overwritten unchanged by the second, so it is done once.
-  tc_status r = E.hold_dkd(0, 0, n, dt, true);
+  tc_status r = gradient ? E.omelyan(0, 0, n, dt, true) : E.hold_dkd(0, 0, n, dt, true);
   if (r == TC_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess) r = TC_ERR_CUDA;
   if (st) *st = E.st;
   return r;
+}
+}  // namespace tc
+
+extern "C" tc_status tc_evolve_hold_dkd(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
+                                        double* ez, double* vx, double* vy, double* vz, double* m, double* timestep,
+                                        double* pot, int* id, double dt_param, double dt, tc_evolve_stats* st) {
+  return tc::tc_evolve_run(ctx, n, x, y, z, ex, ey, ez, vx, vy, vz, m, timestep, pot, id, dt_param, dt, st, false);
+}
+
+extern "C" tc_status tc_evolve_omelyan(tc_ctx* ctx, int n, double* x, double* y, double* z, double* ex, double* ey,
+                                       double* ez, double* vx, double* vy, double* vz, double* m, double* timestep,
+                                       double* pot, int* id, double dt_param, double dt, tc_evolve_stats* st) {
+  return tc::tc_evolve_run(ctx, n, x, y, z, ex, ey, ez, vx, vy, vz, m, timestep, pot, id, dt_param, dt, st, true);
 }

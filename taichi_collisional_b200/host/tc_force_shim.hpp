@@ -60,6 +60,9 @@ inline void get_force_and_potential(Bodies& bodies, bool get_steps) {
   get_steps = false;
 #endif
   const int n = (int)bodies.size();
+  // an empty body list is a call the reference makes (the force-gradient scheme kicks an empty
+  // slow system when every body is fast): nothing to evaluate
+  if (n == 0) return;
   std::vector<double> x(n), y(n), z(n), vx(n), vy(n), vz(n), m(n), ax(n), ay(n), az(n), pot(n), jx(n), jy(n),
       jz(n), ts(n);
   std::vector<unsigned char> flags(n);

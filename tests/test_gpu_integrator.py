@@ -107,13 +107,13 @@ def _evolve_state(gen, n, seed):
                 id=np.arange(n, dtype=np.int32))
 
 
-def _run_device(st0, *, p, ncrit, theta, fa, dtp, dt):
+def _run_device(st0, *, p, ncrit, theta, fa, dtp, dt, gradient=False):
     import taichi_collisional_b200 as t
     g = _gravity(p=p, ncrit=ncrit, theta=theta)
     g.set_error_mac(True, fa)
     dev = {k: _cuda(st0[k]) for k in t.EVOLVE_KEYS}
     dev["id"] = _cuda(st0["id"], torch.int32)
-    stats = g.evolve_hold_dkd(dev, dtp, dt)
+    stats = (g.evolve_omelyan if gradient else g.evolve_hold_dkd)(dev, dtp, dt)
     out = {k: v.cpu().numpy() for k, v in dev.items()}
     g.close()
     return out, stats
@@ -165,3 +165,29 @@ def test_evolve_close_to_reference_fixture(evolve_case):
     assert err.max() / disp.max() < 1e-3
     assert verr.max() / dv.max() < 1e-3
     assert stats["n_evaluations"] > 0 and stats["max_level"] >= 1
+
+
+@pytest.mark.skipif(not os.path.exists(oracle.integ_shim_path(True)),
+                    reason="shim-driven reference integrator (GRADIENT build) not built")
+def test_gradient_scheme_matches_reference_integrator_over_the_same_forces():
+    """The reference's default scheme, evolve_split_omelyan of its GRADIENT / OUTPUTACC build,
+    compiled against this library through the shim, against tc_evolve_omelyan on the same 1,024
+    bodies and step: the same splits (every body gets its system's least time step), the same
+    dt / 6 kicks, drifts and force-gradient kicks at the shifted positions -- the same final order,
+    time and state up to rounding."""
+    f = dict(np.load(os.path.join(GOLD, "evolve_hold_plummer_kroupa1k.npz")))
+    st0 = _evolve_state(str(f["gen"]), int(f["n"]), int(f["seed"]))
+    kw = dict(p=8, ncrit=int(f["ncrit"]), theta=float(f["theta"]), fa=float(f["force_accuracy"]),
+              dtp=float(f["dt_param"]), dt=float(f["dt"]))
+    out, stats = _run_device(st0, gradient=True, **kw)
+    ref, simtime = oracle.ref_evolve_gradient(st0, ncrit=kw["ncrit"], theta=kw["theta"], force_accuracy=kw["fa"],
+                                              dt_param=kw["dtp"], dt=kw["dt"])
+    assert simtime == stats["simtime"]
+    assert np.array_equal(out["id"], ref["id"])
+    assert np.unique(out["timestep"]).size == 1  # the GRADIENT build's shared least time step
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        np.testing.assert_allclose(out[k], ref[k], rtol=1e-12, atol=1e-14, err_msg=k)
+    for k in ("timestep", "pot"):
+        np.testing.assert_allclose(out[k], ref[k], rtol=1e-10, atol=0, err_msg=k)
+    assert stats["max_level"] >= 1 and stats["n_evaluations"] > 0
+

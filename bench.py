@@ -103,7 +103,10 @@ def parse():
     ap.add_argument("--diagnostics", type=int, default=0, metavar="N",
                     help="time the system diagnostics (energies, centre of mass) over N bodies instead")
     ap.add_argument("--evolve", type=int, default=0, metavar="N",
-                    help="time one step of the HOLD block-time-step integrator on N bodies instead")
+                    help="time one step of the reference's block-time-step integrator on N bodies instead")
+    ap.add_argument("--scheme", default="hold", choices=["hold", "gradient"],
+                    help="--evolve: the HOLD scheme or the force-gradient (Omelyan) scheme of the reference's "
+                         "default build")
     return ap.parse_args()
 
 
@@ -328,25 +331,29 @@ def run_evolve(args):
     st["id"] = torch.arange(n, dtype=torch.int32, device="cuda")
     g = tcb.Gravity(p=8, ncrit=64, theta=0.4, variant=tcb.VARIANT_TOP, precision=tcb.PREC_FP64)
     g.set_error_mac(True, fa)
+    grad = args.scheme == "gradient"
+    step = g.evolve_omelyan if grad else g.evolve_hold_dkd
     for _ in range(args.warmup):
-        g.evolve_hold_dkd(st, dtp, dt)
+        step(st, dtp, dt)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     stats = []
     e0.record()
     for _ in range(args.steps):
-        stats.append(g.evolve_hold_dkd(st, dtp, dt))
+        stats.append(step(st, dtp, dt))
     e1.record()
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1) / args.steps
-    line = {"metric": "particle-steps/s of one HOLD block-time-step step (p=8, error MAC)", "impl": "ours",
+    name = "force-gradient (Omelyan)" if grad else "HOLD"
+    line = {"metric": "particle-steps/s of one %s block-time-step step (p=8, error MAC)" % name, "impl": "ours",
             "value": n / (ms * 1e-3), "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms, "higher_is_better": True, "dtype": "f64", "data": "synthetic (seeded Plummer/Kroupa)",
-            "config": {"workload": "hold_dkd_plummer_kroupa_N%d_p8_fa2e-7_dt1/64" % n, "n": n, "p": 8, "ncrit": 64,
+            "config": {"workload": "%s_plummer_kroupa_N%d_p8_fa2e-7_dt1/64" % ("omelyan" if grad else "hold_dkd", n),
+                       "n": n, "p": 8, "ncrit": 64,
                        "force_accuracy": fa, "dt": dt, "dt_param": dtp},
             "per_step": {k: [s[k] for s in stats] for k in ("n_evaluations", "n_direct", "max_level")}}
     import oracle
-    if not args.no_cpu_baseline and oracle.integ_ref_available():
+    if not args.no_cpu_baseline and not grad and oracle.integ_ref_available():
         xs, ys, zs, vxs, vys, vzs, ms_ = make_ics(EVOLVE_CPU_SAMPLE_N, 2027)
         z0 = np.zeros(EVOLVE_CPU_SAMPLE_N)
         s0 = dict(x=xs, y=ys, z=zs, vx=vxs, vy=vys, vz=vzs, m=ms_, ex=z0, ey=z0, ez=z0, timestep=z0, pot=z0,

@@ -26,6 +26,9 @@ struct TcBodies {
   uint8_t* flags;  // bit0 sink, bit1 source
   int* perm;       // sorted position -> caller index
   double eps2 = 0.0;  // Plummer softening squared of the pair interactions (0: Newtonian)
+  // mixed near field only: per body (xh yh zh mh) (xl yl zl ml) (vx vy vz 0), FP32 (hi, lo) splits
+  // of the position and of the source mass (0 for a non-source), filled by k_body_f32
+  float4* f32 = nullptr;
 };
 
 // Cells in breadth-first order; level l occupies [lvl_start[l], lvl_start[l+1]).

@@ -377,6 +377,8 @@ static TcBodies bodies_view(tc_ctx* c, int n, bool jerk) {
   b.flags = c->bflags.p;
   b.perm = c->perm.p;
   b.eps2 = c->prm.softening * c->prm.softening;
+  // the mixed near field's FP32 splits sit after the seven FP64 arrays (16-byte aligned)
+  b.f32 = c->prm.precision != TC_PREC_FP64 ? reinterpret_cast<float4*>(d + 7 * N + (N & 1)) : nullptr;
   return b;
 }
 
@@ -981,10 +983,12 @@ static tc_status run_fmm(tc_ctx* ctx, int n) {
     }
   } else if (hs[1] > 0) {
     int g = nblocks(hs[1], kP2PWarps);
-    if (mixed_p2p)
+    if (mixed_p2p) {
+      k_body_f32<JERK><<<nblocks(n, 256), 256, 0, st>>>(n, b);
+      ctx->launches++;
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, (int)hs[1], ctx->p2p_start.p, ctx->p2p_src.p, b,
                                                        cv, o, kP2PExclFrac);
-    else {
+    } else {
       // few target leaves (small n): split each leaf's sources over up to 16 warps, then fold
       // the chunks in order (k_p2p_join); the split depends on n only, as in the graph path
       const int ntl = (int)hs[1];
@@ -1130,6 +1134,10 @@ static void run_fmm_graph(tc_ctx* ctx, int n) {
   graph_event(ctx, 5, st);
   {
     const int g = nblocks(ccap, kP2PWarps);  // a warp per target slot; warps past the count exit
+    if (prm.precision != TC_PREC_FP64) {
+      k_body_f32<JERK><<<nblocks(n, 256), 256, 0, st>>>(n, b);
+      L++;
+    }
     if (prm.precision != TC_PREC_FP64)
       k_p2p_mixed<JERK><<<g, kP2PWarps * 32, 0, st>>>(ctx->p2p_tl.p, ccap, ctx->p2p_start.p, ctx->p2p_src.p, b, cv, o,
                                                        kP2PExclFrac, ctx->d_small + 1);
@@ -1622,7 +1630,8 @@ static tc_status evaluate_impl(tc_ctx* ctx, int n, const double* x, const double
   // ---- buffers sized by N
   TC_CK(ctx->keys.ensure(N)); TC_CK(ctx->keys_alt.ensure(N));
   TC_CK(ctx->vals.ensure(N)); TC_CK(ctx->vals_alt.ensure(N));
-  TC_CK(ctx->bod.ensure(7 * N)); TC_CK(ctx->bflags.ensure(N)); TC_CK(ctx->perm.ensure(N));
+  TC_CK(ctx->bod.ensure(ctx->prm.precision != TC_PREC_FP64 ? 13 * N + 2 : 7 * N));
+  TC_CK(ctx->bflags.ensure(N)); TC_CK(ctx->perm.ensure(N));
   TC_CK(ctx->outs.ensure(7 * N));
   TC_CK(ctx->hist.ensure(257 * ((N + kRsTile - 1) / kRsTile + 1) + 1024));
   TC_CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(unsigned), st));

@@ -445,9 +445,9 @@ namespace tc {
 // still fill the warp).  A tile takes the next 32 bodies of the target's source cells read as
 // one sequence, so small source leaves still fill it.
 //
-// Arithmetic.  Sources are staged per 32-source tile as FP32 (hi, lo) pairs of positions
-// relative to the target cell's centre and of masses, formed in FP64, so dx = (xj_hi - xi_hi)
-// + (xj_lo - xi_lo) carries one rounding even for close pairs.  Each lane evaluates two
+// Arithmetic.  Sources are staged per 32-source tile as FP32 (hi, lo) pairs of positions and of
+// masses, formed in FP64 once per evaluation (k_body_f32), so dx = (xj_hi - xi_hi) + (xj_lo -
+// xi_lo) carries one rounding even for close pairs (the hi parts of neighbours subtract exactly).  Each lane evaluates two
 // sources at once with the packed FP32x2 instructions of sm_100 (FADD2/FMUL2/FFMA2: one issue
 // for two pairs); the tile stores the two sources' fields side by side so one 16-byte
 // broadcast load feeds both halves.  1/r is the hardware estimate refined by one Newton
@@ -515,17 +515,37 @@ struct TcMixP {
   TcF2 pot, ax, ay, az, jx, jy, jz;   // compensated totals
 };
 
-// stage source j (or a zero-mass source at the cell centre when j < 0) at tile slot l
+// The FP32 splits of every body, once per evaluation: positions as (hi, lo) pairs of the
+// coordinates themselves (the difference (xj_hi - xi_hi) + (xj_lo - xi_lo) of two bodies keeps
+// one rounding, the hi parts of neighbours subtracting exactly), the source mass likewise (0 for
+// a non-source), velocities rounded.  Each tile then reads three 16-byte words per source.
 template <bool JERK>
-__device__ __forceinline__ void tc_tile_put(TcTile& T, int l, const TcBodies& b, int j, double Xc, double Yc,
-                                            double Zc) {
+__global__ void k_body_f32(int n, const TcBodies b) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  float xh, yh, zh, xl, yl, zl, mh, ml;
+  tc_split(b.x[j], 0.0, xh, xl);
+  tc_split(b.y[j], 0.0, yh, yl);
+  tc_split(b.z[j], 0.0, zh, zl);
+  tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, mh, ml);
+  b.f32[3 * (size_t)j] = make_float4(xh, yh, zh, mh);
+  b.f32[3 * (size_t)j + 1] = make_float4(xl, yl, zl, ml);
+  b.f32[3 * (size_t)j + 2] =
+      JERK ? make_float4((float)b.vx[j], (float)b.vy[j], (float)b.vz[j], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// stage source j (or a zero-mass source at the origin when j < 0) at tile slot l
+template <bool JERK>
+__device__ __forceinline__ void tc_tile_put(TcTile& T, int l, const TcBodies& b, int j, double, double, double) {
   float xh = 0.f, yh = 0.f, zh = 0.f, xl = 0.f, yl = 0.f, zl = 0.f, mh = 0.f, ml = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
   if (j >= 0) {
-    tc_split(b.x[j], Xc, xh, xl);
-    tc_split(b.y[j], Yc, yh, yl);
-    tc_split(b.z[j], Zc, zh, zl);
-    tc_split((b.flags[j] & 2) ? b.m[j] : 0.0, 0.0, mh, ml);
-    if (JERK) { vx = (float)b.vx[j]; vy = (float)b.vy[j]; vz = (float)b.vz[j]; }
+    const float4 h = b.f32[3 * (size_t)j], lo = b.f32[3 * (size_t)j + 1];
+    xh = h.x; yh = h.y; zh = h.z; mh = h.w;
+    xl = lo.x; yl = lo.y; zl = lo.z; ml = lo.w;
+    if (JERK) {
+      const float4 v = b.f32[3 * (size_t)j + 2];
+      vx = v.x; vy = v.y; vz = v.z;
+    }
   }
   const int p = l >> 1, h = l & 1;
   float* g0 = reinterpret_cast<float*>(&T.g[0][p]);
@@ -615,10 +635,13 @@ __device__ __forceinline__ void tc_mixp_init(TcMixP<JERK>& T, const TcBodies& b,
   float xh = 0.f, yh = 0.f, zh = 0.f, xl = 0.f, yl = 0.f, zl = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
   T.tau = 0.f;
   if (v) {
-    tc_split(b.x[i], Xc, xh, xl);
-    tc_split(b.y[i], Yc, yh, yl);
-    tc_split(b.z[i], Zc, zh, zl);
-    if (JERK) { vx = (float)b.vx[i]; vy = (float)b.vy[i]; vz = (float)b.vz[i]; }
+    const float4 h = b.f32[3 * (size_t)i], lo = b.f32[3 * (size_t)i + 1];
+    xh = h.x; yh = h.y; zh = h.z;
+    xl = lo.x; yl = lo.y; zl = lo.z;
+    if (JERK) {
+      const float4 w = b.f32[3 * (size_t)i + 2];
+      vx = w.x; vy = w.y; vz = w.z;
+    }
     const double a = sqrt(out.ax[i] * out.ax[i] + out.ay[i] * out.ay[i] + out.az[i] * out.az[i]);
     T.tau = (float)(excl_frac * a);
   }

@@ -91,11 +91,12 @@ __device__ __forceinline__ int tc_pair_class_mlp(const TcCells& c, int t, int s,
                                                  double budget, const TcMlpTc& T, float* act, const TcMlpNorm& norm,
                                                  const float* __restrict__ featc, int lane) {
   constexpr int NO = TcOrderClasses<P>::n;
+  // the features and the budget in FP32 (the network itself runs on TF32 operands)
   const double dx = c.X[t] - c.X[s], dy = c.Y[t] - c.Y[s], dz = c.Z[t] - c.Z[s];
-  const double r2 = dx * dx + dy * dy + dz * dz, r = sqrt(r2);
+  const float r2 = (float)(dx * dx + dy * dy + dz * dz), lr = 0.5f * logf(r2);
   float x[kMlpIn], y[NO];
-  x[0] = (float)log(c.R[t] / r);
-  x[1] = (float)log(c.R[s] / r);
+  x[0] = logf((float)c.R[t]) - lr;
+  x[1] = logf((float)c.R[s]) - lr;
 #pragma unroll
   for (int j = 0; j < 5; j++) x[2 + j] = featc[(size_t)s * 5 + j];
   x[7] = featc[(size_t)t * 5 + 4];
@@ -104,7 +105,8 @@ __device__ __forceinline__ int tc_pair_class_mlp(const TcCells& c, int t, int s,
   tc_mlp_infer_tc<NO>(T, act, x, y, lane);
   if (!(budget > 0.0)) return NO - 1;
   // log10 of the budget relative to the source's monopole acceleration
-  const float lim = (float)log10(budget * r2 / fmax(pn[(size_t)s * (P + 1)], 1e-300));
+  const float lim = (logf((float)budget) + logf(r2) - logf(fmaxf((float)pn[(size_t)s * (P + 1)], 1e-37f))) *
+                    0.43429448f;
 #pragma unroll
   for (int i = 0; i < NO - 1; i++)
     if (y[i] + norm.out_mean <= lim) return i;

@@ -153,42 +153,51 @@ __device__ __forceinline__ void tc_mma_tf32(float* d, const uint32_t* a, const u
 template <int K, int NT, bool TANH>
 __device__ __forceinline__ void tc_mlp_tc_layer(float* act, const float* W, int ws, const float* bias, int lane) {
   const int g = lane >> 2, t = lane & 3;
+  float acc[2][NT][4];
 #pragma unroll
-  for (int mt = 0; mt < 2; mt++) {
-    float acc[NT][4];
+  for (int nt = 0; nt < NT; nt++) {
+    const float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
 #pragma unroll
-    for (int nt = 0; nt < NT; nt++) {
-      acc[nt][0] = acc[nt][2] = bias[nt * 8 + 2 * t];
-      acc[nt][1] = acc[nt][3] = bias[nt * 8 + 2 * t + 1];
+    for (int mt = 0; mt < 2; mt++) {
+      acc[mt][nt][0] = acc[mt][nt][2] = b0;
+      acc[mt][nt][1] = acc[mt][nt][3] = b1;
     }
+  }
+  // each weight fragment is loaded once and feeds both 16-row tiles
 #pragma unroll
-    for (int kt = 0; kt < K / 8; kt++) {
+  for (int kt = 0; kt < K / 8; kt++) {
+    uint32_t a[2][4];
+#pragma unroll
+    for (int mt = 0; mt < 2; mt++) {
       const float* r0 = act + (mt * 16 + g) * kMlpActS + kt * 8;
       const float* r1 = r0 + 8 * kMlpActS;
-      uint32_t a[4];
-      a[0] = __float_as_uint(tc_to_tf32(r0[t]));
-      a[1] = __float_as_uint(tc_to_tf32(r1[t]));
-      a[2] = __float_as_uint(tc_to_tf32(r0[t + 4]));
-      a[3] = __float_as_uint(tc_to_tf32(r1[t + 4]));
-#pragma unroll
-      for (int nt = 0; nt < NT; nt++) {
-        const float* wr = W + (nt * 8 + g) * ws + kt * 8;
-        const uint32_t b[2] = {__float_as_uint(wr[t]), __float_as_uint(wr[t + 4])};
-        tc_mma_tf32(acc[nt], a, b);
-      }
+      a[mt][0] = __float_as_uint(tc_to_tf32(r0[t]));
+      a[mt][1] = __float_as_uint(tc_to_tf32(r1[t]));
+      a[mt][2] = __float_as_uint(tc_to_tf32(r0[t + 4]));
+      a[mt][3] = __float_as_uint(tc_to_tf32(r1[t + 4]));
     }
-    __syncwarp();  // rows mt * 16 .. + 15 are read by every lane before they are overwritten
+#pragma unroll
+    for (int nt = 0; nt < NT; nt++) {
+      const float* wr = W + (nt * 8 + g) * ws + kt * 8;
+      const uint32_t b[2] = {__float_as_uint(wr[t]), __float_as_uint(wr[t + 4])};
+      tc_mma_tf32(acc[0][nt], a[0], b);
+      tc_mma_tf32(acc[1][nt], a[1], b);
+    }
+  }
+  __syncwarp();  // every row is read by every lane before any is overwritten
+#pragma unroll
+  for (int mt = 0; mt < 2; mt++) {
 #pragma unroll
     for (int nt = 0; nt < NT; nt++) {
       float* o0 = act + (mt * 16 + g) * kMlpActS + nt * 8 + 2 * t;
       float* o1 = o0 + 8 * kMlpActS;
-      o0[0] = TANH ? tc_tanh_fast(acc[nt][0]) : acc[nt][0];
-      o0[1] = TANH ? tc_tanh_fast(acc[nt][1]) : acc[nt][1];
-      o1[0] = TANH ? tc_tanh_fast(acc[nt][2]) : acc[nt][2];
-      o1[1] = TANH ? tc_tanh_fast(acc[nt][3]) : acc[nt][3];
+      o0[0] = TANH ? tc_tanh_fast(acc[mt][nt][0]) : acc[mt][nt][0];
+      o0[1] = TANH ? tc_tanh_fast(acc[mt][nt][1]) : acc[mt][nt][1];
+      o1[0] = TANH ? tc_tanh_fast(acc[mt][nt][2]) : acc[mt][nt][2];
+      o1[1] = TANH ? tc_tanh_fast(acc[mt][nt][3]) : acc[mt][nt][3];
     }
-    __syncwarp();
   }
+  __syncwarp();
 }
 
 // warp-wide: every lane passes its pair's standardised features x and gets its outputs y

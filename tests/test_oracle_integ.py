@@ -87,3 +87,16 @@ def test_against_reference_harness_random_inputs():
         p1, f1 = oracle.split_order(ts, dt)
         p2, f2 = oracle.ref_split(ts, dt)
         assert f1 == f2 and np.array_equal(p1, p2)
+
+
+@pytest.mark.parametrize("gradient", [False, True])
+def test_shim_driven_reference_integrators_load(gradient):
+    """The reference's integrator compiled over this library through the shim -- its HOLD build
+    and its default GRADIENT / OUTPUTACC build (the check of tc_evolve_omelyan) -- loads and
+    exports the step entry point (the GPU tests run it)."""
+    import ctypes
+    path = oracle.integ_shim_path(gradient)
+    if not os.path.exists(path):
+        pytest.skip("shim-driven reference integrator not built")
+    lib = ctypes.CDLL(path)
+    assert hasattr(lib, "tcr_evolve_hold")

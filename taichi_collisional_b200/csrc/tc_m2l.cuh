@@ -65,17 +65,16 @@ struct TcPairGeo {
   double rinv;
 };
 
+// the pair's rotation angles and 1/r from two reciprocal square roots (each warp of a group
+// computes them for its lanes' pairs, so they stay off the divide and square-root sequences)
 __device__ __forceinline__ TcPairGeo tc_pair_geo(double dx, double dy, double dz) {
   TcPairGeo g;
-  double rxy2 = dx * dx + dy * dy, rxy = sqrt(rxy2);
-  double r = sqrt(rxy2 + dz * dz);
-  g.rinv = 1.0 / r;
-  g.ez1 = mk(1, 0);
+  const double rxy2 = dx * dx + dy * dy;
+  g.rinv = rsqrt(rxy2 + dz * dz);
+  const double q = rxy2 > 0 ? rsqrt(rxy2) : 0.0;  // 1 / rxy
+  const double rxy = rxy2 * q;
   g.ex1 = mk(dz * g.rinv, -rxy * g.rinv);
-  if (rxy > 0) {
-    double q = 1.0 / rxy;
-    g.ez1 = mk(dy * q, dx * q);
-  }
+  g.ez1 = rxy2 > 0 ? mk(dy * q, dx * q) : mk(1, 0);
   return g;
 }
 
